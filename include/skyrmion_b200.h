@@ -1,0 +1,137 @@
+/* skyrmion_b200 — C ABI of the B200-native (sm_100a) skyrmion_solver lattice engine.
+ *
+ * Every entry point takes plain pointers and sizes; device buffers are raw
+ * CUDA device pointers, "host" arguments are host pointers, `stream` is a
+ * cudaStream_t (NULL = legacy default stream).  Calls are asynchronous on
+ * `stream` unless an output is a host pointer, in which case the call
+ * synchronises that stream before returning.
+ *
+ * Parameter ABI: `p_i` (int32, n_pi entries) and `p_f` (float64, n_pf entries)
+ * are the reference's packed parameter arrays (skyrmion_solver
+ * core/params.py:227-267 plus the theory's pack_device_params):
+ *   p_i = [xlen, ylen, zlen, halo, ncoord, nfields, dim_grid, dim_fields,
+ *          killkinen, newtonflow, unit_length, <theory ints...>]
+ *   p_f = [xsize, ysize, zsize, lsx, lsy, lsz, grid_volume, time_step,
+ *          <theory couplings...>]
+ * Field buffers use the reference layout: FP64, index a*N + x*Y*Z + y*Z + z.
+ *
+ * Return value: a sky_status (0 = success).
+ */
+#ifndef SKYRMION_B200_H
+#define SKYRMION_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SKY_OK = 0,
+    SKY_ERR_INVALID = 1,   /* bad argument: sizes, parameter arrays, theory id */
+    SKY_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    SKY_ERR_NONFINITE = 3, /* a reduction met NaN/Inf */
+    SKY_ERR_TIMEOUT = 4,   /* a bounded device-side wait gave up */
+    SKY_ERR_NOMEM = 5      /* caller-provided scratch too small / allocation failed */
+} sky_status;
+
+typedef enum {
+    SKY_THEORY_NUCLEAR = 0,       /* th/nuclear_skyrme        C = 4  */
+    SKY_THEORY_OMEGA = 1,         /* th/omega_skyrme          C = 5  */
+    SKY_THEORY_COULOMB = 2,       /* th/coulomb_skyrme        C = 5  */
+    SKY_THEORY_RHO = 3,           /* th/rho_skyrme            C = 13 */
+    SKY_THEORY_BERGER = 4,        /* th/berger_skyrme         C = 4  */
+    SKY_THEORY_LIGHTLY_BOUND = 5  /* th/lightly_bound_skyrme  C = 4  */
+} sky_theory;
+
+/* Library version string and the last CUDA error text seen by this thread. */
+const char* sky_version(void);
+const char* sky_last_error(void);
+
+/* Number of field components the theory's kernels are built for. */
+int sky_theory_components(int theory);
+
+/* Doubles of scratch that sky_sum / sky_max / sky_total_* need for n values. */
+int64_t sky_reduce_scratch_size(int64_t n);
+
+/* ------------------------------------------------------------------------ *
+ * Reference-layout FP64 kernels (drop-ins for the reference's launches).
+ * ------------------------------------------------------------------------ */
+
+/* Replaces the theory's do_gradient_step_kernel
+ * (core/integrator.py:37-46 + th/<theory>/kernels.py: do_gradient_step_point):
+ * EG = projected energy gradient of `field`, l_out = -time_step * EG.
+ * The reference's d1fd1x / d2fd2x scratch buffers are not needed. */
+int sky_gradient_step(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                      double* l_out, const double* field, double* energy_gradient, void* stream);
+
+/* Replaces do_rk4_step_kernel (core/integrator.py:50-92):
+ * k_out = dt (velocity + factor l_in); temp = field + factor k_prev. */
+int sky_rk4_stage(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf, double* k_out,
+                  const double* velocity, const double* l_in, double* temp, const double* field,
+                  const double* k_prev, double factor, void* stream);
+
+/* Replaces the theory's do_rk4_kernel (core/integrator.py:163-175 with the
+ * theory's norm / projection).  theory < 0 selects do_rk4_kernel_no_constraint
+ * (core/integrator.py:94-141). */
+int sky_rk4_finalize(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                     double* velocity, double* field, const double* k1, const double* k2, const double* k3,
+                     const double* k4, const double* l1, const double* l2, const double* l3, const double* l4,
+                     void* stream);
+
+/* Replaces compute_energy_kernel (e.g. th/nuclear_skyrme/kernels.py:350-382): en = e * h^3. */
+int sky_energy_density(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                       double* en, const double* field, void* stream);
+
+/* Replaces compute_skyrmion_number_kernel (e.g. th/nuclear_skyrme/kernels.py:450-482). */
+int sky_baryon_density(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                       double* en, const double* field, void* stream);
+
+/* Replaces compute_potential_kernel (th/omega_skyrme/kernels.py:413-441,
+ * th/coulomb_skyrme/kernels.py:417-445): en = field component p_i[11]. */
+int sky_potential_density(const int32_t* p_i, int32_t n_pi, double* en, const double* field, void* stream);
+
+/* Replaces compute_rho_meson_kernel (th/rho_skyrme/kernels.py:385-412): en += sum_{a>=4} field_a^2. */
+int sky_rho_meson_density(const int32_t* p_i, int32_t n_pi, double* en, const double* field, void* stream);
+
+/* Replaces set_field_zero_kernel (core/utils.py:148-174). */
+int sky_set_field_zero(const int32_t* p_i, int32_t n_pi, double* field, void* stream);
+
+/* Replaces create_grid_kernel (e.g. th/nuclear_skyrme/kernels.py:27-56): grid_i = h_i * index. */
+int sky_create_grid(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf, double* grid,
+                    void* stream);
+
+/* Replace compute_sum / compute_max (core/utils.py:201-279, 321-373):
+ * deterministic FP64 reductions (compensated sum; signed max).  `scratch` is a
+ * device buffer of sky_reduce_scratch_size(n) doubles; the result is written to
+ * *out_host (host pointer; the stream is synchronised) and, if out_dev is not
+ * NULL, also to out_dev[0] on the device. */
+int sky_sum(const double* values, int64_t n, double* scratch, int64_t n_scratch, double* out_host,
+            double* out_dev, void* stream);
+int sky_max(const double* values, int64_t n, double* scratch, int64_t n_scratch, double* out_host,
+            double* out_dev, void* stream);
+
+/* Replace the host compute_energy / compute_skyrmion_number
+ * (th/nuclear_skyrme/observables.py:408-474): the per-site density and its
+ * compensated FP64 sum fused into one launch (no per-site buffer round trip). */
+int sky_total_energy(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                     const double* field, double* scratch, int64_t n_scratch, double* out_host, void* stream);
+int sky_total_baryon(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                     const double* field, double* scratch, int64_t n_scratch, double* out_host, void* stream);
+
+/* Replaces do_arrested_newton_flow (core/integrator.py:284-410): one RK4 step of
+ * the arrested Newton flow with the reference's buffers and semantics (k1..k4,
+ * l1..l4, temp and energy_gradient hold the same content afterwards; velocity is
+ * zeroed when killkinen and the new energy exceeds prev_energy).  Writes the new
+ * energy and err (signed max of the stage-4 gradient) to host pointers. */
+int sky_arrested_newton_step(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                             double* velocity, double* field, double* energy_gradient, double* k1, double* k2,
+                             double* k3, double* k4, double* l1, double* l2, double* l3, double* l4, double* temp,
+                             double* scratch, int64_t n_scratch, double prev_energy, double* new_energy_host,
+                             double* err_host, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SKYRMION_B200_H */

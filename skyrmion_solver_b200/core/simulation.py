@@ -1,0 +1,166 @@
+"""Simulation driver with the reference's interface (skyrmion_solver ``core/simulation.py:28-493``).
+
+``Simulation(params, theory)`` owns the FP64 device buffers (torch CUDA tensors
+in the reference's flattened SoA layout) and exposes the same attributes and
+methods: ``initialize``, ``set_params``, ``observables``, ``compute_*_density``,
+``step``, ``save_output``.  Buffers the engine never needs (the derivative
+scratch ``d1fd1x`` / ``d2fd2x`` and the diagnostic tensors) are allocated on
+first access only.
+"""
+from __future__ import annotations
+
+import inspect
+from pathlib import Path
+
+import numpy as np
+
+from .integrator import do_arrested_newton_flow, do_rk4_kernel_no_constraint
+from .launch import DeviceParams
+from .params import Params
+from .utils import launch_3d, scratch_doubles, set_field_zero_kernel
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("skyrmion_b200 needs a CUDA device (sm_100a); none is visible")
+    return torch
+
+
+class Simulation:
+    _LAZY = {
+        "d1fd1x": lambda rp: rp.number_coordinates * rp.number_total_fields * rp.dim_grid,
+        "d2fd2x": lambda rp: rp.number_coordinates ** 2 * rp.number_total_fields * rp.dim_grid,
+        "obs4": lambda rp: 4 * rp.dim_grid,
+        "obs9": lambda rp: 9 * rp.dim_grid,
+        "tensor_scratch": lambda rp: rp.dim_grid,
+        "com_d": lambda rp: 3,
+    }
+
+    def __init__(self, params, theory):
+        self.theory = theory
+        self.kernels = theory.kernels
+        self.initial_config = theory.initial_config
+        self.observables_mod = theory.observables
+        self.threads3d = getattr(self.theory, "threads3d", (8, 8, 4))
+        self.gradient_step_kernel = getattr(self.kernels, "do_gradient_step_kernel", None)
+        if self.gradient_step_kernel is None:
+            raise AttributeError("Theory kernels must provide do_gradient_step_kernel.")
+        self.rk4_kernel = getattr(self.kernels, "do_rk4_kernel", None)
+        if self.rk4_kernel is None:
+            self.rk4_kernel = do_rk4_kernel_no_constraint
+        self.set_params(params)
+        torch = _torch()
+        rp = self.rp
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+
+        def arr(n):
+            return torch.empty(int(n), dtype=torch.float64, device=dev)
+
+        for name in ("Field", "Velocity", "EnergyGradient", "k1", "k2", "k3", "k4", "l1", "l2", "l3", "l4",
+                     "Temp"):
+            setattr(self, name, arr(rp.dim_fields))
+        self.grid = arr(rp.number_coordinates * rp.dim_grid)
+        self.en = torch.zeros(rp.dim_grid, dtype=torch.float64, device=dev)
+        self.entmp = torch.zeros(rp.dim_grid, dtype=torch.float64, device=dev)
+        self.gridsum_partial = torch.zeros(2 * scratch_doubles(), dtype=torch.float64, device=dev)
+        self.max_partial = torch.zeros(scratch_doubles(), dtype=torch.float64, device=dev)
+
+    def __getattr__(self, name):
+        # lazily allocated buffers with the reference's sizes
+        sizes = type(self)._LAZY
+        if name in sizes and "rp" in self.__dict__:
+            torch = _torch()
+            buf = torch.zeros(int(sizes[name](self.rp)), dtype=torch.float64, device=self.device)
+            setattr(self, name, buf)
+            return buf
+        raise AttributeError(name)
+
+    # ------------------------------------------------------------------
+    def set_params(self, p):
+        """Resolve and pack the parameters (core/simulation.py:175-197)."""
+        self.p = p
+        self.rp = p.resolved() if isinstance(p, Params) else p
+        p_i_h, p_f_h = self.theory.params.pack_device_params(self.rp)
+        self.p_i_h = np.asarray(p_i_h, dtype=np.int32)
+        self.p_f_h = np.asarray(p_f_h, dtype=np.float64)
+        self.p_i_d = DeviceParams(self.p_i_h)
+        self.p_f_d = DeviceParams(self.p_f_h)
+
+    def initialize(self, init_config: dict | None = None):
+        """Grid, zeroed Field / Velocity, then the theory's initializer (core/simulation.py:124-173)."""
+        cfg = init_config or {}
+        grid3d, block3d = launch_3d(self.p_i_h, threads=self.threads3d)
+        self.kernels.create_grid_kernel[grid3d, block3d](self.grid, self.p_i_d, self.p_f_d)
+        set_field_zero_kernel[grid3d, block3d](self.Field, self.p_i_d)
+        set_field_zero_kernel[grid3d, block3d](self.Velocity, self.p_i_d)
+        kw = dict(Velocity=self.Velocity, Field=self.Field, grid=self.grid, k1=self.k1, k2=self.k2, k3=self.k3,
+                  k4=self.k4, l1=self.l1, l2=self.l2, l3=self.l3, l4=self.l4, Temp=self.Temp, p_i_d=self.p_i_d,
+                  p_f_d=self.p_f_d, p_i_h=self.p_i_h, p_f_h=self.p_f_h, grid3d=grid3d, block3d=block3d, config=cfg)
+        sig = inspect.signature(self.initial_config.initialize)
+        if "d1fd1x" in sig.parameters:
+            kw["d1fd1x"] = self.d1fd1x
+        self.initial_config.initialize(**kw)
+        _torch().cuda.synchronize()
+
+    def observables(self):
+        """Energy and baryon number (core/simulation.py:199-217)."""
+        obs = {"energy": self.observables_mod.compute_energy(
+            self.Field, None, self.en, self.entmp, self.gridsum_partial, self.p_i_d, self.p_f_d, self.p_i_h,
+            self.p_f_h)}
+        if hasattr(self.observables_mod, "compute_skyrmion_number"):
+            obs["skyrmion_number"] = self.observables_mod.compute_skyrmion_number(
+                self.Field, None, self.en, self.entmp, self.gridsum_partial, self.p_i_d, self.p_f_d, self.p_i_h)
+        return obs
+
+    def _launch(self):
+        return launch_3d(self.p_i_h, threads=self.threads3d)
+
+    def compute_energy_density(self):
+        g, b = self._launch()
+        self.kernels.compute_energy_kernel[g, b](self.en, self.Field, None, self.p_i_d, self.p_f_d)
+
+    def compute_baryon_density(self):
+        g, b = self._launch()
+        self.kernels.compute_skyrmion_number_kernel[g, b](self.en, self.Field, None, self.p_i_d, self.p_f_d)
+
+    def compute_potential_density(self):
+        g, b = self._launch()
+        self.kernels.compute_potential_kernel[g, b](self.en, self.Field, self.p_i_d, self.p_f_d)
+
+    def compute_rho_meson_density(self):
+        g, b = self._launch()
+        self.kernels.compute_rho_meson_kernel[g, b](self.en, self.Field, self.p_i_d)
+
+    def step(self, prev_energy: float):
+        """One arrested-Newton / RK4 step; returns (new_energy, err) (core/simulation.py:287-308)."""
+        compute_norm = getattr(self.observables_mod, "compute_norm", None)
+        do_norm_kernel = getattr(self.kernels, "do_norm_kernel", None)
+        return do_arrested_newton_flow(
+            self.Velocity, self.Field, None, None, self.EnergyGradient, self.k1, self.k2, self.k3, self.k4,
+            self.l1, self.l2, self.l3, self.l4, self.Temp, self.en, self.entmp, self.gridsum_partial,
+            self.max_partial, self.p_i_d, self.p_f_d, self.p_i_h, self.p_f_h, prev_energy,
+            self.observables_mod.compute_energy, self.gradient_step_kernel, self.rk4_kernel,
+            compute_norm=compute_norm, do_norm_kernel=do_norm_kernel)
+
+    def save_output(self, output_dir: str | None = None, precision: int = 32):
+        """Snapshot of the state (field, velocity, densities, parameters) as ``state.npz``."""
+        out = Path(output_dir or "results")
+        out.mkdir(parents=True, exist_ok=True)
+        C = int(self.p_i_h[5])
+        dims = tuple(int(v) for v in self.p_i_h[:3])
+        self.compute_energy_density()
+        ed = self.en.cpu().numpy().reshape(dims)
+        self.compute_baryon_density()
+        bd = self.en.cpu().numpy().reshape(dims)
+        self.en.zero_()
+        np.savez(out / "state.npz", Field=self.Field.cpu().numpy().reshape((C,) + dims),
+                 Velocity=self.Velocity.cpu().numpy().reshape((C,) + dims), EnergyDensity=ed,
+                 BaryonDensity=bd, p_i=self.p_i_h, p_f=self.p_f_h)
+
+    def print_instructions(self):
+        if hasattr(self.theory, "print_instructions"):
+            self.theory.print_instructions()
+        else:
+            print("No specific instructions available for this theory.")

@@ -1,0 +1,4 @@
+"""Initial configurations of the Berger Skyrme model (host-built FP64 fields uploaded to ``Field``)."""
+from .._init_common import make_initialize
+
+initialize = make_initialize("berger")

@@ -1,0 +1,7 @@
+"""Host observables of the Lightly bound Skyrme model with the reference's signatures
+(skyrmion_solver th/lightly_bound_skyrme/observables.py: compute_energy, compute_skyrmion_number)."""
+from ...core.observables import BaryonObservable, EnergyObservable
+from .kernels import THEORY_ID
+
+compute_energy = EnergyObservable(THEORY_ID)
+compute_skyrmion_number = BaryonObservable(THEORY_ID)
