@@ -1,0 +1,528 @@
+#!/usr/bin/env python
+"""Benchmark of the lattice engine on the omega-meson B=4 relaxation (128^3, h = 0.15).
+
+Workload: the pion + omega-meson Skyrme variant (5 components), B = 4 cubic
+rational-map initial field with profile f(r) = pi exp(-r/2), 128^3 sites,
+spacing 0.15, time step 0.2 h, two-site vacuum shell, omega seeded as
+-c_omega B0, couplings of the reference's omega example (f_pi = 139.8,
+m_pi = 43.91, m_omega = 249.5, beta_omega = 8.036: mass 0.176, c_omega 14.34).
+State and stage arithmetic are FP32; energies, baryon numbers and the arrest
+test are FP64 with compensated summation.
+
+One bench step is one arrested-Newton step (four fused gradient stages, the RK4
+update with projection onto S^3, FP64 energy / baryon reductions and the
+device-side arrest decision) of the resident engine, replayed from CUDA graphs.
+
+The headline unit is converged solves/s: the measured step rate divided by the
+number of steps this solve needs before its energy stays within 1e-6 relative
+of the converged plain-FP64 energy (gradient max-norm <= 1e-6).  That step count
+is measured on the GPU by ``python bench.py --calibrate`` and kept in
+``profiles/convergence_omega_B4_128.json``; without it the value is null.
+
+Usage::
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --calibrate          # full FP64 and FP32 solves, writes the step counts
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "converged solves/s and p99 latency at 1e-6 rel. energy vs plain FP64; HBM GB/s"
+UNIT = "solves/s"
+WORKLOAD = "omega_B4_rational_map_128^3_h0.15"
+CALIBRATION = os.path.join(ROOT, "profiles", "convergence_omega_B4_128.json")
+TRAFFIC = os.path.join(ROOT, "profiles", "ncu_engine_stages_omega128_fp32.md")
+L = 128
+H = 0.15
+DT_FACTOR = 0.2
+COUPLINGS = dict(f_pi=139.8, m_pi=43.91, m_omega=249.5, beta_omega=8.036)
+INIT = {"mode": "rational_map", "baryon_number": 4, "scale": 2.0, "vacuum_shell": 2}
+REL_ENERGY_TOL = 1e-6
+GRAD_TOL = 1e-6
+# passes over one C-component field per stage launch (reads + writes)
+STAGE_PASSES = {"stage1": 2, "stage2": 3, "stage3": 4, "stage4": 7}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+
+def workload_params():
+    import numpy as np
+    from skyrmion_solver_b200 import theories as T
+    th = T.by_short_name("omega")
+    p = th.params.default_params(xlen=L, ylen=L, zlen=L, lsx=H, lsy=H, lsz=H, xsize=H * (L - 1),
+                                 ysize=H * (L - 1), zsize=H * (L - 1), time_step=DT_FACTOR * H, **COUPLINGS)
+    p_i, p_f = th.params.pack_device_params(p.resolved())
+    return th, p, np.asarray(p_i, dtype=np.int32), np.asarray(p_f, dtype=np.float64)
+
+
+def workload_field_device(p_i, p_f, device):
+    """Initial field on the device (FP64, reference layout), omega seeded by the library's own kernel."""
+    import torch
+    from skyrmion_solver_b200.theories._init_common import build_host_field, seed_omega
+    f = build_host_field("omega", p_i, p_f, INIT)
+    t = torch.from_numpy(f.ravel()).to(device)
+    seed_omega(t, p_i, p_f)
+    return t
+
+
+def load_calibration():
+    if not os.path.exists(CALIBRATION):
+        return None
+    with open(CALIBRATION) as fh:
+        return json.load(fh)
+
+
+def load_traffic(stage):
+    """Per-launch DRAM bytes (read + write) of one stage kernel from the committed ncu summary, or None."""
+    if not os.path.exists(TRAFFIC):
+        return None
+    import re
+    m = re.search(r"traffic_bytes_per_launch\[%s\]:\s*([0-9.eE+]+)" % stage, open(TRAFFIC).read())
+    return float(m.group(1)) if m else None
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.path = None
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_index), "--query-gpu=timestamp," + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        self.t_start = self.t_end = None
+
+    def mark_start(self):
+        self.t_start = time.time()
+
+    def mark_end(self):
+        self.t_end = time.time()
+
+    def stop(self):
+        if self.proc is None:
+            return {"unavailable": "nvidia-smi not found"}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                ts = time.mktime(time.strptime(parts[0].split(".")[0], "%Y/%m/%d %H:%M:%S"))
+                rows.append((ts, float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"unavailable": "no samples"}
+        lo = (self.t_start or 0) - 1.0
+        hi = (self.t_end or 1e18) + 1.0
+        win = [r for r in rows if lo <= r[0] <= hi] or rows
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in win for i, v in enumerate(r[3]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(r[1] for r in win), "sm_max_mhz": max(r[2] for r in win),
+                "reasons": reasons, "samples": len(win)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP64 NumPy oracle on all host cores (one process per core)
+# ---------------------------------------------------------------------------
+
+def _cpu_worker(args):
+    sub, nsteps, barrier, q = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    import numpy as np
+    from oracle import skyrme_oracle as O
+    th = O.THEORIES["omega"]
+    F, V, p_i, p_f = sub
+    E = O.total_energy(th, F, p_i, p_f)
+    barrier.wait()
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        F, V, E, err, _ = O.arrested_newton_step(th, F, V, p_i, p_f, E)
+    q.put((int(F[0].size) * nsteps, time.perf_counter() - t0))
+
+
+def cpu_sample_inputs(side=64):
+    """Central side^3 crop of the workload field, as its own lattice (same couplings, spacing, dt)."""
+    import numpy as np
+    from oracle import skyrme_oracle as O
+    from skyrmion_solver_b200.theories._init_common import build_host_field
+    th, p, p_i, p_f = workload_params()
+    F = build_host_field("omega", p_i, p_f, INIT)
+    N = int(p_i[6])
+    b = O.baryon_density(O.THEORIES["omega"], F, p_i, p_f)
+    F[4] = -float(p_f[9]) * b / float(p_f[6])
+    o = (L - side) // 2
+    Fc = np.ascontiguousarray(F[:, o:o + side, o:o + side, o:o + side])
+    p_i2 = p_i.copy()
+    p_i2[0:3] = side
+    p_i2[6] = side ** 3
+    p_i2[7] = int(p_i2[5]) * side ** 3
+    return Fc, np.zeros_like(Fc), p_i2, p_f
+
+
+def cpu_baseline(nsteps=2, side=64, max_procs=64):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    procs = max(1, min(os.cpu_count() or 1, max_procs))
+    sub = cpu_sample_inputs(side)
+    barrier = ctx.Barrier(procs)
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_cpu_worker, args=((sub, nsteps, barrier, q),)) for _ in range(procs)]
+    for pr in ps:
+        pr.start()
+    res = [q.get() for _ in ps]
+    for pr in ps:
+        pr.join()
+    site_steps = sum(r[0] for r in res)
+    secs = max(r[1] for r in res)
+    return dict(site_steps_per_s=site_steps / secs, cores=procs, secs=secs,
+                sample=f"{procs} processes x {nsteps} FP64 oracle arrested-Newton steps on a central {side}^3 crop "
+                       f"of the workload field ({site_steps} site-steps in {secs:.1f} s)")
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def emit(obj):
+    print(json.dumps(obj), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    cal = load_calibration()
+    cb = cpu_baseline()
+    N = L ** 3
+    steps_per_s = cb["site_steps_per_s"] / N
+    s64 = cal["fp64_steps_to_converge"] if cal else None
+    value = steps_per_s / s64 if s64 else None
+    emit({"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+          "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+          "config": {"workload": WORKLOAD, "sites": N, "precision": "fp64 (oracle)",
+                     "steps_to_converge": s64, "site_steps_per_s": cb["site_steps_per_s"]},
+          "cpu_baseline": {"value": value, "unit": UNIT, "cores": cb["cores"], "kind": "port",
+                           "sample": cb["sample"]},
+          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from skyrmion_solver_b200.core.simulation import Simulation
+    from skyrmion_solver_b200.engine import Engine
+
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    warmup = max(3, args.warmup)
+    K = args.steps
+    th, p, p_i, p_f = workload_params()
+    C, N = int(p_i[5]), int(p_i[6])
+    field = workload_field_device(p_i, p_f, dev)
+    cal = load_calibration()
+
+    eng = Engine(local)
+    iid = eng.add("omega", (p_i, p_f), field, None, precision="fp32")
+    stream = torch.cuda.ExternalStream(eng.stream, device=dev)
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    eng.step(warmup)
+    clocks = ClockSampler(local)
+    time.sleep(0.3)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.mark_start()
+    ev0.record(stream)
+    eng.step(K)
+    ev1.record(stream)
+    ev1.synchronize()
+    clocks.mark_end()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    if pg is not None:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / K
+    steps_per_s = 1e3 / ms_step
+    launches = eng.launches_per_step * K
+    st = eng.stats(iid)
+
+    # per-launch-kind timing (CUDA events on the engine stream, un-captured launches)
+    stages = eng.time_stages(max(5, min(50, K)))
+    dom = max(("stage1", "stage2", "stage3", "stage4"), key=lambda k: stages[k])
+    alg_bytes = STAGE_PASSES[dom] * C * 4 * N
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (stages[dom] * 1e-3) / 1e9
+    step_bytes = 16 * C * 4 * N
+    traffic = load_traffic(dom)
+
+    # plain FP64 drop-in path (reference layout, sky_arrested_newton_step) on the same field
+    sim = Simulation(p, th)
+    sim.Field.copy_(field)
+    sim.Velocity.zero_()
+    e = sim.observables()["energy"]
+    for _ in range(3):
+        e, _ = sim.step(e)
+    nplain = max(5, min(50, K))
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    cur = torch.cuda.current_stream()
+    t0.record(cur)
+    for _ in range(nplain):
+        e, _ = sim.step(e)
+    t1.record(cur)
+    t1.synchronize()
+    plain_ms = t0.elapsed_time(t1) / nplain
+    del sim
+
+    # engine in FP64 (for the FP64 polishing phase and the calibration)
+    e64 = Engine(local)
+    i64 = e64.add("omega", (p_i, p_f), field, None, precision="fp64")
+    e64.step(3)
+    s64t = torch.cuda.ExternalStream(e64.stream, device=dev)
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(s64t)
+    e64.step(max(8, min(64, K)))
+    a1.record(s64t)
+    a1.synchronize()
+    eng64_ms = a0.elapsed_time(a1) / max(8, min(64, K))
+    e64.close()
+
+    # end to end through the public API: pinned host field in, per-step (E, B, err) out, field out
+    host = torch.empty(C * N, dtype=torch.float64, pin_memory=True)
+    host.copy_(field)
+    host_np = host.numpy().reshape((C, L, L, L))
+    out_np = np.empty_like(host_np)
+    barrier()
+    tw0 = time.perf_counter()
+    ee = Engine(local)
+    j = ee.add("omega", (p_i, p_f), host_np, None, precision="fp32")
+    for _ in range(K):
+        ee.step(1)
+        ee.stats(j)
+    ee._call("sky_engine_read", j, __import__("ctypes").c_void_p(out_np.ctypes.data), None, 0)
+    tw1 = time.perf_counter()
+    ee.close()
+    e2e_s = tw1 - tw0
+    if pg is not None:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    field_bytes = C * N * 8
+    s32 = cal["fp32_steps_to_converge"] if cal else None
+    s64 = cal["fp64_steps_to_converge"] if cal else None
+
+    def solves(sps, s):
+        return world * sps / s if s else None
+
+    value = solves(steps_per_s, s32)
+    e2e_value = solves(K / e2e_s, s32)
+    plain_value = solves(1e3 / plain_ms, s64)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "theory": "omega (C=5)", "sites": N, "instances_per_gpu": 1,
+                   "precision": "fp32 state and stencils, fp64 compensated energy/baryon/arrest",
+                   "dt": DT_FACTOR * H, "couplings": COUPLINGS,
+                   "steps_to_converge": s32, "convergence": f"energy within {REL_ENERGY_TOL:g} rel. of the "
+                   f"plain-FP64 energy at max|g| <= {GRAD_TOL:g} (profiles/convergence_omega_B4_128.json)",
+                   "l2": f"no flush: resident state {7 * C * N * 4 / 1e6:.0f} MB > 126 MB L2",
+                   "parallelism": f"replicas x{world}"},
+        "site_steps_per_s": world * N * steps_per_s,
+        "hbm_gbs_step": step_bytes / (ms_step * 1e-3) / 1e9,
+        "roofline": {"bound": "hbm", "kernel": f"k_engine_stage<Omega,float,{dom[-1]}>", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                     "launch_ms": stages[dom], "stage_ms": stages},
+        "plain_fp64": {"ms_per_step": plain_ms, "solves_per_s": plain_value, "steps_to_converge": s64,
+                       "engine_fp64_ms_per_step": eng64_ms,
+                       "speedup": (value / plain_value) if (value and plain_value) else None},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": field_bytes / K,
+                "d2h_bytes_per_step": (48 * K + field_bytes) / K, "ms_per_step": e2e_s * 1e3 / K,
+                "path": "Engine.add(pinned host field) + K x (Engine.step(1) + Engine.stats) + field read"},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "final": {"energy": st.energy, "baryon": st.baryon, "max_abs_gradient": st.gabs, "step": st.step},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb = cpu_baseline()
+        cval = cb["site_steps_per_s"] / N / s64 if s64 else None
+        line["cpu_baseline"] = {"value": cval, "unit": UNIT, "cores": cb["cores"], "kind": "port",
+                                "sample": cb["sample"], "site_steps_per_s": cb["site_steps_per_s"]}
+    eng.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0:
+        emit(line)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# calibration: steps to converge, FP64 and FP32 engines
+# ---------------------------------------------------------------------------
+
+def run_calibrate(args):
+    import numpy as np
+    import torch
+    from skyrmion_solver_b200.engine import Engine
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    th, p, p_i, p_f = workload_params()
+    field = workload_field_device(p_i, p_f, dev)
+    chunk = 200
+    res = {"workload": WORKLOAD, "chunk": chunk, "grad_tol": GRAD_TOL, "rel_energy_tol": REL_ENERGY_TOL}
+    hist = {}
+    for prec, cap in (("fp64", args.max_steps), ("fp32", None)):
+        eng = Engine(0)
+        iid = eng.add("omega", (p_i, p_f), field, None, precision=prec)
+        limit = cap if cap else int(1.5 * res["fp64_total_steps"]) + 4 * chunk
+        h = [(0, eng.stats(iid).energy, float("inf"))]
+        t0 = time.perf_counter()
+        n = 0
+        while n < limit:
+            eng.step(chunk)
+            n += chunk
+            st = eng.stats(iid)
+            h.append((n, st.energy, st.gabs))
+            if not math.isfinite(st.energy):
+                break
+            if prec == "fp64" and st.gabs <= GRAD_TOL:
+                break
+        secs = time.perf_counter() - t0
+        eng.close()
+        hist[prec] = h
+        res[f"{prec}_total_steps"] = n
+        res[f"{prec}_seconds"] = secs
+        res[f"{prec}_final_energy"] = h[-1][1]
+        res[f"{prec}_final_max_abs_gradient"] = h[-1][2]
+        print(json.dumps({"phase": prec, "steps": n, "secs": secs, "E": h[-1][1], "gabs": h[-1][2]}), flush=True)
+    e_star = res["fp64_final_energy"]
+    res["reference_energy"] = e_star
+
+    def settle(h):
+        """First recorded step after which |E - E*| <= tol |E*| holds to the end of the run."""
+        s = None
+        for n, e, _ in h:
+            if abs(e - e_star) <= REL_ENERGY_TOL * abs(e_star):
+                if s is None:
+                    s = n
+            else:
+                s = None
+        return s
+
+    res["fp64_steps_to_converge"] = settle(hist["fp64"])
+    res["fp32_steps_to_converge"] = settle(hist["fp32"])
+    res["fp32_final_rel_energy_error"] = abs(res["fp32_final_energy"] - e_star) / abs(e_star)
+    res["fp64_reached_grad_tol"] = res["fp64_final_max_abs_gradient"] <= GRAD_TOL
+    res["history_every"] = chunk * 10
+    res["fp64_history"] = hist["fp64"][::10]
+    res["fp32_history"] = hist["fp32"][::10]
+    res["command"] = "python bench.py --calibrate"
+    os.makedirs(os.path.dirname(CALIBRATION), exist_ok=True)
+    out = args.out or CALIBRATION
+    with open(out, "w") as fh:
+        json.dump(res, fh, indent=1)
+    print(json.dumps({k: v for k, v in res.items() if "history" not in k}), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--calibrate", action="store_true")
+    ap.add_argument("--max-steps", type=int, default=240000)
+    ap.add_argument("--out", default=None)
+    args = ap.parse_args()
+    if args.calibrate:
+        return run_calibrate(args)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

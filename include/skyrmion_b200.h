@@ -130,6 +130,67 @@ int sky_arrested_newton_step(int theory, const int32_t* p_i, int32_t n_pi, const
                              double* scratch, int64_t n_scratch, double prev_energy, double* new_energy_host,
                              double* err_host, void* stream);
 
+/* ------------------------------------------------------------------------ *
+ * Resident batched engine.  No reference counterpart as a single call: it
+ * runs the arrested-Newton step of core/integrator.py:284-410 (driven in the
+ * reference by Simulation.step, core/simulation.py:287-308) for many
+ * instances at once, entirely on the device, with fused RK4 stages, FP64
+ * compensated energy / baryon reductions, a device-side arrest decision and
+ * CUDA-graph replay.  The engine owns its device memory.
+ * ------------------------------------------------------------------------ */
+
+/* Create / destroy an engine bound to CUDA device `device`. */
+int sky_engine_create(int device, void** engine_out);
+int sky_engine_destroy(void* engine);
+
+/* Admit one instance.  precision: 0 = FP32 state and stage arithmetic,
+ * 1 = FP64.  field / velocity are FP64 in the reference layout (host pointers,
+ * or device pointers when on_device != 0); velocity may be NULL (zero).  The
+ * energy of the admitted field is evaluated immediately (stats record 0). */
+int sky_engine_add(void* engine, int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                   int precision, const double* field, const double* velocity, int on_device, int* id_out);
+
+/* Retire an instance and free its memory. */
+int sky_engine_remove(void* engine, int id);
+
+/* Change an instance's precision in place (FP32 -> FP64 for the polishing
+ * phase); the field, velocity, step count and pending arrest decision carry over. */
+int sky_engine_set_precision(void* engine, int id, int precision);
+
+/* Pause (0) or resume (1) an instance. */
+int sky_engine_set_active(void* engine, int id, int active);
+
+/* Advance every active instance by nsteps arrested-Newton steps (asynchronous). */
+int sky_engine_step(void* engine, int nsteps);
+int sky_engine_synchronize(void* engine);
+void* sky_engine_stream(void* engine);
+
+/* Statistics after `step` steps of instance id (step < 0: the latest):
+ * out6 = [energy, baryon, err (signed max of the step's stage-4 gradient),
+ *         max|gradient|, arrested (velocity zeroed for the next step), step]. */
+int sky_engine_stats(void* engine, int id, int64_t step, double* out6);
+
+/* Latest statistics of up to `cap` instances: ids_out[k] and out7[7k..7k+6] =
+ * [energy, baryon, err, max|g|, arrested, step, precision]; returns the count
+ * through *count_out. */
+int sky_engine_stats_all(void* engine, int* ids_out, double* out7, int cap, int* count_out);
+
+/* Copy an instance's field and velocity out as FP64 in the reference layout
+ * (host pointers, or device pointers when on_device != 0); either may be NULL.
+ * The velocity reads as zero when the last step arrested it, as in the reference. */
+int sky_engine_read(void* engine, int id, double* field, double* velocity, int on_device);
+
+/* Run nsteps steps without graph capture, timing each launch kind with CUDA
+ * events on the engine stream; ms_out[6] = average milliseconds per step spent
+ * in [stage 1, stage 2, stage 3, stage 4 + update, control, advance]. */
+int sky_engine_time_stages(void* engine, int nsteps, double* ms_out);
+
+/* Kernel launches one step issues (6 per non-empty (theory, precision) group). */
+int sky_engine_launches_per_step(void* engine);
+
+int sky_engine_count(void* engine);
+int64_t sky_engine_bytes(void* engine);
+
 #ifdef __cplusplus
 }
 #endif

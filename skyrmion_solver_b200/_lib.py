@@ -69,6 +69,22 @@ SIGNATURES = {
     "sky_total_baryon": ([_I, _I32P, _I32, _F64P, _I32, _P, _P, _I64, _F64P, _P], _I),
     "sky_arrested_newton_step": ([_I, _I32P, _I32, _F64P, _I32] + [_P] * 12 + [_P, _I64, _D, _F64P, _F64P, _P],
                                  _I),
+    "sky_engine_create": ([_I, ctypes.POINTER(ctypes.c_void_p)], _I),
+    "sky_engine_destroy": ([_P], _I),
+    "sky_engine_add": ([_P, _I, _I32P, _I32, _F64P, _I32, _I, _P, _P, _I, ctypes.POINTER(_I)], _I),
+    "sky_engine_remove": ([_P, _I], _I),
+    "sky_engine_set_precision": ([_P, _I, _I], _I),
+    "sky_engine_set_active": ([_P, _I, _I], _I),
+    "sky_engine_step": ([_P, _I], _I),
+    "sky_engine_synchronize": ([_P], _I),
+    "sky_engine_stream": ([_P], _P),
+    "sky_engine_stats": ([_P, _I, _I64, _F64P], _I),
+    "sky_engine_stats_all": ([_P, ctypes.POINTER(_I), _F64P, _I, ctypes.POINTER(_I)], _I),
+    "sky_engine_read": ([_P, _I, _P, _P, _I], _I),
+    "sky_engine_time_stages": ([_P, _I, _F64P], _I),
+    "sky_engine_launches_per_step": ([_P], _I),
+    "sky_engine_count": ([_P], _I),
+    "sky_engine_bytes": ([_P], _I64),
 }
 
 _lib = None

@@ -1,0 +1,857 @@
+// Resident batched engine (host side): owns device memory for a set of lattice
+// instances, groups them by (theory, precision), launches the fused stage
+// kernels of sky_engine.cuh over every instance of a group at once and replays
+// the per-step launch sequence from CUDA graphs.
+#include <stdio.h>
+#include <string.h>
+
+#include <map>
+#include <vector>
+
+#include "sky_engine.cuh"
+#include "sky_host.h"
+
+namespace sky {
+
+constexpr int kStatsCap = 8192;
+constexpr int kGraphSteps = 8;  // steps captured per graph replay
+
+struct HostInst {
+    int id = -1;
+    int theory = 0;
+    int prec = 0;  // 0 = FP32 storage/arithmetic, 1 = FP64
+    Params p{};
+    int64_t N = 0;
+    int C = 0;
+    void* F[2] = {nullptr, nullptr};
+    void* V[2] = {nullptr, nullptr};
+    void* L[3] = {nullptr, nullptr, nullptr};
+    KSum* epart = nullptr;
+    KSum* bpart = nullptr;
+    double* gpart = nullptr;
+    StepStats* stats = nullptr;
+    int ntiles = 0, tnz = 0, tny = 0, tnx = 0;
+    int group_slot = -1;
+    int64_t steps = 0;  // host mirror of the device step counter
+    bool active = true;
+    size_t bytes = 0;
+};
+
+struct Group {
+    int theory = 0, prec = 0;
+    std::vector<int> members;  // instance ids in slot order
+    void* d_desc = nullptr;    // InstDesc<S>[cap]
+    int* d_tile_inst = nullptr;
+    int desc_cap = 0, tile_cap = 0;
+    int ntiles = 0;
+};
+
+struct Engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::map<int, HostInst> insts;
+    int next_id = 0;
+    Group groups[6][2];
+    cudaGraphExec_t graph = nullptr;
+    bool graph_valid = false;
+    int64_t bytes = 0;
+};
+
+// ---------------------------------------------------------------------------
+// shapes and launches per (theory, precision)
+// ---------------------------------------------------------------------------
+template <template <typename> class Th, typename T>
+using EShape = typename GradTile<Th<T>::C, T>::type;
+
+// One-time kernel attribute setup (kept out of stream capture); returns the
+// number of resident blocks per SM.
+template <template <typename> class Th, typename T, int STAGE>
+static int stage_setup(int* per_sm_out) {
+    using Shape = EShape<Th, T>;
+    auto kern = k_engine_stage<Th, Shape, T, T, STAGE>;
+    const size_t smem = Shape::template smem_bytes<T>();
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(engine stage)", __LINE__);
+        if (rc) return rc;
+        int n = 0;
+        rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, Shape::NTHREADS, smem),
+                        "occupancy query", __LINE__);
+        if (rc) return rc;
+        per_sm = n < 1 ? 1 : n;
+    }
+    *per_sm_out = per_sm;
+    return SKY_OK;
+}
+
+template <template <typename> class Th, typename T, int STAGE>
+static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
+    using Shape = EShape<Th, T>;
+    auto kern = k_engine_stage<Th, Shape, T, T, STAGE>;
+    const size_t smem = Shape::template smem_bytes<T>();
+    int per_sm = 1;
+    int rc = stage_setup<Th, T, STAGE>(&per_sm);
+    if (rc) return rc;
+    int n = t_end - t_begin;
+    if (n <= 0) return SKY_OK;
+    int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
+    kern<<<blocks, dim3(Shape::BZ, Shape::BY), smem, st>>>(reinterpret_cast<InstDesc<T>*>(g.d_desc), g.d_tile_inst,
+                                                          t_begin, t_end);
+    return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
+}
+
+template <template <typename> class Th, typename T>
+static int launch_stage_any(int stage, const Group& g, int tb, int te, cudaStream_t st) {
+    switch (stage) {
+        case 1: return launch_stage<Th, T, 1>(g, tb, te, st);
+        case 2: return launch_stage<Th, T, 2>(g, tb, te, st);
+        case 3: return launch_stage<Th, T, 3>(g, tb, te, st);
+        default: return launch_stage<Th, T, 4>(g, tb, te, st);
+    }
+}
+
+template <template <typename> class Th>
+static int stage_dispatch_prec(int prec, int stage, const Group& g, int tb, int te, cudaStream_t st) {
+    return prec ? launch_stage_any<Th, double>(stage, g, tb, te, st) : launch_stage_any<Th, float>(stage, g, tb, te, st);
+}
+
+template <template <typename> class Th, typename T>
+static int setup_all() {
+    int n, rc;
+    if ((rc = stage_setup<Th, T, 1>(&n)) || (rc = stage_setup<Th, T, 2>(&n)) || (rc = stage_setup<Th, T, 3>(&n)) ||
+        (rc = stage_setup<Th, T, 4>(&n)))
+        return rc;
+    return SKY_OK;
+}
+
+template <template <typename> class Th>
+static int setup_prec(int prec) {
+    return prec ? setup_all<Th, double>() : setup_all<Th, float>();
+}
+
+static int setup_group(const Group& g) {
+    switch (g.theory) {
+        case SKY_THEORY_NUCLEAR: return setup_prec<Nuclear>(g.prec);
+        case SKY_THEORY_OMEGA: return setup_prec<Omega>(g.prec);
+        case SKY_THEORY_COULOMB: return setup_prec<Coulomb>(g.prec);
+        case SKY_THEORY_RHO: return setup_prec<Rho>(g.prec);
+        case SKY_THEORY_BERGER: return setup_prec<Berger>(g.prec);
+        case SKY_THEORY_LIGHTLY_BOUND: return setup_prec<LightlyBound>(g.prec);
+    }
+    return invalid("unknown theory id");
+}
+
+static int launch_stage_group(int stage, const Group& g, int tb, int te, cudaStream_t st) {
+    switch (g.theory) {
+        case SKY_THEORY_NUCLEAR: return stage_dispatch_prec<Nuclear>(g.prec, stage, g, tb, te, st);
+        case SKY_THEORY_OMEGA: return stage_dispatch_prec<Omega>(g.prec, stage, g, tb, te, st);
+        case SKY_THEORY_COULOMB: return stage_dispatch_prec<Coulomb>(g.prec, stage, g, tb, te, st);
+        case SKY_THEORY_RHO: return stage_dispatch_prec<Rho>(g.prec, stage, g, tb, te, st);
+        case SKY_THEORY_BERGER: return stage_dispatch_prec<Berger>(g.prec, stage, g, tb, te, st);
+        case SKY_THEORY_LIGHTLY_BOUND: return stage_dispatch_prec<LightlyBound>(g.prec, stage, g, tb, te, st);
+    }
+    return invalid("unknown theory id");
+}
+
+template <template <typename> class Th>
+static void shape_of(int prec, int& bz, int& by, int& tx) {
+    if (prec) {
+        using S = EShape<Th, double>;
+        bz = S::BZ, by = S::BY, tx = S::TX;
+    } else {
+        using S = EShape<Th, float>;
+        bz = S::BZ, by = S::BY, tx = S::TX;
+    }
+}
+
+static void tile_shape(int theory, int prec, int& bz, int& by, int& tx) {
+    switch (theory) {
+        case SKY_THEORY_NUCLEAR: shape_of<Nuclear>(prec, bz, by, tx); break;
+        case SKY_THEORY_OMEGA: shape_of<Omega>(prec, bz, by, tx); break;
+        case SKY_THEORY_COULOMB: shape_of<Coulomb>(prec, bz, by, tx); break;
+        case SKY_THEORY_RHO: shape_of<Rho>(prec, bz, by, tx); break;
+        case SKY_THEORY_BERGER: shape_of<Berger>(prec, bz, by, tx); break;
+        default: shape_of<LightlyBound>(prec, bz, by, tx); break;
+    }
+}
+
+static int launch_control(const Group& g, int ib, int ie, int mode, cudaStream_t st) {
+    if (ie <= ib) return SKY_OK;
+    if (g.prec)
+        k_engine_control<double><<<ie - ib, 256, 0, st>>>(reinterpret_cast<InstDesc<double>*>(g.d_desc), ib, ie, mode);
+    else
+        k_engine_control<float><<<ie - ib, 256, 0, st>>>(reinterpret_cast<InstDesc<float>*>(g.d_desc), ib, ie, mode);
+    return check_cuda(cudaGetLastError(), "launch engine control", __LINE__);
+}
+
+static int launch_advance(const Group& g, cudaStream_t st) {
+    const int n = (int)g.members.size();
+    if (n == 0) return SKY_OK;
+    const int b = (n + 127) / 128;
+    if (g.prec)
+        k_engine_advance<double><<<b, 128, 0, st>>>(reinterpret_cast<InstDesc<double>*>(g.d_desc), n);
+    else
+        k_engine_advance<float><<<b, 128, 0, st>>>(reinterpret_cast<InstDesc<float>*>(g.d_desc), n);
+    return check_cuda(cudaGetLastError(), "launch engine advance", __LINE__);
+}
+
+// ---------------------------------------------------------------------------
+// conversion kernels (FP64 reference layout <-> engine storage)
+// ---------------------------------------------------------------------------
+template <typename S>
+__global__ void k_convert_in(int64_t n, const double* __restrict__ src, S* __restrict__ dst) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src ? S(src[i]) : S(0);
+}
+template <typename S>
+__global__ void k_convert_out(int64_t n, const S* __restrict__ src, double* __restrict__ dst, int zero) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = zero ? 0.0 : double(src[i]);
+}
+__global__ void k_f32_to_f64(int64_t n, const float* __restrict__ s, double* __restrict__ d) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = double(s[i]);
+}
+__global__ void k_f64_to_f32(int64_t n, const double* __restrict__ s, float* __restrict__ d) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = float(s[i]);
+}
+
+// ---------------------------------------------------------------------------
+// descriptors
+// ---------------------------------------------------------------------------
+template <typename S>
+static InstDesc<S> make_desc(const HostInst& h, int tile_begin) {
+    InstDesc<S> d;
+    memset(&d, 0, sizeof(d));
+    d.p = h.p;
+    for (int i = 0; i < 2; ++i) {
+        d.F[i] = reinterpret_cast<S*>(h.F[i]);
+        d.V[i] = reinterpret_cast<S*>(h.V[i]);
+    }
+    for (int i = 0; i < 3; ++i) d.L[i] = reinterpret_cast<S*>(h.L[i]);
+    d.epart = h.epart;
+    d.bpart = h.bpart;
+    d.gpart = h.gpart;
+    d.stats = h.stats;
+    d.stats_cap = kStatsCap;
+    d.tile_begin = tile_begin;
+    d.ntiles = h.ntiles;
+    d.tiles_nz = h.tnz;
+    d.tiles_ny = h.tny;
+    d.tiles_nx = h.tnx;
+    d.active = h.active ? 1 : 0;
+    return d;
+}
+
+// Rebuild a group's device descriptor array and tile list.  Device-updated
+// control fields (e_prev, step, arrested, cur) of existing members are kept.
+template <typename S>
+static int rebuild_group_t(Engine& e, Group& g) {
+    // gather current device state of the members (they may move slots)
+    std::vector<InstDesc<S>> dev_old;
+    if (g.d_desc && g.desc_cap > 0) {
+        dev_old.resize(g.desc_cap);
+        int rc = check_cuda(cudaMemcpyAsync(dev_old.data(), g.d_desc, sizeof(InstDesc<S>) * g.desc_cap,
+                                            cudaMemcpyDeviceToHost, e.stream),
+                            "read descriptors", __LINE__);
+        if (rc) return rc;
+        if ((rc = check_cuda(cudaStreamSynchronize(e.stream), "sync", __LINE__))) return rc;
+    }
+    std::vector<InstDesc<S>> descs;
+    std::vector<int> tile_inst;
+    int tb = 0;
+    for (size_t k = 0; k < g.members.size(); ++k) {
+        HostInst& h = e.insts[g.members[k]];
+        InstDesc<S> d = make_desc<S>(h, tb);
+        if (h.group_slot >= 0 && h.group_slot < (int)dev_old.size()) {
+            const InstDesc<S>& o = dev_old[h.group_slot];
+            d.e_prev = o.e_prev;
+            d.step = o.step;
+            d.arrested = o.arrested;
+            d.cur = o.cur;
+        }
+        h.group_slot = (int)k;
+        descs.push_back(d);
+        for (int t = 0; t < h.ntiles; ++t) tile_inst.push_back((int)k);
+        tb += h.ntiles;
+    }
+    g.ntiles = tb;
+    if ((int)descs.size() > g.desc_cap) {
+        if (g.d_desc) cudaFree(g.d_desc);
+        g.desc_cap = (int)descs.size() * 2 + 4;
+        int rc = check_cuda(cudaMalloc(&g.d_desc, sizeof(InstDesc<S>) * g.desc_cap), "cudaMalloc(desc)", __LINE__);
+        if (rc) return rc;
+        cudaMemsetAsync(g.d_desc, 0, sizeof(InstDesc<S>) * g.desc_cap, e.stream);
+    }
+    if ((int)tile_inst.size() > g.tile_cap) {
+        if (g.d_tile_inst) cudaFree(g.d_tile_inst);
+        g.tile_cap = (int)tile_inst.size() * 2 + 64;
+        int rc = check_cuda(cudaMalloc(&g.d_tile_inst, sizeof(int) * g.tile_cap), "cudaMalloc(tiles)", __LINE__);
+        if (rc) return rc;
+    }
+    if (!descs.empty()) {
+        int rc = check_cuda(cudaMemcpyAsync(g.d_desc, descs.data(), sizeof(InstDesc<S>) * descs.size(),
+                                            cudaMemcpyHostToDevice, e.stream),
+                            "write descriptors", __LINE__);
+        if (rc) return rc;
+        rc = check_cuda(cudaMemcpyAsync(g.d_tile_inst, tile_inst.data(), sizeof(int) * tile_inst.size(),
+                                        cudaMemcpyHostToDevice, e.stream),
+                        "write tile list", __LINE__);
+        if (rc) return rc;
+    }
+    e.graph_valid = false;
+    return check_cuda(cudaStreamSynchronize(e.stream), "sync", __LINE__);
+}
+
+static int rebuild_group(Engine& e, Group& g) {
+    return g.prec ? rebuild_group_t<double>(e, g) : rebuild_group_t<float>(e, g);
+}
+
+static void free_inst(HostInst& h) {
+    void* ptrs[] = {h.F[0], h.F[1], h.V[0], h.V[1], h.L[0], h.L[1], h.L[2], h.epart, h.bpart, h.gpart, h.stats};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    memset(h.F, 0, sizeof(h.F));
+    memset(h.V, 0, sizeof(h.V));
+    memset(h.L, 0, sizeof(h.L));
+    h.epart = h.bpart = nullptr;
+    h.gpart = nullptr;
+    h.stats = nullptr;
+}
+
+static int alloc_inst(Engine& e, HostInst& h) {
+    const size_t es = h.prec ? sizeof(double) : sizeof(float);
+    const size_t fb = es * (size_t)h.C * (size_t)h.N;
+    int bz, by, tx;
+    tile_shape(h.theory, h.prec, bz, by, tx);
+    h.tnz = (h.p.Z + bz - 1) / bz;
+    h.tny = (h.p.Y + by - 1) / by;
+    h.tnx = (h.p.X + tx - 1) / tx;
+    h.ntiles = h.tnz * h.tny * h.tnx;
+    void** bufs[] = {&h.F[0], &h.F[1], &h.V[0], &h.V[1], &h.L[0], &h.L[1], &h.L[2]};
+    for (void** b : bufs) {
+        if (cudaMalloc(b, fb) != cudaSuccess) {
+            cudaGetLastError();
+            free_inst(h);
+            return SKY_ERR_NOMEM;
+        }
+    }
+    if (cudaMalloc(&h.epart, sizeof(KSum) * h.ntiles) != cudaSuccess ||
+        cudaMalloc(&h.bpart, sizeof(KSum) * h.ntiles) != cudaSuccess ||
+        cudaMalloc(&h.gpart, sizeof(double) * 2 * h.ntiles) != cudaSuccess ||
+        cudaMalloc(&h.stats, sizeof(StepStats) * kStatsCap) != cudaSuccess) {
+        cudaGetLastError();
+        free_inst(h);
+        return SKY_ERR_NOMEM;
+    }
+    cudaMemsetAsync(h.gpart, 0, sizeof(double) * 2 * h.ntiles, e.stream);
+    cudaMemsetAsync(h.stats, 0, sizeof(StepStats) * kStatsCap, e.stream);
+    h.bytes = 7 * fb + (sizeof(KSum) * 2 + sizeof(double) * 2) * h.ntiles + sizeof(StepStats) * kStatsCap;
+    return SKY_OK;
+}
+
+static int upload(Engine& e, HostInst& h, const double* field, const double* velocity, bool on_device) {
+    const int64_t n = (int64_t)h.C * h.N;
+    double* tmp = nullptr;
+    int rc = SKY_OK;
+    const double* srcs[2] = {field, velocity};
+    void* dsts[2] = {h.F[0], h.V[0]};
+    for (int k = 0; k < 2; ++k) {
+        const double* src = srcs[k];
+        if (src && !on_device) {
+            if (!tmp && (rc = check_cuda(cudaMalloc(&tmp, sizeof(double) * n), "cudaMalloc(upload)", __LINE__)))
+                return rc;
+            if ((rc = check_cuda(cudaMemcpyAsync(tmp, src, sizeof(double) * n, cudaMemcpyHostToDevice, e.stream),
+                                 "upload", __LINE__)))
+                break;
+            src = tmp;
+        }
+        if (h.prec)
+            k_convert_in<double><<<ew_blocks(n), 256, 0, e.stream>>>(n, src, reinterpret_cast<double*>(dsts[k]));
+        else
+            k_convert_in<float><<<ew_blocks(n), 256, 0, e.stream>>>(n, src, reinterpret_cast<float*>(dsts[k]));
+        if ((rc = check_cuda(cudaGetLastError(), "convert", __LINE__))) break;
+        if (tmp) cudaStreamSynchronize(e.stream);
+    }
+    if (tmp) {
+        cudaStreamSynchronize(e.stream);
+        cudaFree(tmp);
+    }
+    return rc;
+}
+
+// Stage 1 + control for one instance (admission or precision change).
+static int init_instance(Engine& e, HostInst& h, int mode) {
+    Group& g = e.groups[h.theory][h.prec];
+    int tb = 0;
+    for (int id : g.members) {
+        if (id == h.id) break;
+        tb += e.insts[id].ntiles;
+    }
+    int rc = launch_stage_group(1, g, tb, tb + h.ntiles, e.stream);
+    if (rc) return rc;
+    rc = launch_control(g, h.group_slot, h.group_slot + 1, mode, e.stream);
+    if (rc) return rc;
+    return check_cuda(cudaStreamSynchronize(e.stream), "sync", __LINE__);
+}
+
+// Launch kinds of one step, in order: stage 2, 3, 4 (+ update), advance,
+// stage 1 (on the updated field), control.  Groups are independent, so each
+// kind is issued for every non-empty group before the next kind.
+enum { kKindS2 = 0, kKindS3, kKindS4, kKindAdvance, kKindS1, kKindControl, kNumKinds };
+
+static int launch_kind(Engine& e, int kind) {
+    for (int t = 0; t < 6; ++t)
+        for (int pr = 0; pr < 2; ++pr) {
+            Group& g = e.groups[t][pr];
+            if (g.members.empty()) continue;
+            int rc = SKY_OK;
+            switch (kind) {
+                case kKindS2: rc = launch_stage_group(2, g, 0, g.ntiles, e.stream); break;
+                case kKindS3: rc = launch_stage_group(3, g, 0, g.ntiles, e.stream); break;
+                case kKindS4: rc = launch_stage_group(4, g, 0, g.ntiles, e.stream); break;
+                case kKindAdvance: rc = launch_advance(g, e.stream); break;
+                case kKindS1: rc = launch_stage_group(1, g, 0, g.ntiles, e.stream); break;
+                default: rc = launch_control(g, 0, (int)g.members.size(), 0, e.stream); break;
+            }
+            if (rc) return rc;
+        }
+    return SKY_OK;
+}
+
+static int record_step(Engine& e) {
+    for (int k = 0; k < kNumKinds; ++k) {
+        int rc = launch_kind(e, k);
+        if (rc) return rc;
+    }
+    return SKY_OK;
+}
+
+static int count_launches(Engine& e) {
+    int n = 0;
+    for (int t = 0; t < 6; ++t)
+        for (int pr = 0; pr < 2; ++pr)
+            if (!e.groups[t][pr].members.empty()) n += kNumKinds;
+    return n;
+}
+
+static int build_graph(Engine& e) {
+    if (e.graph) {
+        cudaGraphExecDestroy(e.graph);
+        e.graph = nullptr;
+    }
+    int rc = SKY_OK;
+    for (int t = 0; t < 6; ++t)
+        for (int pr = 0; pr < 2; ++pr)
+            if (!e.groups[t][pr].members.empty() && (rc = setup_group(e.groups[t][pr]))) return rc;
+    cudaGraph_t graph;
+    rc = check_cuda(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal), "begin capture", __LINE__);
+    if (rc) return rc;
+    for (int s = 0; s < kGraphSteps && rc == SKY_OK; ++s) rc = record_step(e);
+    cudaError_t ce = cudaStreamEndCapture(e.stream, &graph);
+    if (rc) {
+        if (ce == cudaSuccess) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if ((rc = check_cuda(ce, "end capture", __LINE__))) return rc;
+    rc = check_cuda(cudaGraphInstantiate(&e.graph, graph, 0), "graph instantiate", __LINE__);
+    cudaGraphDestroy(graph);
+    if (rc) return rc;
+    e.graph_valid = true;
+    return SKY_OK;
+}
+
+static HostInst* find(Engine* e, int id) {
+    auto it = e->insts.find(id);
+    return it == e->insts.end() ? nullptr : &it->second;
+}
+
+static int remove_from_group(Engine& e, HostInst& h) {
+    Group& g = e.groups[h.theory][h.prec];
+    // the remaining members still carry their old slots, from which the
+    // rebuild gathers their device control state
+    std::vector<int> keep;
+    for (int id : g.members)
+        if (id != h.id) keep.push_back(id);
+    g.members = keep;
+    const int rc = rebuild_group(e, g);
+    h.group_slot = -1;
+    return rc;
+}
+
+}  // namespace sky
+
+using namespace sky;
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int sky_engine_create(int device, void** out) {
+    if (!out) return invalid("null output");
+    Engine* e = new Engine();
+    e->device = device;
+    int rc = check_cuda(cudaSetDevice(device), "cudaSetDevice", __LINE__);
+    if (!rc) rc = check_cuda(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "stream", __LINE__);
+    if (rc) {
+        delete e;
+        return rc;
+    }
+    for (int t = 0; t < 6; ++t)
+        for (int p = 0; p < 2; ++p) {
+            e->groups[t][p].theory = t;
+            e->groups[t][p].prec = p;
+        }
+    *out = e;
+    return SKY_OK;
+}
+
+int sky_engine_destroy(void* handle) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return SKY_OK;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    for (auto& kv : e->insts) free_inst(kv.second);
+    for (int t = 0; t < 6; ++t)
+        for (int p = 0; p < 2; ++p) {
+            if (e->groups[t][p].d_desc) cudaFree(e->groups[t][p].d_desc);
+            if (e->groups[t][p].d_tile_inst) cudaFree(e->groups[t][p].d_tile_inst);
+        }
+    cudaStreamDestroy(e->stream);
+    delete e;
+    return SKY_OK;
+}
+
+int sky_engine_add(void* handle, int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                   int precision, const double* field, const double* velocity, int on_device, int* id_out) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e || !id_out || !field) return invalid("null argument");
+    if (precision != 0 && precision != 1) return invalid("precision must be 0 (FP32) or 1 (FP64)");
+    cudaSetDevice(e->device);
+    HostInst h;
+    int rc = pack_params(theory, p_i, n_pi, p_f, n_pf, &h.p);
+    if (rc) return rc;
+    h.id = e->next_id++;
+    h.theory = theory;
+    h.prec = precision;
+    h.N = n_sites(h.p);
+    h.C = h.p.C;
+    if ((rc = alloc_inst(*e, h))) return rc;
+    if ((rc = upload(*e, h, field, velocity, on_device != 0))) {
+        free_inst(h);
+        return rc;
+    }
+    e->insts[h.id] = h;
+    Group& g = e->groups[theory][precision];
+    g.members.push_back(h.id);
+    if ((rc = rebuild_group(*e, g)) || (rc = init_instance(*e, e->insts[h.id], 1))) {
+        g.members.pop_back();
+        free_inst(e->insts[h.id]);
+        e->insts.erase(h.id);
+        rebuild_group(*e, g);
+        return rc;
+    }
+    e->bytes += (int64_t)h.bytes;
+    *id_out = h.id;
+    return SKY_OK;
+}
+
+int sky_engine_remove(void* handle, int id) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return invalid("null engine");
+    HostInst* h = find(e, id);
+    if (!h) return invalid("unknown instance id");
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    int rc = remove_from_group(*e, *h);
+    e->bytes -= (int64_t)h->bytes;
+    free_inst(*h);
+    e->insts.erase(id);
+    return rc;
+}
+
+int sky_engine_set_precision(void* handle, int id, int precision) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return invalid("null engine");
+    HostInst* hp = find(e, id);
+    if (!hp) return invalid("unknown instance id");
+    if (precision != 0 && precision != 1) return invalid("precision must be 0 or 1");
+    if (hp->prec == precision) return SKY_OK;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    HostInst& h = *hp;
+    // read the control state of the instance
+    int cur = 0, arrested = 0, step = 0;
+    double e_prev = 0.0;
+    {
+        Group& g = e->groups[h.theory][h.prec];
+        if (h.prec) {
+            InstDesc<double> d;
+            cudaMemcpy(&d, reinterpret_cast<InstDesc<double>*>(g.d_desc) + h.group_slot, sizeof(d),
+                       cudaMemcpyDeviceToHost);
+            cur = d.cur, arrested = d.arrested, step = d.step, e_prev = d.e_prev;
+        } else {
+            InstDesc<float> d;
+            cudaMemcpy(&d, reinterpret_cast<InstDesc<float>*>(g.d_desc) + h.group_slot, sizeof(d),
+                       cudaMemcpyDeviceToHost);
+            cur = d.cur, arrested = d.arrested, step = d.step, e_prev = d.e_prev;
+        }
+    }
+    HostInst nh = h;
+    nh.prec = precision;
+    nh.group_slot = -1;
+    for (int i = 0; i < 2; ++i) nh.F[i] = nh.V[i] = nullptr;
+    for (int i = 0; i < 3; ++i) nh.L[i] = nullptr;
+    nh.epart = nh.bpart = nullptr;
+    nh.gpart = nullptr;
+    nh.stats = nullptr;
+    int rc = alloc_inst(*e, nh);
+    if (rc) return rc;
+    const int64_t n = (int64_t)h.C * h.N;
+    const void* srcs[2] = {h.F[cur], h.V[cur]};
+    void* dsts[2] = {nh.F[0], nh.V[0]};
+    for (int k = 0; k < 2; ++k) {
+        if (precision)
+            k_f32_to_f64<<<ew_blocks(n), 256, 0, e->stream>>>(n, (const float*)srcs[k], (double*)dsts[k]);
+        else
+            k_f64_to_f32<<<ew_blocks(n), 256, 0, e->stream>>>(n, (const double*)srcs[k], (float*)dsts[k]);
+    }
+    // carry the stats history
+    cudaMemcpyAsync(nh.stats, h.stats, sizeof(StepStats) * kStatsCap, cudaMemcpyDeviceToDevice, e->stream);
+    if ((rc = check_cuda(cudaStreamSynchronize(e->stream), "convert", __LINE__))) {
+        free_inst(nh);
+        return rc;
+    }
+    // leave the old group
+    if ((rc = remove_from_group(*e, h))) {
+        free_inst(nh);
+        return rc;
+    }
+    free_inst(h);
+    e->bytes += (int64_t)nh.bytes - (int64_t)h.bytes;
+    h = nh;
+    Group& g2 = e->groups[h.theory][h.prec];
+    g2.members.push_back(h.id);
+    if ((rc = rebuild_group(*e, g2))) return rc;
+    // restore the control state, then recompute l1 / energy of the converted field
+    if (h.prec) {
+        InstDesc<double>* dd = reinterpret_cast<InstDesc<double>*>(g2.d_desc) + h.group_slot;
+        cudaMemcpyAsync(&dd->step, &step, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+        cudaMemcpyAsync(&dd->arrested, &arrested, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+        cudaMemcpyAsync(&dd->e_prev, &e_prev, sizeof(double), cudaMemcpyHostToDevice, e->stream);
+    } else {
+        InstDesc<float>* dd = reinterpret_cast<InstDesc<float>*>(g2.d_desc) + h.group_slot;
+        cudaMemcpyAsync(&dd->step, &step, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+        cudaMemcpyAsync(&dd->arrested, &arrested, sizeof(int), cudaMemcpyHostToDevice, e->stream);
+        cudaMemcpyAsync(&dd->e_prev, &e_prev, sizeof(double), cudaMemcpyHostToDevice, e->stream);
+    }
+    return init_instance(*e, h, 2);
+}
+
+int sky_engine_set_active(void* handle, int id, int active) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return invalid("null engine");
+    HostInst* h = find(e, id);
+    if (!h) return invalid("unknown instance id");
+    h->active = active != 0;
+    Group& g = e->groups[h->theory][h->prec];
+    const int a = h->active ? 1 : 0;
+    size_t off = h->prec ? offsetof(InstDesc<double>, active) : offsetof(InstDesc<float>, active);
+    size_t sz = h->prec ? sizeof(InstDesc<double>) : sizeof(InstDesc<float>);
+    char* base = reinterpret_cast<char*>(g.d_desc) + sz * h->group_slot + off;
+    int rc = check_cuda(cudaMemcpyAsync(base, &a, sizeof(int), cudaMemcpyHostToDevice, e->stream), "set active",
+                        __LINE__);
+    if (rc) return rc;
+    return check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__);
+}
+
+int sky_engine_step(void* handle, int nsteps) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return invalid("null engine");
+    if (nsteps < 0) return invalid("nsteps must be >= 0");
+    cudaSetDevice(e->device);
+    int rc;
+    int done = 0;
+    if (nsteps >= kGraphSteps) {
+        if (!e->graph_valid && (rc = build_graph(*e))) return rc;
+        while (nsteps - done >= kGraphSteps) {
+            if ((rc = check_cuda(cudaGraphLaunch(e->graph, e->stream), "graph launch", __LINE__))) return rc;
+            done += kGraphSteps;
+        }
+    }
+    for (; done < nsteps; ++done)
+        if ((rc = record_step(*e))) return rc;
+    for (auto& kv : e->insts)
+        if (kv.second.active) kv.second.steps += nsteps;
+    return SKY_OK;
+}
+
+int sky_engine_synchronize(void* handle) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return invalid("null engine");
+    return check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__);
+}
+
+void* sky_engine_stream(void* handle) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    return e ? (void*)e->stream : nullptr;
+}
+
+int sky_engine_stats(void* handle, int id, int64_t step, double* out6) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e || !out6) return invalid("null argument");
+    HostInst* h = find(e, id);
+    if (!h) return invalid("unknown instance id");
+    if (step < 0) step = h->steps;
+    if (step > h->steps || h->steps - step >= kStatsCap) return invalid("step outside the retained history");
+    StepStats st;
+    int rc = check_cuda(cudaMemcpyAsync(&st, h->stats + (step % kStatsCap), sizeof(st), cudaMemcpyDeviceToHost,
+                                        e->stream),
+                        "read stats", __LINE__);
+    if (rc) return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__))) return rc;
+    out6[0] = st.energy;
+    out6[1] = st.baryon;
+    out6[2] = st.err;
+    out6[3] = st.gabs;
+    out6[4] = st.arrested;
+    out6[5] = st.step;
+    return SKY_OK;
+}
+
+int sky_engine_stats_all(void* handle, int* ids_out, double* out7, int cap, int* count_out) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e || !count_out) return invalid("null argument");
+    std::vector<StepStats> st(e->insts.size());
+    std::vector<const HostInst*> hs;
+    int k = 0;
+    for (auto& kv : e->insts) {
+        if (k >= cap) break;
+        const HostInst& h = kv.second;
+        int rc = check_cuda(cudaMemcpyAsync(&st[k], h.stats + (h.steps % kStatsCap), sizeof(StepStats),
+                                            cudaMemcpyDeviceToHost, e->stream),
+                            "read stats", __LINE__);
+        if (rc) return rc;
+        hs.push_back(&h);
+        ++k;
+    }
+    int rc = check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__);
+    if (rc) return rc;
+    for (int i = 0; i < k; ++i) {
+        if (ids_out) ids_out[i] = hs[i]->id;
+        if (out7) {
+            double* o = out7 + 7 * i;
+            o[0] = st[i].energy;
+            o[1] = st[i].baryon;
+            o[2] = st[i].err;
+            o[3] = st[i].gabs;
+            o[4] = st[i].arrested;
+            o[5] = st[i].step;
+            o[6] = hs[i]->prec;
+        }
+    }
+    *count_out = k;
+    return SKY_OK;
+}
+
+int sky_engine_read(void* handle, int id, double* field, double* velocity, int on_device) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return invalid("null engine");
+    HostInst* h = find(e, id);
+    if (!h) return invalid("unknown instance id");
+    cudaSetDevice(e->device);
+    Group& g = e->groups[h->theory][h->prec];
+    int cur = 0, arrested = 0;
+    int rc;
+    size_t sz = h->prec ? sizeof(InstDesc<double>) : sizeof(InstDesc<float>);
+    size_t ocur = h->prec ? offsetof(InstDesc<double>, cur) : offsetof(InstDesc<float>, cur);
+    size_t oarr = h->prec ? offsetof(InstDesc<double>, arrested) : offsetof(InstDesc<float>, arrested);
+    char* base = reinterpret_cast<char*>(g.d_desc) + sz * h->group_slot;
+    cudaMemcpyAsync(&cur, base + ocur, sizeof(int), cudaMemcpyDeviceToHost, e->stream);
+    cudaMemcpyAsync(&arrested, base + oarr, sizeof(int), cudaMemcpyDeviceToHost, e->stream);
+    if ((rc = check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__))) return rc;
+    const int64_t n = (int64_t)h->C * h->N;
+    double* tmp = nullptr;
+    if (!on_device && (rc = check_cuda(cudaMalloc(&tmp, sizeof(double) * n), "cudaMalloc(read)", __LINE__)))
+        return rc;
+    double* outs[2] = {field, velocity};
+    const void* srcs[2] = {h->F[cur], h->V[cur]};
+    for (int k = 0; k < 2 && rc == SKY_OK; ++k) {
+        if (!outs[k]) continue;
+        double* dst = on_device ? outs[k] : tmp;
+        const int zero = (k == 1 && arrested) ? 1 : 0;  // the reference zeroes V on arrest
+        if (h->prec)
+            k_convert_out<double><<<ew_blocks(n), 256, 0, e->stream>>>(n, (const double*)srcs[k], dst, zero);
+        else
+            k_convert_out<float><<<ew_blocks(n), 256, 0, e->stream>>>(n, (const float*)srcs[k], dst, zero);
+        rc = check_cuda(cudaGetLastError(), "convert out", __LINE__);
+        if (!rc && !on_device)
+            rc = check_cuda(cudaMemcpyAsync(outs[k], tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, e->stream),
+                            "download", __LINE__);
+        if (!rc) rc = check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__);
+    }
+    if (tmp) cudaFree(tmp);
+    return rc;
+}
+
+int sky_engine_time_stages(void* handle, int nsteps, double* ms_out) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e || !ms_out) return invalid("null argument");
+    if (nsteps < 1) return invalid("nsteps must be >= 1");
+    cudaSetDevice(e->device);
+    int rc = SKY_OK;
+    for (int t = 0; t < 6; ++t)
+        for (int pr = 0; pr < 2; ++pr)
+            if (!e->groups[t][pr].members.empty() && (rc = setup_group(e->groups[t][pr]))) return rc;
+    cudaEvent_t ev[kNumKinds + 1];
+    for (int k = 0; k <= kNumKinds; ++k)
+        if ((rc = check_cuda(cudaEventCreate(&ev[k]), "cudaEventCreate", __LINE__))) return rc;
+    double acc[kNumKinds] = {0.0};
+    for (int s = 0; s < nsteps && rc == SKY_OK; ++s) {
+        for (int k = 0; k < kNumKinds && rc == SKY_OK; ++k) {
+            cudaEventRecord(ev[k], e->stream);
+            rc = launch_kind(*e, k);
+        }
+        if (rc) break;
+        cudaEventRecord(ev[kNumKinds], e->stream);
+        if ((rc = check_cuda(cudaEventSynchronize(ev[kNumKinds]), "cudaEventSynchronize", __LINE__))) break;
+        for (int k = 0; k < kNumKinds; ++k) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+            acc[k] += ms;
+        }
+    }
+    for (int k = 0; k <= kNumKinds; ++k) cudaEventDestroy(ev[k]);
+    if (rc) return rc;
+    for (auto& kv : e->insts)
+        if (kv.second.active) kv.second.steps += nsteps;
+    // report in the order stage 1, 2, 3, 4, control, advance
+    ms_out[0] = acc[kKindS1] / nsteps;
+    ms_out[1] = acc[kKindS2] / nsteps;
+    ms_out[2] = acc[kKindS3] / nsteps;
+    ms_out[3] = acc[kKindS4] / nsteps;
+    ms_out[4] = acc[kKindControl] / nsteps;
+    ms_out[5] = acc[kKindAdvance] / nsteps;
+    return SKY_OK;
+}
+
+int sky_engine_launches_per_step(void* handle) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    return e ? count_launches(*e) : 0;
+}
+
+int sky_engine_count(void* handle) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    return e ? (int)e->insts.size() : 0;
+}
+
+int64_t sky_engine_bytes(void* handle) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    return e ? e->bytes : 0;
+}
+
+}  // extern "C"

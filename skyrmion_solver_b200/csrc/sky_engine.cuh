@@ -1,0 +1,298 @@
+// Resident engine kernels: the arrested-Newton / RK4 step of
+// core/integrator.py:284-410 as fused stage launches plus a small control
+// launch, for a batch of lattice instances at once.
+//
+// With k1 = dt V, k2 = dt (V + l1/2), k3 = dt (V + l2/2), k4 = dt (V + l3) the
+// stage inputs of the reference schedule are
+//   X1 = F,  X2 = F + (dt/2) V,  X3 = F + (dt/2)(V + l1/2),  X4 = F + dt (V + l2/2)
+// and the update is
+//   V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,   F' = F + dt (V + (l1 + l2 + l3)/6)
+// followed by the theory's normalisation of phi and projection of V'
+// (core/integrator.py:163-175).  Stage s builds X_s for its haloed tile on the
+// fly from F, V and the previous slope and writes only l_s; stage 4 applies the
+// update into the other half of a ping-pong pair.
+//
+// One step is: stage 2, stage 3, stage 4 (+ update), advance, stage 1, control.
+// Stage 1 runs on the freshly updated field, so besides l1 (needed by the next
+// step) it evaluates that field's energy and baryon density in FP64; the
+// control launch reduces them (compensated, fixed order), records the step's
+// (energy, err) exactly as do_arrested_newton_flow returns them, and takes the
+// arrest decision for the next step: the velocity is treated as zero when
+// killkinen is set and the energy rose (core/integrator.py:403-407).
+#pragma once
+
+#include "sky_kernels.cuh"
+
+namespace sky {
+
+// Per-step statistics written by the control launch: record n describes the
+// field after n steps (record 0: the admitted field).
+struct StepStats {
+    double energy;      // E after step n (FP64, compensated)
+    double baryon;      // B after step n
+    double err;         // signed max of step n's stage-4 gradient (reference `err`)
+    double gabs;        // max |g| of step n's stage-4 gradient
+    int arrested;       // velocity treated as zero in step n+1
+    int step;           // n
+    int pad[2];
+};
+
+// Device-resident state of one instance.
+template <typename S>
+struct InstDesc {
+    Params p;
+    S* F[2];           // ping-pong field
+    S* V[2];           // ping-pong velocity
+    S* L[3];           // stage slopes l1, l2, l3
+    KSum* epart;       // per-tile energy partials (stage 1)
+    KSum* bpart;       // per-tile baryon partials (stage 1)
+    double* gpart;     // per-tile [signed max, abs max] of stage-4 g (2 doubles / tile)
+    StepStats* stats;  // ring of per-step records
+    int stats_cap;
+    int tile_begin;    // first global tile index of this instance
+    int ntiles;
+    int tiles_nz, tiles_ny, tiles_nx;
+    // control state (device-updated)
+    double e_prev;     // energy entering the previous step
+    int step;          // steps taken
+    int arrested;      // arrest flag for the current step
+    int active;        // 0 = skip (retired / paused)
+    int cur;           // which half of the F / V ping-pong pairs is current
+};
+
+// Tile loader for X = F + a V + b L (V and/or L optional).
+template <class Shape, typename T, typename S>
+__device__ __forceinline__ void load_stage_tile(T* __restrict__ sm, const Params& p, int64_t N, int x0, int y0, int z0,
+                                                const S* __restrict__ F, const S* __restrict__ V,
+                                                const S* __restrict__ Lp, T a, T b) {
+    const int64_t YZ = (int64_t)p.Y * p.Z;
+    const int nrows = Shape::C * Shape::HX * Shape::HY;
+    for (int row = threadIdx.y; row < nrows; row += Shape::BY) {
+        const int c = row / (Shape::HX * Shape::HY);
+        const int r = row - c * (Shape::HX * Shape::HY);
+        const int xx = r / Shape::HY;
+        const int yy = r - xx * Shape::HY;
+        const int gx = x0 - 2 + xx;
+        const int gy = y0 - 2 + yy;
+        const bool rowok = (gx >= 0) && (gx < p.X) && (gy >= 0) && (gy < p.Y);
+        const int64_t base = (int64_t)c * N + gx * YZ + (int64_t)gy * p.Z;
+        T* dst = sm + c * Shape::VOL + xx * Shape::PLANE + yy * Shape::HZ;
+        for (int zz = threadIdx.x; zz < Shape::HZ; zz += Shape::BZ) {
+            const int gz = z0 - 2 + zz;
+            T v = T(0);
+            if (rowok && gz >= 0 && gz < p.Z) {
+                const int64_t i = base + gz;
+                v = T(F[i]);
+                if (V) v += a * T(V[i]);
+                if (Lp) v += b * T(Lp[i]);
+            }
+            dst[zz] = v;
+        }
+    }
+}
+
+__device__ __forceinline__ int find_inst(const int* __restrict__ tile_inst, int t) { return __ldg(tile_inst + t); }
+
+// ---------------------------------------------------------------------------
+// Fused stage kernel.  STAGE in 1..4.  Grid-strides over the global tile list.
+// ---------------------------------------------------------------------------
+template <template <typename> class Th, class Shape, typename T, typename S, int STAGE>
+__global__ void __launch_bounds__(Shape::NTHREADS)
+    k_engine_stage(InstDesc<S>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
+    constexpr int C = Th<T>::C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
+    __shared__ KSum shk[32];
+    __shared__ double shm[32];
+    for (int t = t_begin + blockIdx.x; t < t_end; t += gridDim.x) {
+        const int ii = find_inst(tile_inst, t);
+        InstDesc<S>& in = insts[ii];
+        if (!in.active) continue;  // uniform across the block
+        const int parity = in.cur;
+        const Params& p = in.p;
+        const int64_t N = n_sites(p);
+        const int lt = t - in.tile_begin;
+        TileGrid tg{in.tiles_nz, in.tiles_ny, in.tiles_nx};
+        int x0, y0, z0;
+        tile_origin(tg, lt, Shape::BZ, Shape::BY, Shape::TX, x0, y0, z0);
+        const S* F = in.F[parity];
+        const S* V = in.arrested ? nullptr : in.V[parity];
+        const T hdt = T(0.5 * p.dt), dtt = T(p.dt);
+        __syncthreads();
+        if (STAGE == 1) load_stage_tile<Shape, T, S>(sm, p, N, x0, y0, z0, F, nullptr, nullptr, T(0), T(0));
+        if (STAGE == 2) load_stage_tile<Shape, T, S>(sm, p, N, x0, y0, z0, F, V, nullptr, hdt, T(0));
+        if (STAGE == 3) load_stage_tile<Shape, T, S>(sm, p, N, x0, y0, z0, F, V, in.L[0], hdt, T(0.25) * dtt);
+        if (STAGE == 4) load_stage_tile<Shape, T, S>(sm, p, N, x0, y0, z0, F, V, in.L[1], dtt, T(0.5) * dtt);
+        __syncthreads();
+        StencilCoef<T> k;
+        k.init(p);
+        KSum esum{0.0, 0.0}, bsum{0.0, 0.0};
+        double gmx = -1.0e300, gab = 0.0;
+        const int z = z0 + threadIdx.x, y = y0 + threadIdx.y;
+        if (z < p.Z && y < p.Y) {
+#pragma unroll 1
+            for (int i = 0; i < Shape::TX; ++i) {
+                const int x = x0 + i;
+                if (x >= p.X) break;
+                const Mask m = site_mask(p, x, y, z);
+                T phi[C], D[3][C], Sd[6][C], g[C];
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                    site_derivs<Shape, T, C>(sm, c, i + 2, threadIdx.y + 2, threadIdx.x + 2, k, m, D, Sd, phi[c]);
+                const int64_t s = ((int64_t)x * p.Y + y) * p.Z + z;
+                if (STAGE == 1) {
+                    // FP64 energy and baryon density of F (the tile holds F exactly)
+                    StencilCoef<double> kd;
+                    kd.init(p);
+                    double phd[C], Dd[3][C];
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        const T* f = sm + c * Shape::VOL + (i + 2) * Shape::PLANE + (threadIdx.y + 2) * Shape::HZ +
+                                     threadIdx.x + 2;
+                        const int st[3] = {Shape::PLANE, Shape::HZ, 1};
+                        const bool pm[3] = {m.px, m.py, m.pz};
+                        phd[c] = double(f[0]);
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            const double v = kd.d1a[d] * (double(f[st[d]]) - double(f[-st[d]])) -
+                                             kd.d1b[d] * (double(f[2 * st[d]]) - double(f[-2 * st[d]]));
+                            Dd[d][c] = pm[d] ? v : 0.0;
+                        }
+                    }
+                    ksum_add(esum, Th<double>::energy(phd, Dd, p));
+                    ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
+                }
+                Th<T>::gradient(phi, D, Sd, p, g);
+                if (STAGE < 4) {
+                    S* lout = in.L[STAGE - 1];
+#pragma unroll
+                    for (int c = 0; c < C; ++c) lout[c * N + s] = S(-dtt * g[c]);
+                } else {
+                    // stage-4 gradient statistics (reference `err`: signed max of EG)
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        const double gd = double(g[c]);
+                        gmx = fmax(gmx, gd);
+                        gab = fmax(gab, fabs(gd));
+                    }
+                    // finalize (core/integrator.py:163-175)
+                    const S* L1 = in.L[0];
+                    const S* L2 = in.L[1];
+                    const S* L3 = in.L[2];
+                    T fv[C], vv[C];
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        const int64_t j = c * N + s;
+                        const T l1 = T(L1[j]), l2 = T(L2[j]), l3 = T(L3[j]), l4 = -dtt * g[c];
+                        const T v0 = V ? T(V[j]) : T(0);
+                        vv[c] = v0 + (l1 + T(2) * l2 + T(2) * l3 + l4) * T(1.0 / 6.0);
+                        fv[c] = T(F[j]) + dtt * (v0 + (l1 + l2 + l3) * T(1.0 / 6.0));
+                    }
+                    if (p.unit_length) {
+                        T ss = T(0);
+#pragma unroll
+                        for (int c = 0; c < C; ++c)
+                            if (c < p.nsky) ss += fv[c] * fv[c];
+                        ss = sqrt(ss);
+                        if (ss != T(0)) {
+#pragma unroll
+                            for (int c = 0; c < C; ++c)
+                                if (c < p.nsky) fv[c] /= ss;
+                        }
+                        T lm = T(0);
+#pragma unroll
+                        for (int c = 0; c < C; ++c)
+                            if (c < p.nsky) lm += vv[c] * fv[c];
+#pragma unroll
+                        for (int c = 0; c < C; ++c)
+                            if (c < p.nsky) vv[c] -= lm * fv[c];
+                    }
+                    S* Fo = in.F[parity ^ 1];
+                    S* Vo = in.V[parity ^ 1];
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        Fo[c * N + s] = S(fv[c]);
+                        Vo[c * N + s] = S(vv[c]);
+                    }
+                }
+            }
+        }
+        if (STAGE == 1) {
+            KSum be = block_ksum(esum, shk);
+            KSum bb = block_ksum(bsum, shk);
+            if (threadIdx.x == 0 && threadIdx.y == 0) {
+                in.epart[lt] = be;
+                in.bpart[lt] = bb;
+            }
+        }
+        if (STAGE == 4) {
+            const double a = block_max(gmx, shm);
+            const double b = block_max(gab, shm);
+            if (threadIdx.x == 0 && threadIdx.y == 0) {
+                in.gpart[2 * lt] = a;
+                in.gpart[2 * lt + 1] = b;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Control: one block per instance.  Reduces the stage-1 partials (energy and
+// baryon number of the field entering this step) and the previous step's
+// stage-4 gradient partials, records StepStats and sets the arrest flag.
+// ---------------------------------------------------------------------------
+// mode 0: end of a step (arrest decision); 1: admission (step 0, no arrest);
+// 2: resume after a precision change (keeps the pending arrest decision).
+template <typename S>
+__global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict__ insts, int i_begin, int i_end,
+                                                        int mode) {
+    __shared__ KSum shk[32];
+    __shared__ double shm[32];
+    const int ii = i_begin + blockIdx.x;
+    if (ii >= i_end) return;
+    InstDesc<S>& in = insts[ii];
+    if (!in.active) return;
+    const int tid = threadIdx.x;
+    KSum e{0.0, 0.0}, b{0.0, 0.0};
+    double gm = -1.0e300, ga = 0.0;
+    for (int t = tid; t < in.ntiles; t += blockDim.x) {
+        ksum_merge(e, in.epart[t]);
+        ksum_merge(b, in.bpart[t]);
+        gm = fmax(gm, in.gpart[2 * t]);
+        ga = fmax(ga, in.gpart[2 * t + 1]);
+    }
+    KSum E = block_ksum(e, shk);
+    KSum B = block_ksum(b, shk);
+    const double GM = block_max(gm, shm);
+    const double GA = block_max(ga, shm);
+    if (tid == 0) {
+        const double en = E.s + E.c;
+        if (mode == 1) in.step = 0;
+        const int n = in.step;
+        // arrest (core/integrator.py:403-407): the energy after step n exceeds the one after step n-1
+        int arrest = in.arrested;
+        if (mode == 0) arrest = (n > 0 && in.p.killkinen && en > in.e_prev) ? 1 : 0;
+        if (mode == 1) arrest = 0;
+        StepStats& st = in.stats[n % in.stats_cap];
+        st.energy = en;
+        st.baryon = B.s + B.c;
+        st.err = (n > 0) ? GM : 0.0;
+        st.gabs = (n > 0) ? GA : 0.0;
+        st.arrested = arrest;
+        st.step = n;
+        in.arrested = arrest;
+        in.e_prev = en;
+    }
+}
+
+// Flip the ping-pong halves and advance the step counter (after stage 4).
+template <typename S>
+__global__ void k_engine_advance(InstDesc<S>* __restrict__ insts, int ninst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ninst && insts[i].active) {
+        insts[i].step += 1;
+        insts[i].cur ^= 1;
+    }
+}
+
+}  // namespace sky

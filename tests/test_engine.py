@@ -1,0 +1,189 @@
+"""Resident batched engine (``sky_engine_*``) against the FP64 oracle.
+
+The engine runs the arrested-Newton step of skyrmion_solver
+``core/integrator.py:284-410`` as fused stage kernels; its arrest rule compares
+each step's energy with the previous step's, which is how the reference's
+viewer loop drives ``Simulation.step`` (``th/nuclear_skyrme/render_gl.py:944-973``).
+Tolerances: the FP64 engine agrees with the oracle to 1e-10 relative per step
+(energy, err, field); the FP32 engine to 2e-5 relative in energy over a few
+steps (single-precision stencil round-off on fields of magnitude ~1).
+"""
+import numpy as np
+import pytest
+
+from oracle import skyrme_oracle as O
+from tests import _golden as G
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_ENERGY_TOL = 2e-5
+FP32_FIELD_TOL = 2e-5
+
+
+def _inputs(name):
+    d = G.load(name)
+    return d, d["field0"], d["velocity0"], d["p_i"], d["p_f"]
+
+
+def _oracle_steps(name, F, V, p_i, p_f, nsteps):
+    th = O.THEORIES[name]
+    E = O.total_energy(th, F, p_i, p_f)
+    out = []
+    for _ in range(nsteps):
+        F, V, E1, err, _ = O.arrested_newton_step(th, F, V, p_i, p_f, E)
+        out.append((F.copy(), V.copy(), E1, err))
+        E = E1
+    return out
+
+
+@pytest.fixture(scope="module")
+def engine():
+    from skyrmion_solver_b200.engine import Engine
+    e = Engine(0)
+    yield e
+    e.close()
+
+
+@pytest.mark.parametrize("name", G.available())
+def test_fp64_engine_matches_oracle(engine, name):
+    d, F, V, p_i, p_f = _inputs(name)
+    nsteps = 3
+    ref = _oracle_steps(name, F, V, p_i, p_f, nsteps)
+    iid = engine.add(name, (p_i, p_f), F, V, precision="fp64")
+    try:
+        s0 = engine.stats(iid, 0)
+        assert abs(s0.energy - O.total_energy(O.THEORIES[name], F, p_i, p_f)) <= FP64_TOL * abs(s0.energy)
+        for n in range(1, nsteps + 1):
+            engine.step(1)
+            st = engine.stats(iid)
+            Fr, Vr, Er, errr = ref[n - 1]
+            assert st.step == n
+            assert abs(st.energy - Er) <= FP64_TOL * abs(Er), (n, st.energy, Er)
+            assert abs(st.err - errr) <= FP64_TOL * max(abs(errr), 1.0), (n, st.err, errr)
+            f, v = engine.read(iid)
+            assert G.rel_err(f, Fr) <= FP64_TOL
+            if np.any(Vr):
+                assert G.rel_err(v, Vr) <= FP64_TOL
+            else:
+                assert not np.any(v)
+    finally:
+        engine.remove(iid)
+
+
+@pytest.mark.parametrize("name", ["nuclear", "omega", "coulomb", "rho"])
+def test_fp32_engine_tracks_fp64(engine, name):
+    d, F, V, p_i, p_f = _inputs(name)
+    a = engine.add(name, (p_i, p_f), F, V, precision="fp64")
+    b = engine.add(name, (p_i, p_f), F, V, precision="fp32")
+    try:
+        engine.step(4)
+        sa, sb = engine.stats(a), engine.stats(b)
+        assert sa.step == sb.step == 4
+        assert abs(sa.energy - sb.energy) <= FP32_ENERGY_TOL * abs(sa.energy)
+        assert abs(sa.baryon - sb.baryon) <= 1e-4
+        fa, _ = engine.read(a)
+        fb, _ = engine.read(b)
+        assert G.rel_err(fb, fa) <= FP32_FIELD_TOL
+    finally:
+        engine.remove(a)
+        engine.remove(b)
+
+
+def test_alone_equals_in_mix():
+    """A solve's trajectory is bitwise the same alone and batched with other theories / sizes."""
+    from skyrmion_solver_b200.engine import Engine
+    d, F, V, p_i, p_f = _inputs("nuclear")
+    with Engine(0) as alone:
+        i = alone.add("nuclear", (p_i, p_f), F, V, precision="fp32")
+        alone.step(11)
+        s_alone = [alone.stats(i, n) for n in range(12)]
+        f_alone, v_alone = alone.read(i)
+    with Engine(0) as mix:
+        others = []
+        for name in ("omega", "rho", "coulomb"):
+            _, Fo, Vo, pio, pfo = _inputs(name)
+            others.append(mix.add(name, (pio, pfo), Fo, Vo, precision="fp32"))
+        j = mix.add("nuclear", (p_i, p_f), F, V, precision="fp32")
+        # a second nuclear instance of another size shares the batch with j
+        from skyrmion_solver_b200 import theories as T
+        th = T.by_short_name("nuclear")
+        p2 = th.params.default_params(xlen=20, ylen=17, zlen=24, lsx=0.2, lsy=0.2, lsz=0.2, time_step=0.04)
+        p2i, p2f = th.params.pack_device_params(p2.resolved())
+        from skyrmion_solver_b200.initial import hedgehog, exp_profile
+        F2 = hedgehog((20, 17, 24), (0.2, 0.2, 0.2), exp_profile(1.0))
+        others.append(mix.add("nuclear", (p2i, p2f), F2, None, precision="fp32"))
+        mix.step(11)
+        s_mix = [mix.stats(j, n) for n in range(12)]
+        f_mix, v_mix = mix.read(j)
+    for a, b in zip(s_alone, s_mix):
+        assert (a.energy, a.baryon, a.err, a.gabs, a.arrested) == (b.energy, b.baryon, b.err, b.gabs, b.arrested)
+    assert np.array_equal(f_alone, f_mix) and np.array_equal(v_alone, v_mix)
+
+
+def test_graph_replay_equals_single_steps():
+    from skyrmion_solver_b200.engine import Engine
+    d, F, V, p_i, p_f = _inputs("omega")
+    with Engine(0) as a, Engine(0) as b:
+        ia = a.add("omega", (p_i, p_f), F, V, precision="fp32")
+        ib = b.add("omega", (p_i, p_f), F, V, precision="fp32")
+        a.step(16)                  # two graph replays
+        for _ in range(16):
+            b.step(1)               # direct launches
+        fa, va = a.read(ia)
+        fb, vb = b.read(ib)
+        assert np.array_equal(fa, fb) and np.array_equal(va, vb)
+        assert a.stats(ia).energy == b.stats(ib).energy
+
+
+def test_precision_switch_and_remove(engine):
+    d, F, V, p_i, p_f = _inputs("nuclear")
+    ref = _oracle_steps("nuclear", F, V, p_i, p_f, 4)
+    iid = engine.add("nuclear", (p_i, p_f), F, V, precision="fp64")
+    bytes_with = engine.bytes
+    engine.step(2)
+    engine.set_precision(iid, "fp32")
+    engine.set_precision(iid, "fp64")   # round trip through FP32 storage
+    engine.step(2)
+    st = engine.stats(iid)
+    assert st.step == 4
+    # the FP32 round trip perturbs the field at 1e-7; the energy stays close to the FP64 trajectory
+    assert abs(st.energy - ref[3][2]) <= 1e-6 * abs(ref[3][2])
+    # record 2 was re-evaluated on the FP32-rounded field when the precision changed
+    assert engine.stats(iid, 2).energy == pytest.approx(ref[1][2], rel=1e-6)
+    engine.remove(iid)
+    assert engine.bytes < bytes_with
+    with pytest.raises(ValueError):
+        engine.stats(iid)
+
+
+def test_pause_keeps_state(engine):
+    d, F, V, p_i, p_f = _inputs("nuclear")
+    a = engine.add("nuclear", (p_i, p_f), F, V, precision="fp64")
+    b = engine.add("nuclear", (p_i, p_f), F, V, precision="fp64")
+    try:
+        engine.set_active(b, False)
+        engine.step(2)
+        engine.set_active(b, True)
+        engine.step(2)
+        assert engine.stats(a).step == 4
+        assert engine.stats(b, 2).step == 2
+        fb, _ = engine.read(b)
+        ref = _oracle_steps("nuclear", F, V, p_i, p_f, 2)
+        assert G.rel_err(fb, ref[1][0]) <= FP64_TOL
+    finally:
+        engine.remove(a)
+        engine.remove(b)
+
+
+def test_invalid_arguments(engine):
+    from skyrmion_solver_b200._lib import SkyInvalidArgument
+    d, F, V, p_i, p_f = _inputs("nuclear")
+    bad = p_i.copy()
+    bad[6] += 1
+    with pytest.raises((SkyInvalidArgument, ValueError)):
+        engine.add("nuclear", (bad, p_f), F, V)
+    with pytest.raises(ValueError):
+        engine.add("nuclear", (p_i, p_f), F[:, :-1], V)
+    with pytest.raises(SkyInvalidArgument):
+        engine.remove(10 ** 6)
