@@ -48,6 +48,14 @@ typedef enum {
 const char* sky_version(void);
 const char* sky_last_error(void);
 
+/* Library-wide tuning options.  Key 0: kernel family of the reference-layout
+ * gradient (sky_gradient_step / sky_arrested_newton_step) for theories with at
+ * most five components: 1 = marching x-plane kernels (default), 0 = 3-D tile
+ * kernels.  Key 1: x-chunk of those marching launches (0 = automatic).
+ * Process-wide; not synchronised with launches in flight on other threads. */
+int sky_set_option(int key, int value);
+int sky_get_option(int key);
+
 /* Number of field components the theory's kernels are built for. */
 int sky_theory_components(int theory);
 
@@ -156,6 +164,13 @@ int sky_engine_remove(void* engine, int id);
 /* Change an instance's precision in place (FP32 -> FP64 for the polishing
  * phase); the field, velocity, step count and pending arrest decision carry over. */
 int sky_engine_set_precision(void* engine, int id, int precision);
+
+/* Re-tile an instance of a marching-kernel theory (C <= 5): x-chunk `xc`
+ * planes per block (0 = automatic choice from the grid and the SM count).  The
+ * state and the pending arrest decision carry over. */
+int sky_engine_retile(void* engine, int id, int xc);
+/* Current x-chunk of an instance (0 for tile-kernel theories, -1 if unknown). */
+int sky_engine_get_xc(void* engine, int id);
 
 /* Pause (0) or resume (1) an instance. */
 int sky_engine_set_active(void* engine, int id, int active);

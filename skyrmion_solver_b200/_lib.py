@@ -52,6 +52,8 @@ _D = ctypes.c_double
 SIGNATURES = {
     "sky_version": ([], ctypes.c_char_p),
     "sky_last_error": ([], ctypes.c_char_p),
+    "sky_set_option": ([_I, _I], _I),
+    "sky_get_option": ([_I], _I),
     "sky_theory_components": ([_I], _I),
     "sky_reduce_scratch_size": ([_I64], _I64),
     "sky_gradient_step": ([_I, _I32P, _I32, _F64P, _I32, _P, _P, _P, _P], _I),
@@ -75,6 +77,8 @@ SIGNATURES = {
     "sky_engine_remove": ([_P, _I], _I),
     "sky_engine_set_precision": ([_P, _I, _I], _I),
     "sky_engine_set_active": ([_P, _I, _I], _I),
+    "sky_engine_retile": ([_P, _I, _I], _I),
+    "sky_engine_get_xc": ([_P, _I], _I),
     "sky_engine_step": ([_P, _I], _I),
     "sky_engine_synchronize": ([_P], _I),
     "sky_engine_stream": ([_P], _P),

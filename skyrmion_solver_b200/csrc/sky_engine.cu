@@ -31,6 +31,8 @@ struct HostInst {
     double* gpart = nullptr;
     StepStats* stats = nullptr;
     int ntiles = 0, tnz = 0, tny = 0, tnx = 0;
+    int xc = 0;          // x-chunk of the marching kernels (0: tile kernels)
+    int xc_request = 0;  // x-chunk asked for by the caller (0: automatic)
     int group_slot = -1;
     int64_t steps = 0;  // host mirror of the device step counter
     bool active = true;
@@ -63,21 +65,47 @@ struct Engine {
 template <template <typename> class Th, typename T>
 using EShape = typename GradTile<Th<T>::C, T>::type;
 
+// Theories with at most five components run the marching kernels
+// (sky_march.cuh); the 13-component rho variant keeps the 3-D tile kernel.
+template <template <typename> class Th>
+constexpr bool uses_march() {
+    return Th<float>::C <= 5;
+}
+constexpr int kMarchBY = 8;
+template <template <typename> class Th, typename T>
+using MShape = MarchShape<Th<T>::C, kMarchBY>;
+
+template <int STAGE>
+constexpr int stage_nsrc() {
+    return STAGE == 1 ? 1 : (STAGE == 2 ? 2 : 3);
+}
+
 // One-time kernel attribute setup (kept out of stream capture); returns the
 // number of resident blocks per SM.
 template <template <typename> class Th, typename T, int STAGE>
 static int stage_setup(int* per_sm_out) {
-    using Shape = EShape<Th, T>;
-    auto kern = k_engine_stage<Th, Shape, T, T, STAGE>;
-    const size_t smem = Shape::template smem_bytes<T>();
     static int per_sm = 0;
     if (per_sm == 0) {
-        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+        int rc, n = 0;
+        if constexpr (uses_march<Th>()) {
+            using M = MShape<Th, T>;
+            auto kern = k_march_stage<Th, M, T, STAGE>;
+            const size_t smem = M::template smem_bytes<T>(stage_nsrc<STAGE>());
+            rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(march stage)", __LINE__);
+            if (rc) return rc;
+            rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem),
+                            "occupancy query", __LINE__);
+        } else {
+            using Shape = EShape<Th, T>;
+            auto kern = k_engine_stage<Th, Shape, T, T, STAGE>;
+            const size_t smem = Shape::template smem_bytes<T>();
+            rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                             "cudaFuncSetAttribute(engine stage)", __LINE__);
-        if (rc) return rc;
-        int n = 0;
-        rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, Shape::NTHREADS, smem),
-                        "occupancy query", __LINE__);
+            if (rc) return rc;
+            rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, Shape::NTHREADS, smem),
+                            "occupancy query", __LINE__);
+        }
         if (rc) return rc;
         per_sm = n < 1 ? 1 : n;
     }
@@ -87,17 +115,23 @@ static int stage_setup(int* per_sm_out) {
 
 template <template <typename> class Th, typename T, int STAGE>
 static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
-    using Shape = EShape<Th, T>;
-    auto kern = k_engine_stage<Th, Shape, T, T, STAGE>;
-    const size_t smem = Shape::template smem_bytes<T>();
     int per_sm = 1;
     int rc = stage_setup<Th, T, STAGE>(&per_sm);
     if (rc) return rc;
     int n = t_end - t_begin;
     if (n <= 0) return SKY_OK;
-    int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
-    kern<<<blocks, dim3(Shape::BZ, Shape::BY), smem, st>>>(reinterpret_cast<InstDesc<T>*>(g.d_desc), g.d_tile_inst,
-                                                          t_begin, t_end);
+    const int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
+    InstDesc<T>* d = reinterpret_cast<InstDesc<T>*>(g.d_desc);
+    if constexpr (uses_march<Th>()) {
+        using M = MShape<Th, T>;
+        const size_t smem = M::template smem_bytes<T>(stage_nsrc<STAGE>());
+        k_march_stage<Th, M, T, STAGE><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(d, g.d_tile_inst, t_begin, t_end);
+    } else {
+        using Shape = EShape<Th, T>;
+        const size_t smem = Shape::template smem_bytes<T>();
+        k_engine_stage<Th, Shape, T, T, STAGE><<<blocks, dim3(Shape::BZ, Shape::BY), smem, st>>>(d, g.d_tile_inst,
+                                                                                                t_begin, t_end);
+    }
     return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
 }
 
@@ -154,25 +188,35 @@ static int launch_stage_group(int stage, const Group& g, int tb, int te, cudaStr
     return invalid("unknown theory id");
 }
 
+// Tile geometry of a (theory, precision): (bz, by, tx) of the tile kernels, or
+// (32, BY, 0) for the marching kernels, whose x-chunk is chosen per instance;
+// per_sm = resident stage-4 blocks per SM.
 template <template <typename> class Th>
-static void shape_of(int prec, int& bz, int& by, int& tx) {
-    if (prec) {
-        using S = EShape<Th, double>;
-        bz = S::BZ, by = S::BY, tx = S::TX;
+static int shape_of(int prec, int& bz, int& by, int& tx, int& per_sm) {
+    per_sm = 1;
+    if constexpr (uses_march<Th>()) {
+        bz = 32, by = kMarchBY, tx = 0;
+        return prec ? stage_setup<Th, double, 4>(&per_sm) : stage_setup<Th, float, 4>(&per_sm);
     } else {
-        using S = EShape<Th, float>;
-        bz = S::BZ, by = S::BY, tx = S::TX;
+        if (prec) {
+            using S = EShape<Th, double>;
+            bz = S::BZ, by = S::BY, tx = S::TX;
+        } else {
+            using S = EShape<Th, float>;
+            bz = S::BZ, by = S::BY, tx = S::TX;
+        }
+        return SKY_OK;
     }
 }
 
-static void tile_shape(int theory, int prec, int& bz, int& by, int& tx) {
+static int tile_shape(int theory, int prec, int& bz, int& by, int& tx, int& per_sm) {
     switch (theory) {
-        case SKY_THEORY_NUCLEAR: shape_of<Nuclear>(prec, bz, by, tx); break;
-        case SKY_THEORY_OMEGA: shape_of<Omega>(prec, bz, by, tx); break;
-        case SKY_THEORY_COULOMB: shape_of<Coulomb>(prec, bz, by, tx); break;
-        case SKY_THEORY_RHO: shape_of<Rho>(prec, bz, by, tx); break;
-        case SKY_THEORY_BERGER: shape_of<Berger>(prec, bz, by, tx); break;
-        default: shape_of<LightlyBound>(prec, bz, by, tx); break;
+        case SKY_THEORY_NUCLEAR: return shape_of<Nuclear>(prec, bz, by, tx, per_sm);
+        case SKY_THEORY_OMEGA: return shape_of<Omega>(prec, bz, by, tx, per_sm);
+        case SKY_THEORY_COULOMB: return shape_of<Coulomb>(prec, bz, by, tx, per_sm);
+        case SKY_THEORY_RHO: return shape_of<Rho>(prec, bz, by, tx, per_sm);
+        case SKY_THEORY_BERGER: return shape_of<Berger>(prec, bz, by, tx, per_sm);
+        default: return shape_of<LightlyBound>(prec, bz, by, tx, per_sm);
     }
 }
 
@@ -241,6 +285,7 @@ static InstDesc<S> make_desc(const HostInst& h, int tile_begin) {
     d.tiles_nz = h.tnz;
     d.tiles_ny = h.tny;
     d.tiles_nx = h.tnx;
+    d.xc = h.xc;
     d.active = h.active ? 1 : 0;
     return d;
 }
@@ -324,10 +369,19 @@ static void free_inst(HostInst& h) {
 static int alloc_inst(Engine& e, HostInst& h) {
     const size_t es = h.prec ? sizeof(double) : sizeof(float);
     const size_t fb = es * (size_t)h.C * (size_t)h.N;
-    int bz, by, tx;
-    tile_shape(h.theory, h.prec, bz, by, tx);
+    int bz, by, tx, per_sm;
+    int rc0 = tile_shape(h.theory, h.prec, bz, by, tx, per_sm);
+    if (rc0) return rc0;
     h.tnz = (h.p.Z + bz - 1) / bz;
     h.tny = (h.p.Y + by - 1) / by;
+    if (tx == 0) {
+        if ((int64_t)h.C * h.N >= ((int64_t)1 << 31)) return invalid("lattice too large for the marching kernels");
+        h.xc = h.xc_request > 0 ? (h.xc_request < h.p.X ? h.xc_request : h.p.X)
+                                : choose_xc(h.p.X, h.tnz * h.tny, num_sms() * per_sm);
+        tx = h.xc;
+    } else {
+        h.xc = 0;
+    }
     h.tnx = (h.p.X + tx - 1) / tx;
     h.ntiles = h.tnz * h.tny * h.tnx;
     void** bufs[] = {&h.F[0], &h.F[1], &h.V[0], &h.V[1], &h.L[0], &h.L[1], &h.L[2]};
@@ -650,6 +704,61 @@ int sky_engine_set_precision(void* handle, int id, int precision) {
         cudaMemcpyAsync(&dd->e_prev, &e_prev, sizeof(double), cudaMemcpyHostToDevice, e->stream);
     }
     return init_instance(*e, h, 2);
+}
+
+int sky_engine_retile(void* handle, int id, int xc) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return invalid("null engine");
+    HostInst* hp = find(e, id);
+    if (!hp) return invalid("unknown instance id");
+    if (xc < 0) return invalid("xc must be >= 0 (0: automatic)");
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    HostInst& h = *hp;
+    int bz, by, tx, per_sm;
+    int rc = tile_shape(h.theory, h.prec, bz, by, tx, per_sm);
+    if (rc) return rc;
+    if (tx != 0) return SKY_OK;  // tile-kernel theory: fixed geometry
+    const int tny = (h.p.Y + by - 1) / by, tnz = (h.p.Z + bz - 1) / bz;
+    const int nxc = xc > 0 ? (xc < h.p.X ? xc : h.p.X) : choose_xc(h.p.X, tnz * tny, num_sms() * per_sm);
+    const int ntiles = tnz * tny * ((h.p.X + nxc - 1) / nxc);
+    KSum *ep = nullptr, *bp = nullptr;
+    double* gp = nullptr;
+    if (cudaMalloc(&ep, sizeof(KSum) * ntiles) != cudaSuccess || cudaMalloc(&bp, sizeof(KSum) * ntiles) != cudaSuccess ||
+        cudaMalloc(&gp, sizeof(double) * 2 * ntiles) != cudaSuccess) {
+        cudaGetLastError();
+        if (ep) cudaFree(ep);
+        if (bp) cudaFree(bp);
+        if (gp) cudaFree(gp);
+        return SKY_ERR_NOMEM;
+    }
+    // The per-tile partials of the latest stage 1 feed the next control launch:
+    // re-run stage 1 and the control in resume mode under the new geometry (the
+    // pending arrest decision and the step's gradient statistics are kept).
+    cudaFree(h.epart);
+    cudaFree(h.bpart);
+    cudaFree(h.gpart);
+    h.epart = ep;
+    h.bpart = bp;
+    h.gpart = gp;
+    cudaMemsetAsync(h.gpart, 0, sizeof(double) * 2 * ntiles, e->stream);
+    const int64_t dbytes = (int64_t)(sizeof(KSum) * 2 + sizeof(double) * 2) * ((int64_t)ntiles - h.ntiles);
+    h.bytes += dbytes;
+    e->bytes += dbytes;
+    h.xc_request = xc;
+    h.xc = nxc;
+    h.tnx = (h.p.X + nxc - 1) / nxc;
+    h.ntiles = ntiles;
+    Group& g = e->groups[h.theory][h.prec];
+    if ((rc = rebuild_group(*e, g))) return rc;
+    return init_instance(*e, h, 2);
+}
+
+int sky_engine_get_xc(void* handle, int id) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return -1;
+    HostInst* h = find(e, id);
+    return h ? h->xc : -1;
 }
 
 int sky_engine_set_active(void* handle, int id, int active) {

@@ -22,6 +22,7 @@
 #pragma once
 
 #include "sky_kernels.cuh"
+#include "sky_march.cuh"
 
 namespace sky {
 
@@ -52,6 +53,7 @@ struct InstDesc {
     int tile_begin;    // first global tile index of this instance
     int ntiles;
     int tiles_nz, tiles_ny, tiles_nx;
+    int xc;            // x-chunk of the marching kernels (0: tile kernels)
     // control state (device-updated)
     double e_prev;     // energy entering the previous step
     int step;          // steps taken
@@ -276,8 +278,10 @@ __global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict_
         StepStats& st = in.stats[n % in.stats_cap];
         st.energy = en;
         st.baryon = B.s + B.c;
-        st.err = (n > 0) ? GM : 0.0;
-        st.gabs = (n > 0) ? GA : 0.0;
+        if (mode != 2) {  // a resume keeps the step's gradient statistics
+            st.err = (n > 0) ? GM : 0.0;
+            st.gabs = (n > 0) ? GA : 0.0;
+        }
         st.arrested = arrest;
         st.step = n;
         in.arrested = arrest;
@@ -292,6 +296,123 @@ __global__ void k_engine_advance(InstDesc<S>* __restrict__ insts, int ninst) {
     if (i < ninst && insts[i].active) {
         insts[i].step += 1;
         insts[i].cur ^= 1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Marching stage kernel (C <= 5 theories): the stage input is built while the
+// x-planes are staged (sky_march.cuh); the epilogue writes l_s, or applies the
+// RK4 update at stage 4.
+// ---------------------------------------------------------------------------
+template <typename T, int STAGE>
+struct EngineEpi {
+    const T* F;
+    const T* V;  // null when the velocity is arrested
+    const T* L1;
+    const T* L2;
+    const T* L3;
+    T* out0;     // l_STAGE (stages 1-3) or F' (stage 4)
+    T* out1;     // V' (stage 4)
+    T dtt;
+    int nsky;
+    int unit_length;
+    double gmx, gab;
+    template <int C>
+    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g)[C]) {
+        if (STAGE < 4) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) out0[c * N + s] = -dtt * g[c];
+            return;
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const double gd = double(g[c]);
+            gmx = fmax(gmx, gd);
+            gab = fmax(gab, fabs(gd));
+        }
+        // core/integrator.py:163-175: V' = V + (l1 + 2 l2 + 2 l3 + l4)/6, F' = F + (k1 + 2k2 + 2k3 + k4)/6
+        T fv[C], vv[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const int64_t j = c * N + s;
+            const T l1 = L1[j], l2 = L2[j], l3 = L3[j], l4 = -dtt * g[c];
+            const T v0 = V ? V[j] : T(0);
+            vv[c] = v0 + (l1 + T(2) * l2 + T(2) * l3 + l4) * T(1.0 / 6.0);
+            fv[c] = F[j] + dtt * (v0 + (l1 + l2 + l3) * T(1.0 / 6.0));
+        }
+        if (unit_length) {
+            T ss = T(0);
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) ss += fv[c] * fv[c];
+            ss = sqrt(ss);
+            if (ss != T(0)) {
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                    if (c < nsky) fv[c] /= ss;
+            }
+            T lm = T(0);
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) lm += vv[c] * fv[c];
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) vv[c] -= lm * fv[c];
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            out0[c * N + s] = fv[c];
+            out1[c * N + s] = vv[c];
+        }
+    }
+};
+
+template <template <typename> class Th, class M, typename T, int STAGE>
+__global__ void __launch_bounds__(M::NTHREADS)
+    k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
+    constexpr int NSRC = STAGE == 1 ? 1 : (STAGE == 2 ? 2 : 3);
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
+    __shared__ KSum shk[32];
+    __shared__ double shm[32];
+    for (int t = t_begin + blockIdx.x; t < t_end; t += gridDim.x) {
+        const int ii = __ldg(tile_inst + t);
+        const InstDesc<T>& in = insts[ii];
+        if (!in.active) continue;  // uniform across the block
+        const Params p = in.p;
+        const int parity = in.cur;
+        const int lt = t - in.tile_begin;
+        const MarchGrid mg{in.tiles_nz, in.tiles_ny, in.tiles_nx, in.xc};
+        int xa, xe, y0, z0;
+        march_origin(mg, lt, M::BY, xa, xe, y0, z0, p.X);
+        const T* F = in.F[parity];
+        const T* V = in.arrested ? nullptr : in.V[parity];
+        const T dtt = T(p.dt), hdt = T(0.5 * p.dt);
+        const T* const src[3] = {F, V, STAGE == 3 ? in.L[0] : in.L[1]};
+        const T a = STAGE == 4 ? dtt : hdt;
+        const T b = STAGE == 3 ? T(0.25) * dtt : T(0.5) * dtt;
+        EngineEpi<T, STAGE> epi{F, V, in.L[0], in.L[1], in.L[2],
+                                STAGE < 4 ? in.L[STAGE - 1] : in.F[parity ^ 1],
+                                STAGE < 4 ? nullptr : in.V[parity ^ 1],
+                                dtt, p.nsky, p.unit_length, -1.0e300, 0.0};
+        KSum es{0.0, 0.0}, bs{0.0, 0.0};
+        march_tile<Th, M, T, NSRC, STAGE == 1>(sm, p, src, a, b, xa, xe, y0, z0, epi, es, bs);
+        if (STAGE == 1) {
+            const KSum be = block_ksum(es, shk);
+            const KSum bb = block_ksum(bs, shk);
+            if (threadIdx.x == 0 && threadIdx.y == 0) {
+                in.epart[lt] = be;
+                in.bpart[lt] = bb;
+            }
+        }
+        if (STAGE == 4) {
+            const double ga = block_max(epi.gmx, shm);
+            const double gb = block_max(epi.gab, shm);
+            if (threadIdx.x == 0 && threadIdx.y == 0) {
+                in.gpart[2 * lt] = ga;
+                in.gpart[2 * lt + 1] = gb;
+            }
+        }
     }
 }
 

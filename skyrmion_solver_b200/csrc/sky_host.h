@@ -16,6 +16,8 @@ int pack_core(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
 int pack_params(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf, Params* out);
 int num_sms();
 int ew_blocks(int64_t n);
+int choose_xc(int X, int tiles_yz, int resident);
+int option(int key);
 
 int gradient_fp64(int theory, const Params& p, const double* f, double* eg, double* l, cudaStream_t st);
 int density_fp64(int theory, const Params& p, int mode, const double* f, double* dens, double* scratch,

@@ -1,0 +1,309 @@
+// Marching stencil kernels ("2.5-D" x-march).
+//
+// A thread block owns a BY x 32 (y, z) tile of one lattice and walks along x
+// over a chunk [xa, xe).  The haloed input planes (BY+4) x 36 of all C
+// components pass through a ring of five shared-memory slots (planes x-2 ..
+// x+2 of the site being finished); the next plane is copied from global memory
+// with cp.async into a staging area while the current one is computed, so the
+// global-load latency overlaps the stencil and point arithmetic.
+//
+// Per thread and component two register queues hold, for planes x-2 .. x+2 at
+// the thread's own (y, z), the raw first-difference sums
+//   uy = f[y-2] - 8 f[y-1] + 8 f[y+1] - f[y+2]   and   uz (same along z),
+// so the mixed derivatives d_x d_y and d_x d_z come from five registers
+// instead of sixteen shared-memory taps each:
+//   sum_{m,n} c_m c_n f[x+m, y+n] = sum_m c_m uy(x+m),  c = (1, -8, 0, 8, -1),
+// which is the reference's 5x5 outer-product stencil (core/derivatives.py:121-173)
+// regrouped; only the rounding order differs.  d_y d_z uses the 16 in-plane taps.
+//
+// The stage input is X = F + a V + b L (the RK4 stage fields of
+// core/integrator.py:50-92, built on the fly), so a stage reads each input
+// array once per site plus the halo.
+#pragma once
+
+#include "sky_kernels.cuh"
+
+namespace sky {
+
+template <int C_, int BY_>
+struct MarchShape {
+    static constexpr int C = C_, BY = BY_, BZ = 32;
+    static constexpr int HY = BY + 4, HZ = BZ + 4;
+    static constexpr int PLANE = HY * HZ;  // one component of one plane, with halo
+    static constexpr int SLOT = C * PLANE;  // all components of one plane
+    static constexpr int RING = 5;
+    static constexpr int NTHREADS = BZ * BY;
+    static constexpr int NPER = (SLOT + NTHREADS - 1) / NTHREADS;  // plane elements per thread
+    template <typename T>
+    static constexpr size_t smem_bytes(int nsrc) {
+        return (size_t(RING) + size_t(nsrc)) * SLOT * sizeof(T);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// cp.async (sm_80+ asynchronous global -> shared copies; zero-fill when the
+// source size is 0, so out-of-lattice halo points read as 0 without a load).
+// ---------------------------------------------------------------------------
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool valid) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    const int n = valid ? BYTES : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem), "n"(BYTES), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Per-thread element offsets of the haloed plane: element k of thread tid is
+// idx = tid + k*NTHREADS of the slot, i.e. (c, yy, zz) = decompose(idx); its
+// global offset within the x-plane is c*N + gy*Z + gz (int32), or -1 when the
+// point lies outside the lattice in y or z (or idx is past the slot).  The
+// host guarantees C*N < 2^31 for marching launches.
+template <class M>
+struct PlaneOffsets {
+    int off[M::NPER];
+    __device__ __forceinline__ void init(const Params& p, int64_t N, int y0, int z0) {
+        const int tid = threadIdx.x + M::BZ * threadIdx.y;
+#pragma unroll
+        for (int k = 0; k < M::NPER; ++k) {
+            const int idx = tid + k * M::NTHREADS;
+            const int row = idx / M::HZ;
+            const int zz = idx - row * M::HZ;
+            const int c = row / M::HY;
+            const int yy = row - c * M::HY;
+            const int gy = y0 - 2 + yy, gz = z0 - 2 + zz;
+            const bool ok = idx < M::SLOT && gy >= 0 && gy < p.Y && gz >= 0 && gz < p.Z;
+            off[k] = ok ? static_cast<int>(c * N + (int64_t)gy * p.Z + gz) : -1;
+        }
+    }
+};
+
+// Issue the cp.async copies of one x-plane (element offset plane_base) of the
+// NSRC source arrays into the staging slots; a null source reads as zero.
+template <class M, int NSRC, typename T>
+__device__ __forceinline__ void plane_issue(T* __restrict__ stage, const PlaneOffsets<M>& po, const T* const (&src)[3],
+                                            int64_t plane_base, bool xok) {
+    const int tid = threadIdx.x + M::BZ * threadIdx.y;
+#pragma unroll
+    for (int k = 0; k < M::NPER; ++k) {
+        const int idx = tid + k * M::NTHREADS;
+        if (M::SLOT % M::NTHREADS == 0 || idx < M::SLOT) {
+            const bool ok = xok && po.off[k] >= 0;
+#pragma unroll
+            for (int s = 0; s < NSRC; ++s) {
+                const T* g = src[s];
+                const bool v = ok && g != nullptr;
+                cp_async<sizeof(T)>(stage + s * M::SLOT + idx,
+                                    v ? (const void*)(g + plane_base + po.off[k]) : (const void*)src[0], v);
+            }
+        }
+    }
+    cp_async_commit();
+}
+
+// Combine the thread's own staged elements into a ring slot: X = F + a V + b L.
+template <class M, int NSRC, typename T>
+__device__ __forceinline__ void plane_combine(T* __restrict__ slot, const T* __restrict__ stage, T a, T b) {
+    const int tid = threadIdx.x + M::BZ * threadIdx.y;
+#pragma unroll
+    for (int k = 0; k < M::NPER; ++k) {
+        const int idx = tid + k * M::NTHREADS;
+        if (M::SLOT % M::NTHREADS == 0 || idx < M::SLOT) {
+            T v = stage[idx];
+            if (NSRC > 1) v += a * stage[M::SLOT + idx];
+            if (NSRC > 2) v += b * stage[2 * M::SLOT + idx];
+            slot[idx] = v;
+        }
+    }
+}
+
+// Raw first-difference sum c_m f[m*st], c = (1, -8, 0, 8, -1) for m = -2..2.
+template <typename T>
+__device__ __forceinline__ T diff5(const T* f, int st) {
+    return (f[-2 * st] - f[2 * st]) + T(8) * (f[st] - f[-st]);
+}
+
+// ---------------------------------------------------------------------------
+// One tile: planes xa-2 .. xe+1 of lattice p through the ring; the point
+// physics Th<T> and the epilogue Epi run at every in-lattice site with x in
+// [xa, xe).  DENS adds the FP64 energy / baryon densities of the stage input
+// to esum / bsum (compensated).
+// ---------------------------------------------------------------------------
+template <template <typename> class Th, class M, typename T, int NSRC, bool DENS, class Epi>
+__device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, const T* const (&src)[3], T a, T b,
+                                           int xa, int xe, int y0, int z0, Epi& epi, KSum& esum, KSum& bsum) {
+    constexpr int C = M::C;
+    static_assert(Th<T>::C == C, "component count mismatch");
+    T* ring = sm;
+    T* stage = sm + M::RING * M::SLOT;
+    const int64_t N = n_sites(p);
+    const int64_t YZ = (int64_t)p.Y * p.Z;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int y = y0 + ty, z = z0 + tx;
+    const bool own = (y < p.Y) && (z < p.Z);
+    StencilCoef<T> k;
+    k.init(p);
+    PlaneOffsets<M> po;
+    po.init(p, N, y0, z0);
+    T uq[C][5], wq[C][5];  // uy / uz queues for planes x-2 .. x+2
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+#pragma unroll
+        for (int m = 0; m < 5; ++m) uq[c][m] = wq[c][m] = T(0);
+    const int q0 = xa - 2, q1 = xe + 1;
+    const int lofs = (ty + 2) * M::HZ + (tx + 2);  // thread's site within a component plane
+    __syncthreads();
+    plane_issue<M, NSRC, T>(stage, po, src, (int64_t)q0 * YZ, q0 >= 0 && q0 < p.X);
+    int slot = 0;  // ring slot of plane q
+    for (int q = q0; q <= q1; ++q) {
+        cp_async_wait_all();
+        __syncthreads();  // (A) every thread finished the previous centre: slot `slot` is free
+        plane_combine<M, NSRC, T>(ring + slot * M::SLOT, stage, a, b);
+        if (q < q1) plane_issue<M, NSRC, T>(stage, po, src, (int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X);
+        __syncthreads();  // (B) slot complete
+        // arrival: first-difference sums of plane q at (y, z)
+        {
+            const T* P = ring + slot * M::SLOT + lofs;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    uq[c][m] = uq[c][m + 1];
+                    wq[c][m] = wq[c][m + 1];
+                }
+                uq[c][4] = diff5<T>(P + c * M::PLANE, M::HZ);
+                wq[c][4] = diff5<T>(P + c * M::PLANE, 1);
+            }
+        }
+        const int x = q - 2;
+        if (x >= xa && own) {
+            // plane q-j sits in slot (slot + 5 - j) % 5: x-2 = q-4, ..., x+2 = q
+            const T* Pm2 = ring + ((slot + 1) % 5) * M::SLOT + lofs;
+            const T* Pm1 = ring + ((slot + 2) % 5) * M::SLOT + lofs;
+            const T* P0 = ring + ((slot + 3) % 5) * M::SLOT + lofs;
+            const T* Pp1 = ring + ((slot + 4) % 5) * M::SLOT + lofs;
+            const T* Pp2 = ring + slot * M::SLOT + lofs;
+            const Mask mk = site_mask(p, x, y, z);
+            T phi[C], D[3][C], Sd[6][C], g[C];
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const int co = c * M::PLANE;
+                const T* f = P0 + co;
+                const T f0 = f[0];
+                phi[c] = f0;
+                {
+                    const T fm2 = Pm2[co], fm1 = Pm1[co], fp1 = Pp1[co], fp2 = Pp2[co];
+                    D[0][c] = mk.px ? k.d1a[0] * (fp1 - fm1) - k.d1b[0] * (fp2 - fm2) : T(0);
+                    Sd[0][c] = mk.px ? k.d2a[0] * (fp1 + fm1) - k.d2b[0] * (fp2 + fm2) - k.d2c[0] * f0 : T(0);
+                }
+                {
+                    const T fm2 = f[-2 * M::HZ], fm1 = f[-M::HZ], fp1 = f[M::HZ], fp2 = f[2 * M::HZ];
+                    D[1][c] = mk.py ? k.d1a[1] * (fp1 - fm1) - k.d1b[1] * (fp2 - fm2) : T(0);
+                    Sd[1][c] = mk.py ? k.d2a[1] * (fp1 + fm1) - k.d2b[1] * (fp2 + fm2) - k.d2c[1] * f0 : T(0);
+                }
+                {
+                    const T fm2 = f[-2], fm1 = f[-1], fp1 = f[1], fp2 = f[2];
+                    D[2][c] = mk.pz ? k.d1a[2] * (fp1 - fm1) - k.d1b[2] * (fp2 - fm2) : T(0);
+                    Sd[2][c] = mk.pz ? k.d2a[2] * (fp1 + fm1) - k.d2b[2] * (fp2 + fm2) - k.d2c[2] * f0 : T(0);
+                }
+                const T sxy = (uq[c][0] - uq[c][4]) + T(8) * (uq[c][3] - uq[c][1]);
+                const T sxz = (wq[c][0] - wq[c][4]) + T(8) * (wq[c][3] - wq[c][1]);
+                Sd[3][c] = (mk.mx && mk.my) ? k.mix[0] * sxy : T(0);
+                Sd[4][c] = (mk.mx && mk.mz) ? k.mix[1] * sxz : T(0);
+                Sd[5][c] = (mk.my && mk.mz) ? k.mix[2] * mixed16<T>(f, M::HZ, 1) : T(0);
+            }
+            Th<T>::gradient(phi, D, Sd, p, g);
+            const int64_t s = (int64_t)x * YZ + (int64_t)y * p.Z + z;
+            epi(s, N, phi, g);
+            if (DENS) {
+                // FP64 energy and baryon densities of the stage input (stage 1: the field itself),
+                // evaluated after the gradient so their registers do not overlap
+                StencilCoef<double> kd;
+                kd.init(p);
+                double phd[C], Dd[3][C];
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    const int co = c * M::PLANE;
+                    const T* f = P0 + co;
+                    phd[c] = double(f[0]);
+                    const double xd = double(Pp1[co]) - double(Pm1[co]), xd2 = double(Pp2[co]) - double(Pm2[co]);
+                    const double yd = double(f[M::HZ]) - double(f[-M::HZ]);
+                    const double yd2 = double(f[2 * M::HZ]) - double(f[-2 * M::HZ]);
+                    const double zd = double(f[1]) - double(f[-1]), zd2 = double(f[2]) - double(f[-2]);
+                    Dd[0][c] = mk.px ? kd.d1a[0] * xd - kd.d1b[0] * xd2 : 0.0;
+                    Dd[1][c] = mk.py ? kd.d1a[1] * yd - kd.d1b[1] * yd2 : 0.0;
+                    Dd[2][c] = mk.pz ? kd.d1a[2] * zd - kd.d1b[2] * zd2 : 0.0;
+                }
+                ksum_add(esum, Th<double>::energy(phd, Dd, p));
+                ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
+            }
+        }
+        slot = (slot + 1) % 5;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tiling of one lattice into (x-chunk, 8-row y, 32-column z) tiles.
+// ---------------------------------------------------------------------------
+struct MarchGrid {
+    int nz, ny, nx, xc;
+    __host__ __device__ int count() const { return nz * ny * nx; }
+};
+
+template <class M>
+__host__ __device__ inline MarchGrid march_grid(const Params& p, int xc) {
+    MarchGrid g;
+    g.xc = xc;
+    g.nz = (p.Z + M::BZ - 1) / M::BZ;
+    g.ny = (p.Y + M::BY - 1) / M::BY;
+    g.nx = (p.X + xc - 1) / xc;
+    return g;
+}
+
+__device__ __forceinline__ void march_origin(const MarchGrid& g, int t, int by, int& xa, int& xe, int& y0, int& z0,
+                                             int X) {
+    const int iz = t % g.nz;
+    const int r = t / g.nz;
+    const int iy = r % g.ny;
+    const int ix = r / g.ny;
+    z0 = iz * 32;
+    y0 = iy * by;
+    xa = ix * g.xc;
+    xe = min(xa + g.xc, X);
+}
+
+// ---------------------------------------------------------------------------
+// Plain reference-layout gradient (drop-in for do_gradient_step_kernel):
+// EG = projected gradient of `field`, l = -dt EG.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct PlainEpi {
+    T* eg;
+    T* l;
+    T mdt;
+    template <int C>
+    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g)[C]) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            eg[c * N + s] = g[c];
+            l[c * N + s] = mdt * g[c];
+        }
+    }
+};
+
+template <template <typename> class Th, class M, typename T>
+__global__ void __launch_bounds__(M::NTHREADS) k_march_plain(Params p, MarchGrid mg, const T* __restrict__ field,
+                                                             T* __restrict__ eg, T* __restrict__ l) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
+    PlainEpi<T> epi{eg, l, T(-p.dt)};
+    const T* const src[3] = {field, nullptr, nullptr};
+    KSum es{0.0, 0.0}, bs{0.0, 0.0};
+    for (int t = blockIdx.x; t < mg.count(); t += gridDim.x) {
+        int xa, xe, y0, z0;
+        march_origin(mg, t, M::BY, xa, xe, y0, z0, p.X);
+        march_tile<Th, M, T, 1, false>(sm, p, src, T(0), T(0), xa, xe, y0, z0, epi, es, bs);
+    }
+}
+
+}  // namespace sky

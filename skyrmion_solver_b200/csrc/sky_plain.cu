@@ -6,6 +6,7 @@
 
 #include "sky_host.h"
 #include "sky_kernels.cuh"
+#include "sky_march.cuh"
 
 namespace sky {
 
@@ -267,9 +268,56 @@ int ew_blocks(int64_t n) {
     return (int)b;
 }
 
+// x-chunk of a marching launch: minimise (waves of tiles over the resident
+// blocks) x (planes a block walks: chunk + 4 halo planes).
+int choose_xc(int X, int tiles_yz, int resident) {
+    int best = X, best_cost = -1;
+    for (int xc = 4; xc <= X; ++xc) {
+        const int nt = tiles_yz * ((X + xc - 1) / xc);
+        const int waves = (nt + resident - 1) / resident;
+        const int cost = waves * (xc + 4);
+        if (best_cost < 0 || cost < best_cost || (cost == best_cost && xc > best)) {
+            best_cost = cost;
+            best = xc;
+        }
+    }
+    return best;
+}
+
+// Library options (sky_set_option): key 0 = kernel family of the
+// reference-layout gradient (1 = marching kernels for C <= 5, 0 = 3-D tile
+// kernels); key 1 = x-chunk of those marching launches (0 = automatic).
+static int g_options[4] = {1, 0, 0, 0};
+int option(int key) { return (key >= 0 && key < 4) ? g_options[key] : 0; }
+
 // ---------------------------------------------------------------------------
 // templated launchers
 // ---------------------------------------------------------------------------
+template <template <typename> class Th, typename T>
+int launch_gradient_march(const Params& p, const T* field, T* eg, T* l, cudaStream_t st) {
+    using M = MarchShape<Th<T>::C, 8>;
+    auto kern = k_march_plain<Th, M, T>;
+    const size_t smem = M::template smem_bytes<T>(1);
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(march gradient)", __LINE__);
+        if (rc) return rc;
+        int n = 0;
+        rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem), "occupancy",
+                        __LINE__);
+        if (rc) return rc;
+        per_sm = n < 1 ? 1 : n;
+    }
+    const int resident = num_sms() * per_sm;
+    const MarchGrid g0 = march_grid<M>(p, p.X);
+    const int xc_opt = option(1);
+    const int xc = xc_opt > 0 ? (xc_opt < p.X ? xc_opt : p.X) : choose_xc(p.X, g0.nz * g0.ny, resident);
+    const MarchGrid mg = march_grid<M>(p, xc);
+    const int blocks = mg.count() < resident ? mg.count() : resident;
+    kern<<<blocks, dim3(M::BZ, M::BY), smem, st>>>(p, mg, field, eg, l);
+    return check_cuda(cudaGetLastError(), "launch march gradient", __LINE__);
+}
 template <template <typename> class Th, typename T, typename S>
 int launch_gradient(const Params& p, const S* field, S* eg, S* l, cudaStream_t st) {
     using Shape = typename GradTile<Th<T>::C, T>::type;
@@ -331,6 +379,10 @@ int launch_density(const Params& p, const S* field, double* dens, double* scratc
 
 template <template <typename> class Th>
 int grad64(const Params& p, const double* f, double* eg, double* l, cudaStream_t st) {
+    if constexpr (Th<double>::C <= 5) {
+        if (option(0) == 1 && (int64_t)p.C * n_sites(p) < ((int64_t)1 << 31))
+            return launch_gradient_march<Th, double>(p, f, eg, l, st);
+    }
     return launch_gradient<Th, double, double>(p, f, eg, l, st);
 }
 template <template <typename> class Th>
@@ -418,7 +470,17 @@ using namespace sky;
 // ===========================================================================
 extern "C" {
 
-const char* sky_version(void) { return "skyrmion_b200 0.1 (sm_100a)"; }
+const char* sky_version(void) { return "skyrmion_b200 0.2 (sm_100a)"; }
+
+int sky_set_option(int key, int value) {
+    if (key == 0 && value != 0 && value != 1) return invalid("option 0 takes 0 (tile kernels) or 1 (marching kernels)");
+    if (key == 1 && value < 0) return invalid("option 1 (x-chunk) must be >= 0");
+    if (key != 0 && key != 1) return invalid("unknown option key");
+    g_options[key] = value;
+    return SKY_OK;
+}
+
+int sky_get_option(int key) { return option(key); }
 const char* sky_last_error(void) { return last_error(); }
 int sky_theory_components(int theory) { return theory_components(theory); }
 int64_t sky_reduce_scratch_size(int64_t n) {

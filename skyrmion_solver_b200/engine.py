@@ -137,6 +137,13 @@ class Engine:
         self._call("sky_engine_set_precision", int(iid), PRECISIONS[precision])
         self.meta[iid]["precision"] = precision
 
+    def retile(self, iid: int, xc: int = 0):
+        """x-chunk of the marching kernels for this instance (0 = automatic)."""
+        self._call("sky_engine_retile", int(iid), int(xc))
+
+    def xc(self, iid: int) -> int:
+        return int(self._lib.sky_engine_get_xc(self._h, int(iid)))
+
     def set_active(self, iid: int, active: bool):
         self._call("sky_engine_set_active", int(iid), 1 if active else 0)
 
