@@ -138,6 +138,24 @@ int sky_arrested_newton_step(int theory, const int32_t* p_i, int32_t n_pi, const
                              double* scratch, int64_t n_scratch, double prev_energy, double* new_energy_host,
                              double* err_host, void* stream);
 
+/* No counterpart in the reference.  The same step as sky_arrested_newton_step
+ * for callers that cannot allocate device memory: a plugin handed only the
+ * field and velocity of a host application whose allocator owns the device
+ * memory, or an interactive loop that must not call cudaMalloc / cudaFree
+ * (they synchronise the device) between frames.  The eight RK4 slopes, the
+ * stage field and the reduction scratch live in a 16 MiB static device array
+ * that every GPU loading the library holds until exit, so the lattice is
+ * limited to C*N <= 232488 values (e.g. 36^3 sites at C = 5); larger lattices
+ * are rejected with SKY_ERR_INVALID before anything is launched.  The array's
+ * device address is looked up on the first call on each device, so make that
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU (other streams, other threads) race.  The slopes are
+ * not returned; velocity, field and energy_gradient are updated as by
+ * sky_arrested_newton_step, and the new energy and err go to host pointers. */
+int sky_arrested_newton_step_noalloc(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                                     double* velocity, double* field, double* energy_gradient, double prev_energy,
+                                     double* new_energy_host, double* err_host, void* stream);
+
 /* ------------------------------------------------------------------------ *
  * Resident batched engine.  No reference counterpart as a single call: it
  * runs the arrested-Newton step of core/integrator.py:284-410 (driven in the
