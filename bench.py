@@ -452,10 +452,10 @@ def run_calibrate(args):
     chunk = 200
     res = {"workload": WORKLOAD, "chunk": chunk, "grad_tol": GRAD_TOL, "rel_energy_tol": REL_ENERGY_TOL}
     hist = {}
-    for prec, cap in (("fp64", args.max_steps), ("fp32", None)):
+    for prec, cap in (("fp64", args.max_steps), ("fp32c", None), ("fp32", None)):
         eng = Engine(0)
         iid = eng.add("omega", (p_i, p_f), field, None, precision=prec)
-        limit = cap if cap else int(1.5 * res["fp64_total_steps"]) + 4 * chunk
+        limit = cap if cap else int(1.2 * res["fp64_total_steps"]) + 4 * chunk
         h = [(0, eng.stats(iid).energy, float("inf"))]
         t0 = time.perf_counter()
         n = 0
@@ -490,13 +490,13 @@ def run_calibrate(args):
                 s = None
         return s
 
-    res["fp64_steps_to_converge"] = settle(hist["fp64"])
-    res["fp32_steps_to_converge"] = settle(hist["fp32"])
-    res["fp32_final_rel_energy_error"] = abs(res["fp32_final_energy"] - e_star) / abs(e_star)
+    for prec in ("fp64", "fp32c", "fp32"):
+        res[f"{prec}_steps_to_converge"] = settle(hist[prec])
+        res[f"{prec}_final_rel_energy_error"] = abs(res[f"{prec}_final_energy"] - e_star) / abs(e_star)
     res["fp64_reached_grad_tol"] = res["fp64_final_max_abs_gradient"] <= GRAD_TOL
     res["history_every"] = chunk * 10
-    res["fp64_history"] = hist["fp64"][::10]
-    res["fp32_history"] = hist["fp32"][::10]
+    for prec in ("fp64", "fp32c", "fp32"):
+        res[f"{prec}_history"] = hist[prec][::10]
     res["command"] = "python bench.py --calibrate"
     os.makedirs(os.path.dirname(CALIBRATION), exist_ok=True)
     out = args.out or CALIBRATION

@@ -170,7 +170,10 @@ int sky_engine_create(int device, void** engine_out);
 int sky_engine_destroy(void* engine);
 
 /* Admit one instance.  precision: 0 = FP32 state and stage arithmetic,
- * 1 = FP64.  field / velocity are FP64 in the reference layout (host pointers,
+ * 1 = FP64, 2 = FP32 stage arithmetic with a compensated field (stored as an
+ * unevaluated FP32 sum hi + lo and updated in FP64 at the end of each step, so
+ * that near convergence updates far below one FP32 ulp still accumulate; the
+ * stencils read hi only).  field / velocity are FP64 in the reference layout (host pointers,
  * or device pointers when on_device != 0); velocity may be NULL (zero).  The
  * energy of the admitted field is evaluated immediately (stats record 0). */
 int sky_engine_add(void* engine, int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
@@ -179,8 +182,9 @@ int sky_engine_add(void* engine, int theory, const int32_t* p_i, int32_t n_pi, c
 /* Retire an instance and free its memory. */
 int sky_engine_remove(void* engine, int id);
 
-/* Change an instance's precision in place (FP32 -> FP64 for the polishing
- * phase); the field, velocity, step count and pending arrest decision carry over. */
+/* Change an instance's precision (0, 1 or 2 as for sky_engine_add) in place,
+ * e.g. to FP64 for the polishing phase; the field, velocity, step count and
+ * pending arrest decision carry over. */
 int sky_engine_set_precision(void* engine, int id, int precision);
 
 /* Re-tile an instance of a marching-kernel theory (C <= 5): x-chunk `xc`

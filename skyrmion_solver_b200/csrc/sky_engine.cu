@@ -19,11 +19,13 @@ constexpr int kGraphSteps = 8;  // steps captured per graph replay
 struct HostInst {
     int id = -1;
     int theory = 0;
-    int prec = 0;  // 0 = FP32 storage/arithmetic, 1 = FP64
+    int prec = 0;  // storage: 0 = FP32 storage/arithmetic, 1 = FP64
+    int comp = 0;  // FP32 storage with a compensated (hi + lo) field
     Params p{};
     int64_t N = 0;
     int C = 0;
     void* F[2] = {nullptr, nullptr};
+    void* Flo[2] = {nullptr, nullptr};
     void* V[2] = {nullptr, nullptr};
     void* L[3] = {nullptr, nullptr, nullptr};
     KSum* epart = nullptr;
@@ -261,6 +263,21 @@ __global__ void k_f64_to_f32(int64_t n, const double* __restrict__ s, float* __r
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         d[i] = float(s[i]);
 }
+// FP64 -> compensated FP32 pair (hi = nearest float, lo = nearest float of the remainder)
+__global__ void k_f64_to_f32c(int64_t n, const double* __restrict__ s, float* __restrict__ hi,
+                              float* __restrict__ lo) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = s[i];
+        const float h = float(v);
+        hi[i] = h;
+        lo[i] = float(v - double(h));
+    }
+}
+__global__ void k_f32c_to_f64(int64_t n, const float* __restrict__ hi, const float* __restrict__ lo,
+                              double* __restrict__ d, int zero) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = zero ? 0.0 : double(hi[i]) + double(lo[i]);
+}
 
 // ---------------------------------------------------------------------------
 // descriptors
@@ -272,6 +289,7 @@ static InstDesc<S> make_desc(const HostInst& h, int tile_begin) {
     d.p = h.p;
     for (int i = 0; i < 2; ++i) {
         d.F[i] = reinterpret_cast<S*>(h.F[i]);
+        d.Flo[i] = reinterpret_cast<S*>(h.Flo[i]);
         d.V[i] = reinterpret_cast<S*>(h.V[i]);
     }
     for (int i = 0; i < 3; ++i) d.L[i] = reinterpret_cast<S*>(h.L[i]);
@@ -355,10 +373,12 @@ static int rebuild_group(Engine& e, Group& g) {
 }
 
 static void free_inst(HostInst& h) {
-    void* ptrs[] = {h.F[0], h.F[1], h.V[0], h.V[1], h.L[0], h.L[1], h.L[2], h.epart, h.bpart, h.gpart, h.stats};
+    void* ptrs[] = {h.F[0], h.F[1], h.Flo[0], h.Flo[1], h.V[0], h.V[1], h.L[0], h.L[1], h.L[2],
+                    h.epart, h.bpart, h.gpart, h.stats};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     memset(h.F, 0, sizeof(h.F));
+    memset(h.Flo, 0, sizeof(h.Flo));
     memset(h.V, 0, sizeof(h.V));
     memset(h.L, 0, sizeof(h.L));
     h.epart = h.bpart = nullptr;
@@ -400,9 +420,20 @@ static int alloc_inst(Engine& e, HostInst& h) {
         free_inst(h);
         return SKY_ERR_NOMEM;
     }
+    if (h.comp) {
+        for (int i = 0; i < 2; ++i) {
+            if (cudaMalloc(&h.Flo[i], fb) != cudaSuccess) {
+                cudaGetLastError();
+                free_inst(h);
+                return SKY_ERR_NOMEM;
+            }
+            cudaMemsetAsync(h.Flo[i], 0, fb, e.stream);
+        }
+    }
     cudaMemsetAsync(h.gpart, 0, sizeof(double) * 2 * h.ntiles, e.stream);
     cudaMemsetAsync(h.stats, 0, sizeof(StepStats) * kStatsCap, e.stream);
-    h.bytes = 7 * fb + (sizeof(KSum) * 2 + sizeof(double) * 2) * h.ntiles + sizeof(StepStats) * kStatsCap;
+    h.bytes = (h.comp ? 9 : 7) * fb + (sizeof(KSum) * 2 + sizeof(double) * 2) * h.ntiles +
+              sizeof(StepStats) * kStatsCap;
     return SKY_OK;
 }
 
@@ -424,6 +455,9 @@ static int upload(Engine& e, HostInst& h, const double* field, const double* vel
         }
         if (h.prec)
             k_convert_in<double><<<ew_blocks(n), 256, 0, e.stream>>>(n, src, reinterpret_cast<double*>(dsts[k]));
+        else if (k == 0 && h.comp)
+            k_f64_to_f32c<<<ew_blocks(n), 256, 0, e.stream>>>(n, src, reinterpret_cast<float*>(h.F[0]),
+                                                              reinterpret_cast<float*>(h.Flo[0]));
         else
             k_convert_in<float><<<ew_blocks(n), 256, 0, e.stream>>>(n, src, reinterpret_cast<float*>(dsts[k]));
         if ((rc = check_cuda(cudaGetLastError(), "convert", __LINE__))) break;
@@ -584,14 +618,16 @@ int sky_engine_add(void* handle, int theory, const int32_t* p_i, int32_t n_pi, c
                    int precision, const double* field, const double* velocity, int on_device, int* id_out) {
     Engine* e = reinterpret_cast<Engine*>(handle);
     if (!e || !id_out || !field) return invalid("null argument");
-    if (precision != 0 && precision != 1) return invalid("precision must be 0 (FP32) or 1 (FP64)");
+    if (precision < 0 || precision > 2)
+        return invalid("precision must be 0 (FP32), 1 (FP64) or 2 (FP32 with a compensated field)");
     cudaSetDevice(e->device);
     HostInst h;
     int rc = pack_params(theory, p_i, n_pi, p_f, n_pf, &h.p);
     if (rc) return rc;
     h.id = e->next_id++;
     h.theory = theory;
-    h.prec = precision;
+    h.prec = precision == 1 ? 1 : 0;
+    h.comp = precision == 2 ? 1 : 0;
     h.N = n_sites(h.p);
     h.C = h.p.C;
     if ((rc = alloc_inst(*e, h))) return rc;
@@ -600,7 +636,7 @@ int sky_engine_add(void* handle, int theory, const int32_t* p_i, int32_t n_pi, c
         return rc;
     }
     e->insts[h.id] = h;
-    Group& g = e->groups[theory][precision];
+    Group& g = e->groups[theory][h.prec];
     g.members.push_back(h.id);
     if ((rc = rebuild_group(*e, g)) || (rc = init_instance(*e, e->insts[h.id], 1))) {
         g.members.pop_back();
@@ -633,8 +669,8 @@ int sky_engine_set_precision(void* handle, int id, int precision) {
     if (!e) return invalid("null engine");
     HostInst* hp = find(e, id);
     if (!hp) return invalid("unknown instance id");
-    if (precision != 0 && precision != 1) return invalid("precision must be 0 or 1");
-    if (hp->prec == precision) return SKY_OK;
+    if (precision < 0 || precision > 2) return invalid("precision must be 0, 1 or 2");
+    if ((hp->comp ? 2 : hp->prec) == precision) return SKY_OK;
     cudaSetDevice(e->device);
     cudaStreamSynchronize(e->stream);
     HostInst& h = *hp;
@@ -656,9 +692,10 @@ int sky_engine_set_precision(void* handle, int id, int precision) {
         }
     }
     HostInst nh = h;
-    nh.prec = precision;
+    nh.prec = precision == 1 ? 1 : 0;
+    nh.comp = precision == 2 ? 1 : 0;
     nh.group_slot = -1;
-    for (int i = 0; i < 2; ++i) nh.F[i] = nh.V[i] = nullptr;
+    for (int i = 0; i < 2; ++i) nh.F[i] = nh.Flo[i] = nh.V[i] = nullptr;
     for (int i = 0; i < 3; ++i) nh.L[i] = nullptr;
     nh.epart = nh.bpart = nullptr;
     nh.gpart = nullptr;
@@ -668,11 +705,24 @@ int sky_engine_set_precision(void* handle, int id, int precision) {
     const int64_t n = (int64_t)h.C * h.N;
     const void* srcs[2] = {h.F[cur], h.V[cur]};
     void* dsts[2] = {nh.F[0], nh.V[0]};
+    const size_t fb = (h.prec ? sizeof(double) : sizeof(float)) * (size_t)n;
     for (int k = 0; k < 2; ++k) {
-        if (precision)
-            k_f32_to_f64<<<ew_blocks(n), 256, 0, e->stream>>>(n, (const float*)srcs[k], (double*)dsts[k]);
-        else
-            k_f64_to_f32<<<ew_blocks(n), 256, 0, e->stream>>>(n, (const double*)srcs[k], (float*)dsts[k]);
+        const bool fieldk = k == 0;
+        if (nh.prec == h.prec) {  // FP32 <-> compensated FP32: the high part carries over
+            cudaMemcpyAsync(dsts[k], srcs[k], fb, cudaMemcpyDeviceToDevice, e->stream);
+        } else if (nh.prec) {     // FP32 (+ low part) -> FP64
+            if (fieldk && h.comp)
+                k_f32c_to_f64<<<ew_blocks(n), 256, 0, e->stream>>>(n, (const float*)srcs[k], (const float*)h.Flo[cur],
+                                                                   (double*)dsts[k], 0);
+            else
+                k_f32_to_f64<<<ew_blocks(n), 256, 0, e->stream>>>(n, (const float*)srcs[k], (double*)dsts[k]);
+        } else {                  // FP64 -> FP32 (+ low part)
+            if (fieldk && nh.comp)
+                k_f64_to_f32c<<<ew_blocks(n), 256, 0, e->stream>>>(n, (const double*)srcs[k], (float*)dsts[k],
+                                                                   (float*)nh.Flo[0]);
+            else
+                k_f64_to_f32<<<ew_blocks(n), 256, 0, e->stream>>>(n, (const double*)srcs[k], (float*)dsts[k]);
+        }
     }
     // carry the stats history
     cudaMemcpyAsync(nh.stats, h.stats, sizeof(StepStats) * kStatsCap, cudaMemcpyDeviceToDevice, e->stream);
@@ -860,7 +910,7 @@ int sky_engine_stats_all(void* handle, int* ids_out, double* out7, int cap, int*
             o[3] = st[i].gabs;
             o[4] = st[i].arrested;
             o[5] = st[i].step;
-            o[6] = hs[i]->prec;
+            o[6] = hs[i]->comp ? 2 : hs[i]->prec;
         }
     }
     *count_out = k;
@@ -895,6 +945,9 @@ int sky_engine_read(void* handle, int id, double* field, double* velocity, int o
         const int zero = (k == 1 && arrested) ? 1 : 0;  // the reference zeroes V on arrest
         if (h->prec)
             k_convert_out<double><<<ew_blocks(n), 256, 0, e->stream>>>(n, (const double*)srcs[k], dst, zero);
+        else if (k == 0 && h->comp)
+            k_f32c_to_f64<<<ew_blocks(n), 256, 0, e->stream>>>(n, (const float*)srcs[k], (const float*)h->Flo[cur],
+                                                               dst, 0);
         else
             k_convert_out<float><<<ew_blocks(n), 256, 0, e->stream>>>(n, (const float*)srcs[k], dst, zero);
         rc = check_cuda(cudaGetLastError(), "convert out", __LINE__);

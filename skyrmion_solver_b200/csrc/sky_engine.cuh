@@ -43,6 +43,7 @@ template <typename S>
 struct InstDesc {
     Params p;
     S* F[2];           // ping-pong field
+    S* Flo[2];         // ping-pong low parts of a compensated FP32 field (null otherwise)
     S* V[2];           // ping-pong velocity
     S* L[3];           // stage slopes l1, l2, l3
     KSum* epart;       // per-tile energy partials (stage 1)
@@ -61,6 +62,95 @@ struct InstDesc {
     int active;        // 0 = skip (retired / paused)
     int cur;           // which half of the F / V ping-pong pairs is current
 };
+
+// RK4 update of one site (core/integrator.py:163-175): V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,
+// F' = F + (k1 + 2 k2 + 2 k3 + k4)/6 = F + dt (V + (l1 + l2 + l3)/6), then the theory's
+// normalisation of the first nsky components and projection of V' orthogonal to them.
+// With a compensated field (Flo_in != null) F is the unevaluated sum hi + lo of two FP32
+// values: the update, the normalisation and the projection run in FP64 and the result is
+// split back into hi + lo, so increments far below one FP32 ulp of F still accumulate.
+template <typename T, typename S, int C>
+__device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __restrict__ F,
+                                              const S* __restrict__ Flo_in, const S* __restrict__ V,
+                                              const S* __restrict__ L1, const S* __restrict__ L2,
+                                              const S* __restrict__ L3, const T (&g)[C], T dtt, int nsky,
+                                              int unit_length, S* __restrict__ Fo, S* __restrict__ Flo_out,
+                                              S* __restrict__ Vo) {
+    T vv[C], inc[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const int64_t j = c * N + s;
+        const T l1 = T(L1[j]), l2 = T(L2[j]), l3 = T(L3[j]), l4 = -dtt * g[c];
+        const T v0 = V ? T(V[j]) : T(0);
+        vv[c] = v0 + (l1 + T(2) * l2 + T(2) * l3 + l4) * T(1.0 / 6.0);
+        inc[c] = dtt * (v0 + (l1 + l2 + l3) * T(1.0 / 6.0));
+    }
+    if (Flo_in == nullptr) {
+        T fv[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) fv[c] = T(F[c * N + s]) + inc[c];
+        if (unit_length) {
+            T ss = T(0);
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) ss += fv[c] * fv[c];
+            ss = sqrt(ss);
+            if (ss != T(0)) {
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                    if (c < nsky) fv[c] /= ss;
+            }
+            T lm = T(0);
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) lm += vv[c] * fv[c];
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) vv[c] -= lm * fv[c];
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            Fo[c * N + s] = S(fv[c]);
+            Vo[c * N + s] = S(vv[c]);
+        }
+    } else {
+        double fd[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const int64_t j = c * N + s;
+            fd[c] = (double(F[j]) + double(Flo_in[j])) + double(inc[c]);
+        }
+        double vd[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) vd[c] = double(vv[c]);
+        if (unit_length) {
+            double ss = 0.0;
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) ss += fd[c] * fd[c];
+            ss = sqrt(ss);
+            if (ss != 0.0) {
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                    if (c < nsky) fd[c] /= ss;
+            }
+            double lm = 0.0;
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) lm += vd[c] * fd[c];
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) vd[c] -= lm * fd[c];
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const S hi = S(fd[c]);
+            Fo[c * N + s] = hi;
+            Flo_out[c * N + s] = S(fd[c] - double(hi));
+            Vo[c * N + s] = S(vd[c]);
+        }
+    }
+}
 
 // Tile loader for X = F + a V + b L (V and/or L optional).
 template <class Shape, typename T, typename S>
@@ -177,45 +267,8 @@ __global__ void __launch_bounds__(Shape::NTHREADS)
                         gmx = fmax(gmx, gd);
                         gab = fmax(gab, fabs(gd));
                     }
-                    // finalize (core/integrator.py:163-175)
-                    const S* L1 = in.L[0];
-                    const S* L2 = in.L[1];
-                    const S* L3 = in.L[2];
-                    T fv[C], vv[C];
-#pragma unroll
-                    for (int c = 0; c < C; ++c) {
-                        const int64_t j = c * N + s;
-                        const T l1 = T(L1[j]), l2 = T(L2[j]), l3 = T(L3[j]), l4 = -dtt * g[c];
-                        const T v0 = V ? T(V[j]) : T(0);
-                        vv[c] = v0 + (l1 + T(2) * l2 + T(2) * l3 + l4) * T(1.0 / 6.0);
-                        fv[c] = T(F[j]) + dtt * (v0 + (l1 + l2 + l3) * T(1.0 / 6.0));
-                    }
-                    if (p.unit_length) {
-                        T ss = T(0);
-#pragma unroll
-                        for (int c = 0; c < C; ++c)
-                            if (c < p.nsky) ss += fv[c] * fv[c];
-                        ss = sqrt(ss);
-                        if (ss != T(0)) {
-#pragma unroll
-                            for (int c = 0; c < C; ++c)
-                                if (c < p.nsky) fv[c] /= ss;
-                        }
-                        T lm = T(0);
-#pragma unroll
-                        for (int c = 0; c < C; ++c)
-                            if (c < p.nsky) lm += vv[c] * fv[c];
-#pragma unroll
-                        for (int c = 0; c < C; ++c)
-                            if (c < p.nsky) vv[c] -= lm * fv[c];
-                    }
-                    S* Fo = in.F[parity ^ 1];
-                    S* Vo = in.V[parity ^ 1];
-#pragma unroll
-                    for (int c = 0; c < C; ++c) {
-                        Fo[c * N + s] = S(fv[c]);
-                        Vo[c * N + s] = S(vv[c]);
-                    }
+                    finalize_site<T, S, C>(s, N, F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2], g, dtt, p.nsky,
+                                           p.unit_length, in.F[parity ^ 1], in.Flo[parity ^ 1], in.V[parity ^ 1]);
                 }
             }
         }
@@ -313,6 +366,8 @@ struct EngineEpi {
     const T* L3;
     T* out0;     // l_STAGE (stages 1-3) or F' (stage 4)
     T* out1;     // V' (stage 4)
+    const T* Flo_in;  // compensated field: low parts in / out (stage 4; null otherwise)
+    T* Flo_out;
     T dtt;
     int nsky;
     int unit_length;
@@ -330,40 +385,7 @@ struct EngineEpi {
             gmx = fmax(gmx, gd);
             gab = fmax(gab, fabs(gd));
         }
-        // core/integrator.py:163-175: V' = V + (l1 + 2 l2 + 2 l3 + l4)/6, F' = F + (k1 + 2k2 + 2k3 + k4)/6
-        T fv[C], vv[C];
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            const int64_t j = c * N + s;
-            const T l1 = L1[j], l2 = L2[j], l3 = L3[j], l4 = -dtt * g[c];
-            const T v0 = V ? V[j] : T(0);
-            vv[c] = v0 + (l1 + T(2) * l2 + T(2) * l3 + l4) * T(1.0 / 6.0);
-            fv[c] = F[j] + dtt * (v0 + (l1 + l2 + l3) * T(1.0 / 6.0));
-        }
-        if (unit_length) {
-            T ss = T(0);
-#pragma unroll
-            for (int c = 0; c < C; ++c)
-                if (c < nsky) ss += fv[c] * fv[c];
-            ss = sqrt(ss);
-            if (ss != T(0)) {
-#pragma unroll
-                for (int c = 0; c < C; ++c)
-                    if (c < nsky) fv[c] /= ss;
-            }
-            T lm = T(0);
-#pragma unroll
-            for (int c = 0; c < C; ++c)
-                if (c < nsky) lm += vv[c] * fv[c];
-#pragma unroll
-            for (int c = 0; c < C; ++c)
-                if (c < nsky) vv[c] -= lm * fv[c];
-        }
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            out0[c * N + s] = fv[c];
-            out1[c * N + s] = vv[c];
-        }
+        finalize_site<T, T, C>(s, N, F, Flo_in, V, L1, L2, L3, g, dtt, nsky, unit_length, out0, Flo_out, out1);
     }
 };
 
@@ -394,6 +416,7 @@ __global__ void __launch_bounds__(M::NTHREADS)
         EngineEpi<T, STAGE> epi{F, V, in.L[0], in.L[1], in.L[2],
                                 STAGE < 4 ? in.L[STAGE - 1] : in.F[parity ^ 1],
                                 STAGE < 4 ? nullptr : in.V[parity ^ 1],
+                                in.Flo[parity], in.Flo[parity ^ 1],
                                 dtt, p.nsky, p.unit_length, -1.0e300, 0.0};
         KSum es{0.0, 0.0}, bs{0.0, 0.0};
         march_tile<Th, M, T, NSRC, STAGE == 1>(sm, p, src, a, b, xa, xe, y0, z0, epi, es, bs);

@@ -6,7 +6,9 @@ skyrmion_solver ``core/integrator.py:284-410`` as fused stage kernels over all
 instances of a theory at once, reduces energies and baryon numbers in FP64
 with compensated summation, takes the arrest decision on the device and
 replays the per-step launches from a CUDA graph.  Instances are FP32
-(``precision="fp32"``, stage arithmetic and state in FP32) or FP64.
+(``precision="fp32"``, stage arithmetic and state in FP32), FP32 with a
+compensated field (``"fp32c"``: the field is an unevaluated FP32 sum hi + lo
+updated in FP64, so sub-ulp updates near convergence are not lost) or FP64.
 """
 from __future__ import annotations
 
@@ -18,7 +20,8 @@ import numpy as np
 from . import _lib
 from ._lib import THEORY_IDS, f64p, i32p
 
-PRECISIONS = {"fp32": 0, "fp64": 1}
+PRECISIONS = {"fp32": 0, "fp64": 1, "fp32c": 2}
+PRECISION_NAMES = {v: k for k, v in PRECISIONS.items()}
 
 
 @dataclass
@@ -173,7 +176,7 @@ class Engine:
         for k in range(cnt.value):
             o = vals[7 * k:7 * k + 7]
             res[int(ids[k])] = StepStats(o[0], o[1], o[2], o[3], bool(o[4]), int(o[5]),
-                                         "fp64" if o[6] else "fp32")
+                                         PRECISION_NAMES.get(int(o[6]), "fp32"))
         return res
 
     def read(self, iid: int, velocity: bool = True):

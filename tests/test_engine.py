@@ -187,3 +187,64 @@ def test_invalid_arguments(engine):
         engine.add("nuclear", (p_i, p_f), F[:, :-1], V)
     with pytest.raises(SkyInvalidArgument):
         engine.remove(10 ** 6)
+
+
+@pytest.mark.parametrize("name", ["nuclear", "omega", "coulomb", "rho"])
+def test_fp32c_engine_tracks_fp64(engine, name):
+    """Compensated FP32 field: FP32 stencils, FP64 update; tracks the FP64 trajectory like FP32 does."""
+    d, F, V, p_i, p_f = _inputs(name)
+    a = engine.add(name, (p_i, p_f), F, V, precision="fp64")
+    b = engine.add(name, (p_i, p_f), F, V, precision="fp32c")
+    try:
+        engine.step(4)
+        sa, sb = engine.stats(a), engine.stats(b)
+        assert sb.precision == "fp32c" or engine.stats_all()[b].precision == "fp32c"
+        assert abs(sa.energy - sb.energy) <= FP32_ENERGY_TOL * abs(sa.energy)
+        fa, _ = engine.read(a)
+        fb, _ = engine.read(b)
+        assert G.rel_err(fb, fa) <= FP32_FIELD_TOL
+    finally:
+        engine.remove(a)
+        engine.remove(b)
+
+
+def test_fp32c_holds_the_field_to_fp64_resolution(engine):
+    """hi + lo keeps an FP64 field to ~2^-48 relative; switching fp64 -> fp32c -> fp64 preserves it."""
+    d, F, V, p_i, p_f = _inputs("omega")
+    i = engine.add("omega", (p_i, p_f), F, V, precision="fp32c")
+    try:
+        f, _ = engine.read(i)
+        assert np.max(np.abs(f - F)) <= 2.0 ** -46 * np.max(np.abs(F))
+        engine.set_precision(i, "fp64")
+        engine.set_precision(i, "fp32c")
+        engine.set_precision(i, "fp32")
+        engine.set_precision(i, "fp32c")
+        f2, _ = engine.read(i)
+        assert np.max(np.abs(f2 - F)) <= 2.0 ** -23 * np.max(np.abs(F))   # the FP32 leg dropped the low parts
+        assert engine.stats_all()[i].precision == "fp32c"
+    finally:
+        engine.remove(i)
+
+
+def test_fp32c_keeps_moving_below_fp32_resolution():
+    """An update far below one FP32 ulp is lost by plain FP32 storage and kept by the compensated field."""
+    from skyrmion_solver_b200.engine import Engine
+    d, F, V, p_i, p_f = _inputs("nuclear")
+    p_f = p_f.copy()
+    p_f[7] = 1e-6            # dt: from rest, the field moves ~1e-10 per step, below FP32 resolution near |phi| = 1
+    V = np.zeros_like(V)
+    with Engine(0) as eng:
+        a = eng.add("nuclear", (p_i, p_f), F, V, precision="fp32")
+        b = eng.add("nuclear", (p_i, p_f), F, V, precision="fp32c")
+        c = eng.add("nuclear", (p_i, p_f), F, V, precision="fp64")
+        eng.step(40)
+        fa, _ = eng.read(a)
+        fb, _ = eng.read(b)
+        fc, _ = eng.read(c)
+    f0 = F.astype(np.float32).astype(np.float64)
+    moved_fp64 = np.max(np.abs(fc - F))
+    assert moved_fp64 > 0
+    # compensated: follows the FP64 trajectory to well below an FP32 ulp
+    assert np.max(np.abs(fb - fc)) <= 0.1 * moved_fp64 + 1e-13
+    # plain FP32: the sub-ulp updates are rounded away (normalisation noise aside)
+    assert np.max(np.abs((fa - f0) - (fc - F))) > np.max(np.abs(fb - fc))
