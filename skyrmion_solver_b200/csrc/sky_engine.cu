@@ -82,16 +82,25 @@ constexpr int stage_nsrc() {
     return STAGE == 1 ? 1 : (STAGE == 2 ? 2 : 3);
 }
 
+// Minimum resident blocks per SM the FP32 marching stages are compiled for
+// (__launch_bounds__): 2 or 3, chosen at run time by option 2.  FP64 stages
+// are compiled for one block per SM (their shared memory allows no more).
+template <typename T>
+constexpr int march_minb_lo() {
+    return sizeof(T) == 4 ? 2 : 1;
+}
+static int march_minb_float() { return option(2) == 3 ? 3 : 2; }
+
 // One-time kernel attribute setup (kept out of stream capture); returns the
 // number of resident blocks per SM.
-template <template <typename> class Th, typename T, int STAGE>
-static int stage_setup(int* per_sm_out) {
+template <template <typename> class Th, typename T, int STAGE, int MINB>
+static int stage_setup_b(int* per_sm_out) {
     static int per_sm = 0;
     if (per_sm == 0) {
         int rc, n = 0;
         if constexpr (uses_march<Th>()) {
             using M = MShape<Th, T>;
-            auto kern = k_march_stage<Th, M, T, STAGE>;
+            auto kern = k_march_stage<Th, M, T, STAGE, MINB>;
             const size_t smem = M::template smem_bytes<T>(stage_nsrc<STAGE>());
             rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                             "cudaFuncSetAttribute(march stage)", __LINE__);
@@ -116,9 +125,17 @@ static int stage_setup(int* per_sm_out) {
 }
 
 template <template <typename> class Th, typename T, int STAGE>
-static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
+static int stage_setup(int* per_sm_out) {
+    if constexpr (sizeof(T) == 4 && uses_march<Th>()) {
+        if (march_minb_float() == 3) return stage_setup_b<Th, T, STAGE, 3>(per_sm_out);
+    }
+    return stage_setup_b<Th, T, STAGE, march_minb_lo<T>()>(per_sm_out);
+}
+
+template <template <typename> class Th, typename T, int STAGE, int MINB>
+static int launch_stage_b(const Group& g, int t_begin, int t_end, cudaStream_t st) {
     int per_sm = 1;
-    int rc = stage_setup<Th, T, STAGE>(&per_sm);
+    int rc = stage_setup_b<Th, T, STAGE, MINB>(&per_sm);
     if (rc) return rc;
     int n = t_end - t_begin;
     if (n <= 0) return SKY_OK;
@@ -127,7 +144,8 @@ static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st)
     if constexpr (uses_march<Th>()) {
         using M = MShape<Th, T>;
         const size_t smem = M::template smem_bytes<T>(stage_nsrc<STAGE>());
-        k_march_stage<Th, M, T, STAGE><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(d, g.d_tile_inst, t_begin, t_end);
+        k_march_stage<Th, M, T, STAGE, MINB><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(d, g.d_tile_inst, t_begin,
+                                                                                      t_end);
     } else {
         using Shape = EShape<Th, T>;
         const size_t smem = Shape::template smem_bytes<T>();
@@ -135,6 +153,14 @@ static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st)
                                                                                                 t_begin, t_end);
     }
     return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
+}
+
+template <template <typename> class Th, typename T, int STAGE>
+static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
+    if constexpr (sizeof(T) == 4 && uses_march<Th>()) {
+        if (march_minb_float() == 3) return launch_stage_b<Th, T, STAGE, 3>(g, t_begin, t_end, st);
+    }
+    return launch_stage_b<Th, T, STAGE, march_minb_lo<T>()>(g, t_begin, t_end, st);
 }
 
 template <template <typename> class Th, typename T>

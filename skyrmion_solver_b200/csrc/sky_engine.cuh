@@ -389,8 +389,8 @@ struct EngineEpi {
     }
 };
 
-template <template <typename> class Th, class M, typename T, int STAGE>
-__global__ void __launch_bounds__(M::NTHREADS)
+template <template <typename> class Th, class M, typename T, int STAGE, int MINB>
+__global__ void __launch_bounds__(M::NTHREADS, MINB)
     k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
     constexpr int NSRC = STAGE == 1 ? 1 : (STAGE == 2 ? 2 : 3);
     extern __shared__ __align__(16) unsigned char smraw[];

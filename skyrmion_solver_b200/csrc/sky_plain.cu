@@ -286,8 +286,9 @@ int choose_xc(int X, int tiles_yz, int resident) {
 
 // Library options (sky_set_option): key 0 = kernel family of the
 // reference-layout gradient (1 = marching kernels for C <= 5, 0 = 3-D tile
-// kernels); key 1 = x-chunk of those marching launches (0 = automatic).
-static int g_options[4] = {1, 0, 0, 0};
+// kernels); key 1 = x-chunk of those marching launches (0 = automatic); key 2
+// = resident blocks per SM the engine's FP32 marching stages are compiled for.
+static int g_options[4] = {1, 0, 2, 0};
 int option(int key) { return (key >= 0 && key < 4) ? g_options[key] : 0; }
 
 // ---------------------------------------------------------------------------
@@ -475,7 +476,8 @@ const char* sky_version(void) { return "skyrmion_b200 0.2 (sm_100a)"; }
 int sky_set_option(int key, int value) {
     if (key == 0 && value != 0 && value != 1) return invalid("option 0 takes 0 (tile kernels) or 1 (marching kernels)");
     if (key == 1 && value < 0) return invalid("option 1 (x-chunk) must be >= 0");
-    if (key != 0 && key != 1) return invalid("unknown option key");
+    if (key == 2 && value != 2 && value != 3) return invalid("option 2 (FP32 stage blocks per SM) takes 2 or 3");
+    if (key < 0 || key > 2) return invalid("unknown option key");
     g_options[key] = value;
     return SKY_OK;
 }
