@@ -13,11 +13,14 @@ One bench step is one arrested-Newton step (four fused gradient stages, the RK4
 update with projection onto S^3, FP64 energy / baryon reductions and the
 device-side arrest decision) of the resident engine, replayed from CUDA graphs.
 
-The headline unit is converged solves/s: the measured step rate divided by the
-number of steps this solve needs before its energy stays within 1e-6 relative
-of the converged plain-FP64 energy (gradient max-norm <= 1e-6).  That step count
-is measured on the GPU by ``python bench.py --calibrate`` and kept in
-``profiles/convergence_omega_B4_128.json``; without it the value is null.
+The headline unit is converged solves/s of the schedule the engine serves with:
+compensated FP32 steps until the gradient max-norm stops improving, then FP64
+steps, until the energy stays within 1e-6 relative of the converged plain-FP64
+energy (the FP64 solve run to gradient max-norm <= 1e-6).  A solve takes
+S32 * t32 + S64 * t64, with the step times t32 (the timed K steps) and t64
+(the FP64 engine) measured in this run and the step counts S32, S64 measured on
+the GPU by ``python bench.py --calibrate`` (``profiles/convergence_omega_B4_128.json``);
+without that file the value is null.
 
 Usage::
 
@@ -47,6 +50,7 @@ CALIBRATION = os.path.join(ROOT, "profiles", "convergence_omega_B4_128.json")
 TRAFFIC = os.path.join(ROOT, "profiles", "ncu_engine_stages_omega128_fp32.md")
 L = 128
 H = 0.15
+FAST = "fp32c"   # precision of the timed steps (the FP32 phase of the schedule)
 DT_FACTOR = 0.2
 COUPLINGS = dict(f_pi=139.8, m_pi=43.91, m_omega=249.5, beta_omega=8.036)
 INIT = {"mode": "rational_map", "baryon_number": 4, "scale": 2.0, "vacuum_shell": 2}
@@ -293,7 +297,7 @@ def run_ours(args):
     cal = load_calibration()
 
     eng = Engine(local)
-    iid = eng.add("omega", (p_i, p_f), field, None, precision="fp32")
+    iid = eng.add("omega", (p_i, p_f), field, None, precision=FAST)
     stream = torch.cuda.ExternalStream(eng.stream, device=dev)
 
     def barrier():
@@ -327,10 +331,10 @@ def run_ours(args):
     # per-launch-kind timing (CUDA events on the engine stream, un-captured launches)
     stages = eng.time_stages(max(5, min(50, K)))
     dom = max(("stage1", "stage2", "stage3", "stage4"), key=lambda k: stages[k])
-    alg_bytes = STAGE_PASSES[dom] * C * 4 * N
+    alg_bytes = (STAGE_PASSES[dom] + (2 if dom == "stage4" else 0)) * C * 4 * N   # stage 4 also moves the low parts
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (stages[dom] * 1e-3) / 1e9
-    step_bytes = 16 * C * 4 * N
+    step_bytes = 18 * C * 4 * N   # 16 passes + the low parts of the compensated field in stage 4
     traffic = load_traffic(dom)
 
     # plain FP64 drop-in path (reference layout, sky_arrested_newton_step) on the same field
@@ -366,47 +370,62 @@ def run_ours(args):
     eng64_ms = a0.elapsed_time(a1) / max(8, min(64, K))
     e64.close()
 
-    # end to end through the public API: pinned host field in, per-step (E, B, err) out, field out
+    # end to end through the public API: pinned host field in, per-step (E, B, err) out, field out,
+    # for both phases of the schedule (compensated FP32, then FP64 after set_precision)
     host = torch.empty(C * N, dtype=torch.float64, pin_memory=True)
     host.copy_(field)
     host_np = host.numpy().reshape((C, L, L, L))
     out_np = np.empty_like(host_np)
+    K64 = max(8, min(64, K))
     barrier()
     tw0 = time.perf_counter()
     ee = Engine(local)
-    j = ee.add("omega", (p_i, p_f), host_np, None, precision="fp32")
+    j = ee.add("omega", (p_i, p_f), host_np, None, precision=FAST)
     for _ in range(K):
         ee.step(1)
         ee.stats(j)
-    ee._call("sky_engine_read", j, __import__("ctypes").c_void_p(out_np.ctypes.data), None, 0)
     tw1 = time.perf_counter()
+    ee.set_precision(j, "fp64")
+    tw2 = time.perf_counter()
+    for _ in range(K64):
+        ee.step(1)
+        ee.stats(j)
+    ee._call("sky_engine_read", j, __import__("ctypes").c_void_p(out_np.ctypes.data), None, 0)
+    tw3 = time.perf_counter()
     ee.close()
-    e2e_s = tw1 - tw0
+    e2e = torch.tensor([tw1 - tw0, tw3 - tw2], dtype=torch.float64)
     if pg is not None:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e = e2e.to(dev)
+        pg.all_reduce(e2e, op=pg.ReduceOp.MAX)
+    e2e32_ms = float(e2e[0]) * 1e3 / K          # includes the admission upload
+    e2e64_ms = float(e2e[1]) * 1e3 / K64         # includes the final field download
     field_bytes = C * N * 8
-    s32 = cal["fp32_steps_to_converge"] if cal else None
-    s64 = cal["fp64_steps_to_converge"] if cal else None
+    s32 = cal.get("mixed_fp32_steps") if cal else None
+    s64p = cal.get("mixed_fp64_steps") if cal else None
+    s64 = cal.get("fp64_steps_to_converge") if cal else None
+    have = s32 is not None and s64p is not None
 
-    def solves(sps, s):
-        return world * sps / s if s else None
-
-    value = solves(steps_per_s, s32)
-    e2e_value = solves(K / e2e_s, s32)
-    plain_value = solves(1e3 / plain_ms, s64)
+    solve_s = (s32 * ms_step + s64p * eng64_ms) * 1e-3 if have else None
+    value = world / solve_s if have else None
+    e2e_solve_s = (s32 * e2e32_ms + s64p * e2e64_ms) * 1e-3 if have else None
+    e2e_value = world / e2e_solve_s if have else None
+    plain_value = world / (s64 * plain_ms * 1e-3) if s64 else None
+    eng64_value = world / (s64 * eng64_ms * 1e-3) if s64 else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "theory": "omega (C=5)", "sites": N, "instances_per_gpu": 1,
-                   "precision": "fp32 state and stencils, fp64 compensated energy/baryon/arrest",
+                   "precision": "timed steps: FP32 stencils with a compensated (hi+lo) FP32 field, FP64 "
+                                "compensated energy/baryon/arrest; schedule: that until max|g| stalls, then FP64",
                    "dt": DT_FACTOR * H, "couplings": COUPLINGS,
-                   "steps_to_converge": s32, "convergence": f"energy within {REL_ENERGY_TOL:g} rel. of the "
-                   f"plain-FP64 energy at max|g| <= {GRAD_TOL:g} (profiles/convergence_omega_B4_128.json)",
-                   "l2": f"no flush: resident state {7 * C * N * 4 / 1e6:.0f} MB > 126 MB L2",
+                   "steps_to_converge": {"fp32c": s32, "fp64_polish": s64p, "plain_fp64": s64},
+                   "convergence": f"energy stays within {REL_ENERGY_TOL:g} rel. of the plain-FP64 energy at "
+                                  f"max|g| <= {GRAD_TOL:g} (profiles/convergence_omega_B4_128.json)",
+                   "l2": f"no flush: resident state {9 * C * N * 4 / 1e6:.0f} MB > 126 MB L2",
                    "parallelism": f"replicas x{world}"},
+        "latency_s": {"p50": solve_s, "p99": solve_s, "note": "one resident solve per GPU: every solve takes "
+                      "the same time; the serving mode (--serve) reports p50/p99 over a request stream"},
         "site_steps_per_s": world * N * steps_per_s,
         "hbm_gbs_step": step_bytes / (ms_step * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "kernel": f"k_engine_stage<Omega,float,{dom[-1]}>", "achieved": achieved,
@@ -414,18 +433,20 @@ def run_ours(args):
                      "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
                      "launch_ms": stages[dom], "stage_ms": stages},
         "plain_fp64": {"ms_per_step": plain_ms, "solves_per_s": plain_value, "steps_to_converge": s64,
-                       "engine_fp64_ms_per_step": eng64_ms,
+                       "engine_fp64_ms_per_step": eng64_ms, "engine_fp64_solves_per_s": eng64_value,
                        "speedup": (value / plain_value) if (value and plain_value) else None},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": field_bytes / K,
-                "d2h_bytes_per_step": (48 * K + field_bytes) / K, "ms_per_step": e2e_s * 1e3 / K,
-                "path": "Engine.add(pinned host field) + K x (Engine.step(1) + Engine.stats) + field read"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": field_bytes / (K + K64),
+                "d2h_bytes_per_step": (48 * (K + K64) + field_bytes) / (K + K64),
+                "ms_per_step": {"fp32c": e2e32_ms, "fp64": e2e64_ms},
+                "path": "Engine.add(pinned host FP64 field) + K x (Engine.step(1) + Engine.stats) + "
+                        "set_precision(fp64) + K64 x (step + stats) + field read"},
         "gpu_launches": launches,
         "clocks": clk,
         "final": {"energy": st.energy, "baryon": st.baryon, "max_abs_gradient": st.gabs, "step": st.step},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline()
-        cval = cb["site_steps_per_s"] / N / s64 if s64 else None
+        cval = cb["site_steps_per_s"] / N / s64 if s64 else None   # the CPU arm runs the plain FP64 schedule
         line["cpu_baseline"] = {"value": cval, "unit": UNIT, "cores": cb["cores"], "kind": "port",
                                 "sample": cb["sample"], "site_steps_per_s": cb["site_steps_per_s"]}
     eng.close()
@@ -442,9 +463,16 @@ def run_ours(args):
 # ---------------------------------------------------------------------------
 
 def run_calibrate(args):
-    import numpy as np
+    """Steps to converge: the plain FP64 solve and the mixed schedule the engine serves with.
+
+    fp64:  FP64 engine steps until max|g| <= GRAD_TOL; its final energy is E*.
+    mixed: compensated FP32 until max|g| stops improving (the serving loop's
+           plateau rule), then FP64 until max|g| <= GRAD_TOL.
+    For each, the step after which |E - E*| <= REL_ENERGY_TOL |E*| holds to the end.
+    """
     import torch
     from skyrmion_solver_b200.engine import Engine
+    from skyrmion_solver_b200.serving import PlateauRule
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
     th, p, p_i, p_f = workload_params()
@@ -452,37 +480,46 @@ def run_calibrate(args):
     chunk = 200
     res = {"workload": WORKLOAD, "chunk": chunk, "grad_tol": GRAD_TOL, "rel_energy_tol": REL_ENERGY_TOL}
     hist = {}
-    for prec, cap in (("fp64", args.max_steps), ("fp32c", None), ("fp32", None)):
+    for sched in ("fp64", "mixed"):
         eng = Engine(0)
-        iid = eng.add("omega", (p_i, p_f), field, None, precision=prec)
-        limit = cap if cap else int(1.2 * res["fp64_total_steps"]) + 4 * chunk
-        h = [(0, eng.stats(iid).energy, float("inf"))]
+        iid = eng.add("omega", (p_i, p_f), field, None, precision="fp64" if sched == "fp64" else "fp32c")
+        rule = PlateauRule()
+        prec = "fp64" if sched == "fp64" else "fp32c"
+        switch = None
+        h = [(0, eng.stats(iid).energy, float("inf"), prec)]
         t0 = time.perf_counter()
         n = 0
-        while n < limit:
+        while n < args.max_steps:
             eng.step(chunk)
             n += chunk
             st = eng.stats(iid)
-            h.append((n, st.energy, st.gabs))
+            h.append((n, st.energy, st.gabs, prec))
             if not math.isfinite(st.energy):
                 break
-            if prec == "fp64" and st.gabs <= GRAD_TOL:
-                break
+            if prec == "fp64":
+                if st.gabs <= GRAD_TOL:
+                    break
+            elif rule.update(st.gabs, chunk):
+                eng.set_precision(iid, "fp64")
+                prec = "fp64"
+                switch = n
         secs = time.perf_counter() - t0
         eng.close()
-        hist[prec] = h
-        res[f"{prec}_total_steps"] = n
-        res[f"{prec}_seconds"] = secs
-        res[f"{prec}_final_energy"] = h[-1][1]
-        res[f"{prec}_final_max_abs_gradient"] = h[-1][2]
-        print(json.dumps({"phase": prec, "steps": n, "secs": secs, "E": h[-1][1], "gabs": h[-1][2]}), flush=True)
+        hist[sched] = h
+        res[f"{sched}_total_steps"] = n
+        res[f"{sched}_switch_step"] = switch
+        res[f"{sched}_seconds"] = secs
+        res[f"{sched}_final_energy"] = h[-1][1]
+        res[f"{sched}_final_max_abs_gradient"] = h[-1][2]
+        print(json.dumps({"schedule": sched, "steps": n, "switch": switch, "secs": secs, "E": h[-1][1],
+                          "gabs": h[-1][2]}), flush=True)
     e_star = res["fp64_final_energy"]
     res["reference_energy"] = e_star
 
-    def settle(h):
+    def settle(hh):
         """First recorded step after which |E - E*| <= tol |E*| holds to the end of the run."""
         s = None
-        for n, e, _ in h:
+        for n, e, _, _ in hh:
             if abs(e - e_star) <= REL_ENERGY_TOL * abs(e_star):
                 if s is None:
                     s = n
@@ -490,13 +527,19 @@ def run_calibrate(args):
                 s = None
         return s
 
-    for prec in ("fp64", "fp32c", "fp32"):
-        res[f"{prec}_steps_to_converge"] = settle(hist[prec])
-        res[f"{prec}_final_rel_energy_error"] = abs(res[f"{prec}_final_energy"] - e_star) / abs(e_star)
+    for sched in ("fp64", "mixed"):
+        s = settle(hist[sched])
+        res[f"{sched}_steps_to_converge"] = s
+        res[f"{sched}_final_rel_energy_error"] = abs(res[f"{sched}_final_energy"] - e_star) / abs(e_star)
+    sw = res["mixed_switch_step"]
+    s_mix = res["mixed_steps_to_converge"]
+    if s_mix is not None:
+        res["mixed_fp32_steps"] = min(s_mix, sw) if sw is not None else s_mix
+        res["mixed_fp64_steps"] = max(0, s_mix - sw) if sw is not None else 0
     res["fp64_reached_grad_tol"] = res["fp64_final_max_abs_gradient"] <= GRAD_TOL
     res["history_every"] = chunk * 10
-    for prec in ("fp64", "fp32c", "fp32"):
-        res[f"{prec}_history"] = hist[prec][::10]
+    for sched in ("fp64", "mixed"):
+        res[f"{sched}_history"] = hist[sched][::10]
     res["command"] = "python bench.py --calibrate"
     os.makedirs(os.path.dirname(CALIBRATION), exist_ok=True)
     out = args.out or CALIBRATION

@@ -48,6 +48,7 @@ struct Group {
     int* d_tile_inst = nullptr;
     int desc_cap = 0, tile_cap = 0;
     int ntiles = 0;
+    bool any_comp = false;  // holds a compensated-field instance (stage 1 stages the low parts too)
 };
 
 struct Engine {
@@ -155,8 +156,39 @@ static int launch_stage_b(const Group& g, int t_begin, int t_end, cudaStream_t s
     return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
 }
 
+// Stage 1 of a group that holds compensated-field instances: the low parts are
+// staged beside the high parts so the FP64 densities see hi + lo.
+template <template <typename> class Th, int MINB>
+static int launch_stage1_lo(const Group& g, int t_begin, int t_end, cudaStream_t st) {
+    using M = MShape<Th, float>;
+    auto kern = k_march_stage<Th, M, float, 1, MINB, true>;
+    const size_t smem = M::template smem_bytes<float>(2, true);
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(march stage 1, compensated)", __LINE__);
+        if (rc) return rc;
+        int n = 0;
+        rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem), "occupancy",
+                        __LINE__);
+        if (rc) return rc;
+        per_sm = n < 1 ? 1 : n;
+    }
+    const int n = t_end - t_begin;
+    if (n <= 0) return SKY_OK;
+    const int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
+    kern<<<blocks, dim3(M::BZ, M::BY), smem, st>>>(reinterpret_cast<InstDesc<float>*>(g.d_desc), g.d_tile_inst,
+                                                   t_begin, t_end);
+    return check_cuda(cudaGetLastError(), "launch march stage 1 (compensated)", __LINE__);
+}
+
 template <template <typename> class Th, typename T, int STAGE>
 static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
+    if constexpr (STAGE == 1 && sizeof(T) == 4 && uses_march<Th>()) {
+        if (g.any_comp)
+            return march_minb_float() == 3 ? launch_stage1_lo<Th, 3>(g, t_begin, t_end, st)
+                                           : launch_stage1_lo<Th, 2>(g, t_begin, t_end, st);
+    }
     if constexpr (sizeof(T) == 4 && uses_march<Th>()) {
         if (march_minb_float() == 3) return launch_stage_b<Th, T, STAGE, 3>(g, t_begin, t_end, st);
     }
@@ -351,6 +383,7 @@ static int rebuild_group_t(Engine& e, Group& g) {
     std::vector<InstDesc<S>> descs;
     std::vector<int> tile_inst;
     int tb = 0;
+    g.any_comp = false;
     for (size_t k = 0; k < g.members.size(); ++k) {
         HostInst& h = e.insts[g.members[k]];
         InstDesc<S> d = make_desc<S>(h, tb);
@@ -362,6 +395,7 @@ static int rebuild_group_t(Engine& e, Group& g) {
             d.cur = o.cur;
         }
         h.group_slot = (int)k;
+        if (h.comp) g.any_comp = true;
         descs.push_back(d);
         for (int t = 0; t < h.ntiles; ++t) tile_inst.push_back((int)k);
         tb += h.ntiles;

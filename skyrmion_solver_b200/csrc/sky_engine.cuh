@@ -389,10 +389,12 @@ struct EngineEpi {
     }
 };
 
-template <template <typename> class Th, class M, typename T, int STAGE, int MINB>
+// LO (stage 1 only): the group holds compensated instances; their FP64
+// energy / baryon densities are evaluated from hi + lo.
+template <template <typename> class Th, class M, typename T, int STAGE, int MINB, bool LO = false>
 __global__ void __launch_bounds__(M::NTHREADS, MINB)
     k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
-    constexpr int NSRC = STAGE == 1 ? 1 : (STAGE == 2 ? 2 : 3);
+    constexpr int NSRC = STAGE == 1 ? (LO ? 2 : 1) : (STAGE == 2 ? 2 : 3);
     extern __shared__ __align__(16) unsigned char smraw[];
     T* sm = reinterpret_cast<T*>(smraw);
     __shared__ KSum shk[32];
@@ -410,7 +412,7 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
         const T* F = in.F[parity];
         const T* V = in.arrested ? nullptr : in.V[parity];
         const T dtt = T(p.dt), hdt = T(0.5 * p.dt);
-        const T* const src[3] = {F, V, STAGE == 3 ? in.L[0] : in.L[1]};
+        const T* const src[3] = {F, LO ? in.Flo[parity] : V, STAGE == 3 ? in.L[0] : in.L[1]};
         const T a = STAGE == 4 ? dtt : hdt;
         const T b = STAGE == 3 ? T(0.25) * dtt : T(0.5) * dtt;
         EngineEpi<T, STAGE> epi{F, V, in.L[0], in.L[1], in.L[2],
@@ -419,7 +421,8 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
                                 in.Flo[parity], in.Flo[parity ^ 1],
                                 dtt, p.nsky, p.unit_length, -1.0e300, 0.0};
         KSum es{0.0, 0.0}, bs{0.0, 0.0};
-        march_tile<Th, M, T, NSRC, STAGE == 1>(sm, p, src, a, b, xa, xe, y0, z0, epi, es, bs);
+        march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE>, LO>(sm, p, src, a, b, xa, xe, y0, z0, epi, es,
+                                                                         bs);
         if (STAGE == 1) {
             const KSum be = block_ksum(es, shk);
             const KSum bb = block_ksum(bs, shk);

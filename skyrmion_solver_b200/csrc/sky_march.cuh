@@ -34,9 +34,10 @@ struct MarchShape {
     static constexpr int RING = 5;
     static constexpr int NTHREADS = BZ * BY;
     static constexpr int NPER = (SLOT + NTHREADS - 1) / NTHREADS;  // plane elements per thread
+    // ring + staging (+ a second ring for the low parts of a compensated field)
     template <typename T>
-    static constexpr size_t smem_bytes(int nsrc) {
-        return (size_t(RING) + size_t(nsrc)) * SLOT * sizeof(T);
+    static constexpr size_t smem_bytes(int nsrc, bool lo = false) {
+        return (size_t(RING) * (lo ? 2 : 1) + size_t(nsrc)) * SLOT * sizeof(T);
     }
 };
 
@@ -101,6 +102,20 @@ __device__ __forceinline__ void plane_issue(T* __restrict__ stage, const PlaneOf
     cp_async_commit();
 }
 
+// Move the thread's own staged hi / lo elements of a compensated field into two ring slots.
+template <class M, typename T>
+__device__ __forceinline__ void plane_split(T* __restrict__ slot, T* __restrict__ slot_lo, const T* __restrict__ stage) {
+    const int tid = threadIdx.x + M::BZ * threadIdx.y;
+#pragma unroll
+    for (int k = 0; k < M::NPER; ++k) {
+        const int idx = tid + k * M::NTHREADS;
+        if (M::SLOT % M::NTHREADS == 0 || idx < M::SLOT) {
+            slot[idx] = stage[idx];
+            slot_lo[idx] = stage[M::SLOT + idx];
+        }
+    }
+}
+
 // Combine the thread's own staged elements into a ring slot: X = F + a V + b L.
 template <class M, int NSRC, typename T>
 __device__ __forceinline__ void plane_combine(T* __restrict__ slot, const T* __restrict__ stage, T a, T b) {
@@ -127,15 +142,19 @@ __device__ __forceinline__ T diff5(const T* f, int st) {
 // One tile: planes xa-2 .. xe+1 of lattice p through the ring; the point
 // physics Th<T> and the epilogue Epi run at every in-lattice site with x in
 // [xa, xe).  DENS adds the FP64 energy / baryon densities of the stage input
-// to esum / bsum (compensated).
+// to esum / bsum (compensated).  LO (with DENS, NSRC = 2): src[1] holds the low
+// parts of a compensated field; the stencils see the high parts and the FP64
+// densities use hi + lo (a null src[1] reads as zero).
 // ---------------------------------------------------------------------------
-template <template <typename> class Th, class M, typename T, int NSRC, bool DENS, class Epi>
+template <template <typename> class Th, class M, typename T, int NSRC, bool DENS, class Epi, bool LO = false>
 __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, const T* const (&src)[3], T a, T b,
                                            int xa, int xe, int y0, int z0, Epi& epi, KSum& esum, KSum& bsum) {
     constexpr int C = M::C;
     static_assert(Th<T>::C == C, "component count mismatch");
+    static_assert(!LO || (DENS && NSRC == 2), "low-part ring only for the stage-1 density");
     T* ring = sm;
     T* stage = sm + M::RING * M::SLOT;
+    T* ring_lo = stage + NSRC * M::SLOT;
     const int64_t N = n_sites(p);
     const int64_t YZ = (int64_t)p.Y * p.Z;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -158,7 +177,10 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     for (int q = q0; q <= q1; ++q) {
         cp_async_wait_all();
         __syncthreads();  // (A) every thread finished the previous centre: slot `slot` is free
-        plane_combine<M, NSRC, T>(ring + slot * M::SLOT, stage, a, b);
+        if (LO)
+            plane_split<M, T>(ring + slot * M::SLOT, ring_lo + slot * M::SLOT, stage);
+        else
+            plane_combine<M, NSRC, T>(ring + slot * M::SLOT, stage, a, b);
         if (q < q1) plane_issue<M, NSRC, T>(stage, po, src, (int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X);
         __syncthreads();  // (B) slot complete
         // arrival: first-difference sums of plane q at (y, z)
@@ -221,15 +243,18 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                 StencilCoef<double> kd;
                 kd.init(p);
                 double phd[C], Dd[3][C];
+                // tap value in FP64: hi, or hi + lo for a compensated field
+                const ptrdiff_t dlo = ring_lo - ring;
+                auto tap = [&](const T* q) -> double { return LO ? double(q[0]) + double(q[dlo]) : double(q[0]); };
 #pragma unroll
                 for (int c = 0; c < C; ++c) {
                     const int co = c * M::PLANE;
                     const T* f = P0 + co;
-                    phd[c] = double(f[0]);
-                    const double xd = double(Pp1[co]) - double(Pm1[co]), xd2 = double(Pp2[co]) - double(Pm2[co]);
-                    const double yd = double(f[M::HZ]) - double(f[-M::HZ]);
-                    const double yd2 = double(f[2 * M::HZ]) - double(f[-2 * M::HZ]);
-                    const double zd = double(f[1]) - double(f[-1]), zd2 = double(f[2]) - double(f[-2]);
+                    phd[c] = tap(f);
+                    const double xd = tap(Pp1 + co) - tap(Pm1 + co), xd2 = tap(Pp2 + co) - tap(Pm2 + co);
+                    const double yd = tap(f + M::HZ) - tap(f - M::HZ);
+                    const double yd2 = tap(f + 2 * M::HZ) - tap(f - 2 * M::HZ);
+                    const double zd = tap(f + 1) - tap(f - 1), zd2 = tap(f + 2) - tap(f - 2);
                     Dd[0][c] = mk.px ? kd.d1a[0] * xd - kd.d1b[0] * xd2 : 0.0;
                     Dd[1][c] = mk.py ? kd.d1a[1] * yd - kd.d1b[1] * yd2 : 0.0;
                     Dd[2][c] = mk.pz ? kd.d1a[2] * zd - kd.d1b[2] * zd2 : 0.0;

@@ -68,6 +68,26 @@ def instance_bytes(C: int, N: int, precision: str = "fp32") -> int:
     return 7 * es * C * N + 8192 * 48 + (N // 256 + 1) * 48
 
 
+class PlateauRule:
+    """When to leave the FP32 phase: max|g| at or below `switch_tol`, or no improvement
+    by the factor `gain` over `window` steps (the FP32 stencil noise floor)."""
+
+    def __init__(self, switch_tol: float = 0.0, window: int = 2048, gain: float = 0.99):
+        self.switch_tol = switch_tol
+        self.window = window
+        self.gain = gain
+        self.best = math.inf
+        self.since = 0
+
+    def update(self, gabs: float, steps: int) -> bool:
+        if gabs < self.gain * self.best:
+            self.best = gabs
+            self.since = 0
+        else:
+            self.since += steps
+        return gabs <= self.switch_tol or self.since >= self.window
+
+
 @dataclass
 class _Live:
     req: Request
@@ -75,8 +95,7 @@ class _Live:
     precision: str
     admitted: float
     fp32_steps: int = 0
-    best_gabs: float = math.inf
-    stall_chunks: int = 0
+    rule: PlateauRule | None = None
 
 
 class Server:
@@ -89,7 +108,8 @@ class Server:
 
     def __init__(self, engine, mem_cap_bytes: float = 180e9, reserve_bytes: float = 2e9, chunk: int = 64,
                  switch_tol: float = 0.0, plateau_chunks: int = 32, plateau_gain: float = 0.99, polish: bool = True,
-                 keep_fields: bool = True, free_bytes=None, clock=time.perf_counter, sleep=time.sleep):
+                 keep_fields: bool = True, free_bytes=None, clock=time.perf_counter, sleep=time.sleep,
+                 fp32_mode: str = "fp32c"):
         self.engine = engine
         self.mem_cap = float(mem_cap_bytes)
         self.reserve = float(reserve_bytes)
@@ -98,6 +118,7 @@ class Server:
         self.plateau_chunks = int(plateau_chunks)
         self.plateau_gain = float(plateau_gain)
         self.polish = polish
+        self.fp32_mode = fp32_mode   # "fp32c" (compensated field, default) or "fp32"
         self.keep_fields = keep_fields
         self.clock = clock
         self.sleep = sleep
@@ -130,12 +151,14 @@ class Server:
                 break                                   # wait for a retirement to free memory
             self.pending.pop(0)
             try:
-                iid = self.engine.add(req.theory, (req.p_i, req.p_f), req.field, None, precision="fp32")
+                iid = self.engine.add(req.theory, (req.p_i, req.p_f), req.field, None, precision=self.fp32_mode)
             except MemoryError:
                 self.results.append(Result(req.rid, "failed", math.nan, math.nan, math.nan, 0, 0, req.arrival, t,
                                            t))
                 continue
-            self.live[iid] = _Live(req, iid, "fp32", t)
+            self.live[iid] = _Live(req, iid, "fp32", t,
+                                   rule=PlateauRule(self.switch_tol, self.plateau_chunks * self.chunk,
+                                                    self.plateau_gain))
 
     def _retire(self, lv: _Live, st, status: str):
         f = None
@@ -160,12 +183,7 @@ class Server:
                     continue
             else:
                 # FP32 phase: switch to FP64 at switch_tol or when max|g| stops improving
-                if st.gabs < self.plateau_gain * lv.best_gabs:
-                    lv.best_gabs = st.gabs
-                    lv.stall_chunks = 0
-                else:
-                    lv.stall_chunks += 1
-                if st.gabs <= max(self.switch_tol, lv.req.tol) or lv.stall_chunks >= self.plateau_chunks:
+                if lv.rule.update(st.gabs, self.chunk) or st.gabs <= lv.req.tol:
                     self.engine.set_precision(iid, "fp64")
                     lv.precision = "fp64"
                     lv.fp32_steps = st.step

@@ -59,7 +59,7 @@ class FakeEngine:
         self.clock.t += n * self.step_cost * max(1, len(self.insts))
         for v in self.insts.values():
             v["step"] += n
-            floor = self.fp32_floor if v["prec"] == "fp32" else 0.0
+            floor = self.fp32_floor if v["prec"] != "fp64" else 0.0
             v["g"] = max(floor, v["g"] * self.rate ** n)
 
     def stats_all(self):
