@@ -472,7 +472,7 @@ def run_calibrate(args):
     """
     import torch
     from skyrmion_solver_b200.engine import Engine
-    from skyrmion_solver_b200.serving import PlateauRule
+    from skyrmion_solver_b200.serving import PlateauRule, fp32_gradient_floor
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
     th, p, p_i, p_f = workload_params()
@@ -483,7 +483,7 @@ def run_calibrate(args):
     for sched in ("fp64", "mixed"):
         eng = Engine(0)
         iid = eng.add("omega", (p_i, p_f), field, None, precision="fp64" if sched == "fp64" else "fp32c")
-        rule = PlateauRule()
+        rule = PlateauRule(2.0 * fp32_gradient_floor(p_f))
         prec = "fp64" if sched == "fp64" else "fp32c"
         switch = None
         h = [(0, eng.stats(iid).energy, float("inf"), prec)]

@@ -66,29 +66,25 @@ struct InstDesc {
 // RK4 update of one site (core/integrator.py:163-175): V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,
 // F' = F + (k1 + 2 k2 + 2 k3 + k4)/6 = F + dt (V + (l1 + l2 + l3)/6), then the theory's
 // normalisation of the first nsky components and projection of V' orthogonal to them.
-// With a compensated field (Flo_in != null) F is the unevaluated sum hi + lo of two FP32
+// With a compensated field (comp) F is the unevaluated sum hi + lo of two FP32
 // values: the update, the normalisation and the projection run in FP64 and the result is
 // split back into hi + lo, so increments far below one FP32 ulp of F still accumulate.
 template <typename T, typename S, int C>
-__device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __restrict__ F,
-                                              const S* __restrict__ Flo_in, const S* __restrict__ V,
-                                              const S* __restrict__ L1, const S* __restrict__ L2,
-                                              const S* __restrict__ L3, const T (&g)[C], T dtt, int nsky,
-                                              int unit_length, S* __restrict__ Fo, S* __restrict__ Flo_out,
-                                              S* __restrict__ Vo) {
+__device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0)[C], const T (&flo)[C], bool comp,
+                                              const T (&v0)[C], const T (&l1)[C], const T (&l2)[C],
+                                              const T (&l3)[C], const T (&g)[C], T dtt, int nsky, int unit_length,
+                                              S* __restrict__ Fo, S* __restrict__ Flo_out, S* __restrict__ Vo) {
     T vv[C], inc[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
-        const int64_t j = c * N + s;
-        const T l1 = T(L1[j]), l2 = T(L2[j]), l3 = T(L3[j]), l4 = -dtt * g[c];
-        const T v0 = V ? T(V[j]) : T(0);
-        vv[c] = v0 + (l1 + T(2) * l2 + T(2) * l3 + l4) * T(1.0 / 6.0);
-        inc[c] = dtt * (v0 + (l1 + l2 + l3) * T(1.0 / 6.0));
+        const T l4 = -dtt * g[c];
+        vv[c] = v0[c] + (l1[c] + T(2) * l2[c] + T(2) * l3[c] + l4) * T(1.0 / 6.0);
+        inc[c] = dtt * (v0[c] + (l1[c] + l2[c] + l3[c]) * T(1.0 / 6.0));
     }
-    if (Flo_in == nullptr) {
+    if (!comp) {
         T fv[C];
 #pragma unroll
-        for (int c = 0; c < C; ++c) fv[c] = T(F[c * N + s]) + inc[c];
+        for (int c = 0; c < C; ++c) fv[c] = f0[c] + inc[c];
         if (unit_length) {
             T ss = T(0);
 #pragma unroll
@@ -114,15 +110,12 @@ __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __r
             Vo[c * N + s] = S(vv[c]);
         }
     } else {
-        double fd[C];
+        double fd[C], vd[C];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            const int64_t j = c * N + s;
-            fd[c] = (double(F[j]) + double(Flo_in[j])) + double(inc[c]);
+            fd[c] = (double(f0[c]) + double(flo[c])) + double(inc[c]);
+            vd[c] = double(vv[c]);
         }
-        double vd[C];
-#pragma unroll
-        for (int c = 0; c < C; ++c) vd[c] = double(vv[c]);
         if (unit_length) {
             double ss = 0.0;
 #pragma unroll
@@ -150,6 +143,29 @@ __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __r
             Vo[c * N + s] = S(vd[c]);
         }
     }
+}
+
+// finalize_vals with the inputs read from global memory (3-D tile kernels).
+template <typename T, typename S, int C>
+__device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __restrict__ F,
+                                              const S* __restrict__ Flo_in, const S* __restrict__ V,
+                                              const S* __restrict__ L1, const S* __restrict__ L2,
+                                              const S* __restrict__ L3, const T (&g)[C], T dtt, int nsky,
+                                              int unit_length, S* __restrict__ Fo, S* __restrict__ Flo_out,
+                                              S* __restrict__ Vo) {
+    T f0[C], flo[C], v0[C], a1[C], a2[C], a3[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const int64_t j = c * N + s;
+        f0[c] = T(F[j]);
+        flo[c] = Flo_in ? T(Flo_in[j]) : T(0);
+        v0[c] = V ? T(V[j]) : T(0);
+        a1[c] = T(L1[j]);
+        a2[c] = T(L2[j]);
+        a3[c] = T(L3[j]);
+    }
+    finalize_vals<T, S, C>(s, N, f0, flo, Flo_in != nullptr, v0, a1, a2, a3, g, dtt, nsky, unit_length, Fo, Flo_out,
+                           Vo);
 }
 
 // Tile loader for X = F + a V + b L (V and/or L optional).
@@ -359,21 +375,19 @@ __global__ void k_engine_advance(InstDesc<S>* __restrict__ insts, int ninst) {
 // ---------------------------------------------------------------------------
 template <typename T, int STAGE>
 struct EngineEpi {
-    const T* F;
-    const T* V;  // null when the velocity is arrested
-    const T* L1;
-    const T* L2;
-    const T* L3;
-    T* out0;     // l_STAGE (stages 1-3) or F' (stage 4)
-    T* out1;     // V' (stage 4)
-    const T* Flo_in;  // compensated field: low parts in / out (stage 4; null otherwise)
-    T* Flo_out;
+    // stage 4 prefetches F, F_lo, V, l1, l2, l3 of the next site into shared memory
+    static constexpr int NFIN = STAGE == 4 ? 6 : 0;
+    const T* fin_src[6];  // F, F_lo (null unless compensated), V (null when arrested), l1, l2, l3
+    T* out0;              // l_STAGE (stages 1-3) or F' (stage 4)
+    T* out1;              // V' (stage 4)
+    T* Flo_out;           // compensated field: low parts out (stage 4)
     T dtt;
     int nsky;
     int unit_length;
     double gmx, gab;
-    template <int C>
-    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g)[C]) {
+    template <int C, int NT>
+    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g)[C],
+                                               const T* __restrict__ fin) {
         if (STAGE < 4) {
 #pragma unroll
             for (int c = 0; c < C; ++c) out0[c * N + s] = -dtt * g[c];
@@ -385,12 +399,21 @@ struct EngineEpi {
             gmx = fmax(gmx, gd);
             gab = fmax(gab, fabs(gd));
         }
-        finalize_site<T, T, C>(s, N, F, Flo_in, V, L1, L2, L3, g, dtt, nsky, unit_length, out0, Flo_out, out1);
+        T f0[C], flo[C], v0[C], a1[C], a2[C], a3[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            f0[c] = fin[(0 * C + c) * NT];
+            flo[c] = fin[(1 * C + c) * NT];
+            v0[c] = fin[(2 * C + c) * NT];
+            a1[c] = fin[(3 * C + c) * NT];
+            a2[c] = fin[(4 * C + c) * NT];
+            a3[c] = fin[(5 * C + c) * NT];
+        }
+        finalize_vals<T, T, C>(s, N, f0, flo, fin_src[1] != nullptr, v0, a1, a2, a3, g, dtt, nsky, unit_length,
+                               out0, Flo_out, out1);
     }
 };
 
-// LO (stage 1 only): the group holds compensated instances; their FP64
-// energy / baryon densities are evaluated from hi + lo.
 template <template <typename> class Th, class M, typename T, int STAGE, int MINB, bool LO = false>
 __global__ void __launch_bounds__(M::NTHREADS, MINB)
     k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
@@ -415,10 +438,10 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
         const T* const src[3] = {F, LO ? in.Flo[parity] : V, STAGE == 3 ? in.L[0] : in.L[1]};
         const T a = STAGE == 4 ? dtt : hdt;
         const T b = STAGE == 3 ? T(0.25) * dtt : T(0.5) * dtt;
-        EngineEpi<T, STAGE> epi{F, V, in.L[0], in.L[1], in.L[2],
+        EngineEpi<T, STAGE> epi{{F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2]},
                                 STAGE < 4 ? in.L[STAGE - 1] : in.F[parity ^ 1],
                                 STAGE < 4 ? nullptr : in.V[parity ^ 1],
-                                in.Flo[parity], in.Flo[parity ^ 1],
+                                in.Flo[parity ^ 1],
                                 dtt, p.nsky, p.unit_length, -1.0e300, 0.0};
         KSum es{0.0, 0.0}, bs{0.0, 0.0};
         march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE>, LO>(sm, p, src, a, b, xa, xe, y0, z0, epi, es,

@@ -35,9 +35,10 @@ struct MarchShape {
     static constexpr int NTHREADS = BZ * BY;
     static constexpr int NPER = (SLOT + NTHREADS - 1) / NTHREADS;  // plane elements per thread
     // ring + staging (+ a second ring for the low parts of a compensated field)
+    // + nfin per-thread values of C components for the epilogue
     template <typename T>
-    static constexpr size_t smem_bytes(int nsrc, bool lo = false) {
-        return (size_t(RING) * (lo ? 2 : 1) + size_t(nsrc)) * SLOT * sizeof(T);
+    static constexpr size_t smem_bytes(int nsrc, bool lo = false, int nfin = 0) {
+        return ((size_t(RING) * (lo ? 2 : 1) + size_t(nsrc)) * SLOT + size_t(nfin) * C * NTHREADS) * sizeof(T);
     }
 };
 
@@ -144,7 +145,10 @@ __device__ __forceinline__ T diff5(const T* f, int st) {
 // [xa, xe).  DENS adds the FP64 energy / baryon densities of the stage input
 // to esum / bsum (compensated).  LO (with DENS, NSRC = 2): src[1] holds the low
 // parts of a compensated field; the stencils see the high parts and the FP64
-// densities use hi + lo (a null src[1] reads as zero).
+// densities use hi + lo (a null src[1] reads as zero).  When Epi::NFIN > 0 the
+// epilogue's per-site inputs Epi::fin_src[0..NFIN) (C components each; null
+// reads as zero) of site x+1 are copied with cp.async into a per-thread
+// shared-memory area while site x is computed, and handed to the epilogue.
 // ---------------------------------------------------------------------------
 template <template <typename> class Th, class M, typename T, int NSRC, bool DENS, class Epi, bool LO = false>
 __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, const T* const (&src)[3], T a, T b,
@@ -155,6 +159,8 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     T* ring = sm;
     T* stage = sm + M::RING * M::SLOT;
     T* ring_lo = stage + NSRC * M::SLOT;
+    constexpr int NFIN = Epi::NFIN;
+    T* fin = (LO ? ring_lo + M::RING * M::SLOT : ring_lo) + (threadIdx.x + M::BZ * threadIdx.y);
     const int64_t N = n_sites(p);
     const int64_t YZ = (int64_t)p.Y * p.Z;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -236,7 +242,7 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
             }
             Th<T>::gradient(phi, D, Sd, p, g);
             const int64_t s = (int64_t)x * YZ + (int64_t)y * p.Z + z;
-            epi(s, N, phi, g);
+            epi.template operator()<C, M::NTHREADS>(s, N, phi, g, fin);
             if (DENS) {
                 // FP64 energy and baryon densities of the stage input (stage 1: the field itself),
                 // evaluated after the gradient so their registers do not overlap
@@ -262,6 +268,21 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                 ksum_add(esum, Th<double>::energy(phd, Dd, p));
                 ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
             }
+        }
+        if constexpr (NFIN > 0) {
+          if (own && x + 1 >= xa && x + 1 < xe) {
+            // epilogue inputs of the next site, in flight during the next plane's work
+            const int64_t sn = (int64_t)(x + 1) * YZ + (int64_t)y * p.Z + z;
+#pragma unroll
+            for (int k = 0; k < NFIN; ++k) {
+                const T* g0 = epi.fin_src[k];
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                    cp_async<sizeof(T)>(fin + (k * C + c) * M::NTHREADS,
+                                        g0 ? (const void*)(g0 + c * N + sn) : (const void*)src[0], g0 != nullptr);
+            }
+            cp_async_commit();
+          }
         }
         slot = (slot + 1) % 5;
     }
@@ -303,11 +324,12 @@ __device__ __forceinline__ void march_origin(const MarchGrid& g, int t, int by, 
 // ---------------------------------------------------------------------------
 template <typename T>
 struct PlainEpi {
+    static constexpr int NFIN = 0;
     T* eg;
     T* l;
     T mdt;
-    template <int C>
-    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g)[C]) {
+    template <int C, int NT>
+    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g)[C], const T*) {
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             eg[c * N + s] = g[c];

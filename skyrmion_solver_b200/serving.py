@@ -10,8 +10,9 @@ FP64 field) arrive open-loop.  The loop:
   a time (graph-replayed launches, all theories and sizes in the same step);
 * after each chunk reads every instance's latest statistics in one call and
   - switches an FP32 instance to FP64 once its gradient max-norm reaches
-    ``switch_tol`` or has not improved by 1 % over ``plateau_chunks`` chunks
-    (the FP32 stencil noise floor), so the last digits are polished in FP64,
+    ``switch_tol`` (by default twice the estimated FP32 stencil noise floor,
+    ``fp32_gradient_floor``) or has not improved by 1 % over
+    ``plateau_chunks`` chunks, so the last digits are polished in FP64,
   - retires an instance whose FP64 gradient max-norm is at or below ``tol``
     (converged), whose energy is not finite (failed) or that used up
     ``max_steps`` (not converged), reading its field back and freeing its
@@ -68,11 +69,21 @@ def instance_bytes(C: int, N: int, precision: str = "fp32") -> int:
     return 7 * es * C * N + 8192 * 48 + (N // 256 + 1) * 48
 
 
-class PlateauRule:
-    """When to leave the FP32 phase: max|g| at or below `switch_tol`, or no improvement
-    by the factor `gain` over `window` steps (the FP32 stencil noise floor)."""
+def fp32_gradient_floor(p_f) -> float:
+    """Estimated FP32 noise floor of the gradient max-norm on a lattice with spacings p_f[3:6].
 
-    def __init__(self, switch_tol: float = 0.0, window: int = 2048, gain: float = 0.99):
+    The second-difference stencil sums |coefficients| = 16/3 per axis over h^2, and a
+    unit-size field is stored to 2^-24 relative, so an FP32 gradient carries errors
+    of about 2^-24 * sum_i 16 / (3 h_i^2) (4.2e-5 at h = 0.15).
+    """
+    return 2.0 ** -24 * sum(16.0 / (3.0 * float(p_f[k]) ** 2) for k in (3, 4, 5))
+
+
+class PlateauRule:
+    """When to leave the FP32 phase: max|g| at or below `switch_tol` (by default twice the
+    estimated FP32 noise floor), or no improvement by the factor `gain` over `window` steps."""
+
+    def __init__(self, switch_tol: float = 0.0, window: int = 16384, gain: float = 0.99):
         self.switch_tol = switch_tol
         self.window = window
         self.gain = gain
@@ -107,14 +118,15 @@ class Server:
     """
 
     def __init__(self, engine, mem_cap_bytes: float = 180e9, reserve_bytes: float = 2e9, chunk: int = 64,
-                 switch_tol: float = 0.0, plateau_chunks: int = 32, plateau_gain: float = 0.99, polish: bool = True,
+                 switch_tol: float | None = None, plateau_chunks: int = 256, plateau_gain: float = 0.99,
+                 polish: bool = True,
                  keep_fields: bool = True, free_bytes=None, clock=time.perf_counter, sleep=time.sleep,
                  fp32_mode: str = "fp32c"):
         self.engine = engine
         self.mem_cap = float(mem_cap_bytes)
         self.reserve = float(reserve_bytes)
         self.chunk = int(chunk)
-        self.switch_tol = float(switch_tol)
+        self.switch_tol = switch_tol   # None: twice the request's estimated FP32 gradient floor
         self.plateau_chunks = int(plateau_chunks)
         self.plateau_gain = float(plateau_gain)
         self.polish = polish
@@ -157,8 +169,13 @@ class Server:
                                            t))
                 continue
             self.live[iid] = _Live(req, iid, "fp32", t,
-                                   rule=PlateauRule(self.switch_tol, self.plateau_chunks * self.chunk,
+                                   rule=PlateauRule(self._switch_tol(req), self.plateau_chunks * self.chunk,
                                                     self.plateau_gain))
+
+    def _switch_tol(self, req: Request) -> float:
+        if self.switch_tol is not None:
+            return float(self.switch_tol)
+        return 2.0 * fp32_gradient_floor(req.p_f)
 
     def _retire(self, lv: _Live, st, status: str):
         f = None

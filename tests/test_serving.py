@@ -93,7 +93,8 @@ class FakeClock:
 
 def _req(rid, arrival, C=4, L=16, theory="nuclear", tol=1e-6, max_steps=10 ** 6):
     p_i = np.array([L, L, L, 2, 3, C, L ** 3, C * L ** 3, 1, 1, 1], np.int32)
-    return Request(rid, theory, p_i, np.zeros(8), np.zeros((C, L, L, L)), arrival, tol, max_steps)
+    p_f = np.array([0.0, 0.0, 0.0, 0.2, 0.2, 0.2, 0.008, 0.02])
+    return Request(rid, theory, p_i, p_f, np.zeros((C, L, L, L)), arrival, tol, max_steps)
 
 
 def test_all_requests_converge_with_fp64_polish():
@@ -153,6 +154,12 @@ def test_failures_and_step_limit():
     assert res[0].status == "failed"
     assert res[1].status == "not_converged" and res[1].steps >= 640
     assert srv.summary()["converged"] == 0
+
+
+def test_fp32_floor_estimate():
+    from skyrmion_solver_b200.serving import fp32_gradient_floor
+    f = fp32_gradient_floor([0, 0, 0, 0.15, 0.15, 0.15])
+    assert 4.0e-5 < f < 4.5e-5          # the plateau observed for FP32 omega solves at h = 0.15
 
 
 def test_poisson_arrivals_rate():
