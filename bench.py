@@ -549,6 +549,121 @@ def run_calibrate(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# serving: a Poisson request stream, continuous batching vs serial plain FP64
+# ---------------------------------------------------------------------------
+
+SERVE_THEORIES = {"nuclear": {}, "omega": dict(COUPLINGS),
+                  "coulomb": dict(f_pi=105.9, m_pi=138.0, g=4.010, e=0.302822),
+                  "rho": dict(mpi=0.586, mrho=3.29, c_alpha=0.2256)}
+
+
+def serve_requests(n, rate, seed, mix, bmax, max_side, tol, max_steps):
+    """Requests drawn as the serving configuration draws them: theory by weight, B uniform in 1..bmax,
+    side min(max_side, max(48, ceil((48 + 12 B) / 16) * 16)), h = 0.2, dt = 0.2 h, a product of B
+    hedgehogs at seeded positions (minimum separation 2) with Haar-random orientations."""
+    import numpy as np
+    from skyrmion_solver_b200 import theories as T
+    from skyrmion_solver_b200.serving import Request, poisson_arrivals
+    from skyrmion_solver_b200.theories._init_common import build_host_field
+    rng = np.random.default_rng(seed)
+    names = list(mix)
+    w = np.array([mix[k] for k in names], dtype=np.float64)
+    w /= w.sum()
+    arrivals = poisson_arrivals(rate, n, seed)
+    reqs = []
+    for k in range(n):
+        name = names[int(rng.choice(len(names), p=w))]
+        B = int(rng.integers(1, bmax + 1))
+        side = int(min(max_side, max(48, math.ceil((48 + 12 * B) / 16) * 16)))
+        h = 0.2
+        th = T.by_short_name(name)
+        prm = th.params.default_params(xlen=side, ylen=side, zlen=side, lsx=h, lsy=h, lsz=h, xsize=h * (side - 1),
+                                       ysize=h * (side - 1), zsize=h * (side - 1), time_step=0.2 * h,
+                                       **SERVE_THEORIES[name])
+        p_i, p_f = th.params.pack_device_params(prm.resolved())
+        p_i = np.asarray(p_i, np.int32)
+        p_f = np.asarray(p_f, np.float64)
+        cfg = {"mode": "smorgasbord", "count": B, "seed": seed * 1000 + k, "scale": 1.5, "vacuum_shell": 2}
+        f = build_host_field(name, p_i, p_f, cfg)
+        reqs.append((Request(k, name, p_i, p_f, f, float(arrivals[k]), tol, max_steps), prm, th))
+    return reqs
+
+
+def run_serve(args):
+    import numpy as np
+    import torch
+    from skyrmion_solver_b200.core.simulation import Simulation
+    from skyrmion_solver_b200.engine import Engine
+    from skyrmion_solver_b200.serving import Server
+    from skyrmion_solver_b200.theories._init_common import seed_omega
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    mix = dict(kv.split(":") for kv in args.mix.split(","))
+    mix = {k: float(v) for k, v in mix.items()}
+    reqs = serve_requests(args.requests, args.rate, args.seed, mix, args.bmax, args.max_side, GRAD_TOL,
+                          args.max_steps)
+    for r, _, _ in reqs:           # omega: seed the omega component as -c_omega B0, on the device
+        if r.theory == "omega":
+            t = torch.from_numpy(r.field.ravel().copy()).to(dev)
+            seed_omega(t, r.p_i, r.p_f)
+            r.field = t.cpu().numpy().reshape(r.field.shape)
+    # 1. continuous batching on the resident engine
+    with Engine(0) as eng:
+        srv = Server(eng, chunk=64)
+        for r, _, _ in reqs:
+            srv.submit(r)
+        torch.cuda.synchronize()
+        served = {x.rid: x for x in srv.run()}
+        summ = srv.summary()
+    # 2. the same requests solved one after another on the plain FP64 drop-in path
+    serial = {}
+    t_all = 0.0
+    for r, prm, th in reqs:
+        sim = Simulation(prm, th)
+        sim.Field.copy_(torch.from_numpy(r.field.ravel()).to(dev))
+        sim.Velocity.zero_()
+        e = sim.observables()["energy"]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n, status = 0, "not_converged"
+        while n < args.max_steps:
+            e, _ = sim.step(e)
+            n += 1
+            if n % 64 == 0:
+                if not math.isfinite(e):
+                    status = "failed"
+                    break
+                if float(sim.EnergyGradient.abs().max()) <= GRAD_TOL:
+                    status = "converged"
+                    break
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        t_all += dt
+        serial[r.rid] = dict(status=status, steps=n, energy=e, seconds=dt)
+        del sim
+    rel = [abs(served[k].energy - serial[k]["energy"]) / abs(serial[k]["energy"]) for k in served
+           if served[k].status == "converged" and serial[k]["status"] == "converged"]
+    n_serial = sum(v["status"] == "converged" for v in serial.values())
+    serial_sps = n_serial / t_all if t_all > 0 else None
+    line = {"mode": "serve", "metric": METRIC, "unit": UNIT,
+            "config": {"workload": "poisson_stream", "requests": args.requests, "rate_per_s": args.rate,
+                       "mix": mix, "B": f"1..{args.bmax}", "max_side": args.max_side, "h": 0.2, "dt": "0.2 h",
+                       "tol_max_abs_gradient": GRAD_TOL, "schedule": "fp32c until the gradient floor, then fp64"},
+            "served": summ,
+            "serial_plain_fp64": {"converged": n_serial, "seconds": t_all, "solves_per_s": serial_sps},
+            "speedup_solves_per_s": (summ["solves_per_s"] / serial_sps) if (summ["solves_per_s"] and serial_sps)
+            else None,
+            "max_rel_energy_diff_vs_plain_fp64": max(rel) if rel else None,
+            "per_request": [dict(rid=k, theory=reqs[k][0].theory, sites=int(reqs[k][0].p_i[6]),
+                                 served_steps=served[k].steps, fp32_steps=served[k].fp32_steps,
+                                 latency_s=served[k].latency, status=served[k].status,
+                                 serial_steps=serial[k]["steps"], serial_s=serial[k]["seconds"])
+                            for k in sorted(served)]}
+    emit(line)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -559,9 +674,20 @@ def main():
     ap.add_argument("--calibrate", action="store_true")
     ap.add_argument("--max-steps", type=int, default=240000)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--serve", action="store_true", help="serving stream: continuous batching vs serial plain FP64")
+    ap.add_argument("--requests", type=int, default=16)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--mix", default="nuclear:1")
+    ap.add_argument("--bmax", type=int, default=4)
+    ap.add_argument("--max-side", type=int, default=64)
     args = ap.parse_args()
     if args.calibrate:
         return run_calibrate(args)
+    if args.serve:
+        if args.max_steps == 240000:
+            args.max_steps = 60000
+        return run_serve(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
