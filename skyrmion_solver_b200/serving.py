@@ -121,7 +121,7 @@ class Server:
                  switch_tol: float | None = None, plateau_chunks: int = 256, plateau_gain: float = 0.99,
                  polish: bool = True,
                  keep_fields: bool = True, free_bytes=None, clock=time.perf_counter, sleep=time.sleep,
-                 fp32_mode: str = "fp32c"):
+                 fp32_mode: str = "fp32c", tune_cache=None):
         self.engine = engine
         self.mem_cap = float(mem_cap_bytes)
         self.reserve = float(reserve_bytes)
@@ -131,6 +131,7 @@ class Server:
         self.plateau_gain = float(plateau_gain)
         self.polish = polish
         self.fp32_mode = fp32_mode   # "fp32c" (compensated field, default) or "fp32"
+        self.tune_cache = tune_cache  # autotune.TuneCache: re-tile admitted instances with cached choices
         self.keep_fields = keep_fields
         self.clock = clock
         self.sleep = sleep
@@ -168,6 +169,9 @@ class Server:
                 self.results.append(Result(req.rid, "failed", math.nan, math.nan, math.nan, 0, 0, req.arrival, t,
                                            t))
                 continue
+            if self.tune_cache is not None:
+                from .autotune import apply
+                apply(self.engine, iid, req.theory, self.fp32_mode, req.p_i, self.tune_cache, self.engine.device)
             self.live[iid] = _Live(req, iid, "fp32", t,
                                    rule=PlateauRule(self._switch_tol(req), self.plateau_chunks * self.chunk,
                                                     self.plateau_gain))

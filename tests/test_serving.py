@@ -198,3 +198,29 @@ def test_result_same_alone_and_in_mix():
     assert (alone.steps, alone.fp32_steps) == (mix.steps, mix.fp32_steps)
     assert alone.energy == mix.energy and alone.gabs == mix.gabs
     assert np.array_equal(alone.field, mix.field)
+
+
+def test_tune_cache_roundtrip(tmp_path):
+    from skyrmion_solver_b200.autotune import TuneCache, candidate_chunks, shape_key
+    path = str(tmp_path / "tune.json")
+    c = TuneCache(path)
+    p_i = np.array([128, 128, 128, 2, 3, 5, 128 ** 3, 5 * 128 ** 3, 1, 1, 1, 4], np.int32)
+    k = shape_key("omega", "fp32c", p_i, "NVIDIA B200")
+    assert c.get(k) is None
+    c.put(k, {"xc": 32, "ms_per_step": 0.5, "timings": {"32": 0.5}})
+    assert TuneCache(path).get(k)["xc"] == 32
+    ch = candidate_chunks(128)
+    assert 0 in ch and 128 in ch and 32 in ch and all(0 <= x <= 128 for x in ch)
+    assert candidate_chunks(5) == [0, 5]
+
+
+@pytest.mark.gpu
+def test_autotune_picks_a_measured_chunk(tmp_path):
+    from skyrmion_solver_b200 import autotune
+    from tests.test_march import params_for
+    th, p_i, p_f = params_for("omega", (40, 24, 36))
+    cache = autotune.TuneCache(str(tmp_path / "tune.json"))
+    res = autotune.tune("omega", p_i, p_f, "fp32c", cache=cache, steps=4)
+    assert res["xc"] in [int(k) for k in res["timings"]]
+    assert res["ms_per_step"] == min(res["timings"].values())
+    assert autotune.tune("omega", p_i, p_f, "fp32c", cache=cache) == res      # cached
