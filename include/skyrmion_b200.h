@@ -210,6 +210,12 @@ void* sky_engine_stream(void* engine);
  *         max|gradient|, arrested (velocity zeroed for the next step), step]. */
 int sky_engine_stats(void* engine, int id, int64_t step, double* out6);
 
+/* As sky_engine_stats, with out8 = [energy, baryon, err, max|g|, arrested, step,
+ * kinetic energy (1/2) h^3 sum |V|^2 of the velocity the step produced (before any
+ * arrest; with killkinen = 0 this is the RK4 dynamics' kinetic energy),
+ * precision (0, 1 or 2)]. */
+int sky_engine_stats_ex(void* engine, int id, int64_t step, double* out8);
+
 /* Latest statistics of up to `cap` instances: ids_out[k] and out7[7k..7k+6] =
  * [energy, baryon, err, max|g|, arrested, step, precision]; returns the count
  * through *count_out. */

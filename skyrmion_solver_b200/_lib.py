@@ -84,6 +84,7 @@ SIGNATURES = {
     "sky_engine_synchronize": ([_P], _I),
     "sky_engine_stream": ([_P], _P),
     "sky_engine_stats": ([_P, _I, _I64, _F64P], _I),
+    "sky_engine_stats_ex": ([_P, _I, _I64, _F64P], _I),
     "sky_engine_stats_all": ([_P, ctypes.POINTER(_I), _F64P, _I, ctypes.POINTER(_I)], _I),
     "sky_engine_read": ([_P, _I, _P, _P, _I], _I),
     "sky_engine_time_stages": ([_P, _I, _F64P], _I),

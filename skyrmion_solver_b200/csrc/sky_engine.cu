@@ -474,7 +474,7 @@ static int alloc_inst(Engine& e, HostInst& h) {
     }
     if (cudaMalloc(&h.epart, sizeof(KSum) * h.ntiles) != cudaSuccess ||
         cudaMalloc(&h.bpart, sizeof(KSum) * h.ntiles) != cudaSuccess ||
-        cudaMalloc(&h.gpart, sizeof(double) * 2 * h.ntiles) != cudaSuccess ||
+        cudaMalloc(&h.gpart, sizeof(double) * 4 * h.ntiles) != cudaSuccess ||
         cudaMalloc(&h.stats, sizeof(StepStats) * kStatsCap) != cudaSuccess) {
         cudaGetLastError();
         free_inst(h);
@@ -490,9 +490,9 @@ static int alloc_inst(Engine& e, HostInst& h) {
             cudaMemsetAsync(h.Flo[i], 0, fb, e.stream);
         }
     }
-    cudaMemsetAsync(h.gpart, 0, sizeof(double) * 2 * h.ntiles, e.stream);
+    cudaMemsetAsync(h.gpart, 0, sizeof(double) * 4 * h.ntiles, e.stream);
     cudaMemsetAsync(h.stats, 0, sizeof(StepStats) * kStatsCap, e.stream);
-    h.bytes = (h.comp ? 9 : 7) * fb + (sizeof(KSum) * 2 + sizeof(double) * 2) * h.ntiles +
+    h.bytes = (h.comp ? 9 : 7) * fb + (sizeof(KSum) * 2 + sizeof(double) * 4) * h.ntiles +
               sizeof(StepStats) * kStatsCap;
     return SKY_OK;
 }
@@ -835,7 +835,7 @@ int sky_engine_retile(void* handle, int id, int xc) {
     KSum *ep = nullptr, *bp = nullptr;
     double* gp = nullptr;
     if (cudaMalloc(&ep, sizeof(KSum) * ntiles) != cudaSuccess || cudaMalloc(&bp, sizeof(KSum) * ntiles) != cudaSuccess ||
-        cudaMalloc(&gp, sizeof(double) * 2 * ntiles) != cudaSuccess) {
+        cudaMalloc(&gp, sizeof(double) * 4 * ntiles) != cudaSuccess) {
         cudaGetLastError();
         if (ep) cudaFree(ep);
         if (bp) cudaFree(bp);
@@ -851,8 +851,8 @@ int sky_engine_retile(void* handle, int id, int xc) {
     h.epart = ep;
     h.bpart = bp;
     h.gpart = gp;
-    cudaMemsetAsync(h.gpart, 0, sizeof(double) * 2 * ntiles, e->stream);
-    const int64_t dbytes = (int64_t)(sizeof(KSum) * 2 + sizeof(double) * 2) * ((int64_t)ntiles - h.ntiles);
+    cudaMemsetAsync(h.gpart, 0, sizeof(double) * 4 * ntiles, e->stream);
+    const int64_t dbytes = (int64_t)(sizeof(KSum) * 2 + sizeof(double) * 4) * ((int64_t)ntiles - h.ntiles);
     h.bytes += dbytes;
     e->bytes += dbytes;
     h.xc_request = xc;
@@ -939,6 +939,30 @@ int sky_engine_stats(void* handle, int id, int64_t step, double* out6) {
     out6[3] = st.gabs;
     out6[4] = st.arrested;
     out6[5] = st.step;
+    return SKY_OK;
+}
+
+int sky_engine_stats_ex(void* handle, int id, int64_t step, double* out8) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e || !out8) return invalid("null argument");
+    HostInst* h = find(e, id);
+    if (!h) return invalid("unknown instance id");
+    if (step < 0) step = h->steps;
+    if (step > h->steps || h->steps - step >= kStatsCap) return invalid("step outside the retained history");
+    StepStats st;
+    int rc = check_cuda(cudaMemcpyAsync(&st, h->stats + (step % kStatsCap), sizeof(st), cudaMemcpyDeviceToHost,
+                                        e->stream),
+                        "read stats", __LINE__);
+    if (rc) return rc;
+    if ((rc = check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__))) return rc;
+    out8[0] = st.energy;
+    out8[1] = st.baryon;
+    out8[2] = st.err;
+    out8[3] = st.gabs;
+    out8[4] = st.arrested;
+    out8[5] = st.step;
+    out8[6] = st.kinetic;
+    out8[7] = h->comp ? 2 : h->prec;
     return SKY_OK;
 }
 

@@ -35,7 +35,7 @@ struct StepStats {
     double gabs;        // max |g| of step n's stage-4 gradient
     int arrested;       // velocity treated as zero in step n+1
     int step;           // n
-    int pad[2];
+    double kinetic;     // (1/2) h^3 sum |V'|^2 of the velocity step n produced (before any arrest)
 };
 
 // Device-resident state of one instance.
@@ -48,7 +48,7 @@ struct InstDesc {
     S* L[3];           // stage slopes l1, l2, l3
     KSum* epart;       // per-tile energy partials (stage 1)
     KSum* bpart;       // per-tile baryon partials (stage 1)
-    double* gpart;     // per-tile [signed max, abs max] of stage-4 g (2 doubles / tile)
+    double* gpart;     // per-tile [signed max, abs max of stage-4 g, kinetic KSum (s, c)] (4 doubles / tile)
     StepStats* stats;  // ring of per-step records
     int stats_cap;
     int tile_begin;    // first global tile index of this instance
@@ -73,7 +73,8 @@ template <typename T, typename S, int C>
 __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0)[C], const T (&flo)[C], bool comp,
                                               const T (&v0)[C], const T (&l1)[C], const T (&l2)[C],
                                               const T (&l3)[C], const T (&g)[C], T dtt, int nsky, int unit_length,
-                                              S* __restrict__ Fo, S* __restrict__ Flo_out, S* __restrict__ Vo) {
+                                              S* __restrict__ Fo, S* __restrict__ Flo_out, S* __restrict__ Vo,
+                                              double& v2) {
     T vv[C], inc[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
@@ -104,10 +105,12 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
             for (int c = 0; c < C; ++c)
                 if (c < nsky) vv[c] -= lm * fv[c];
         }
+        v2 = 0.0;
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             Fo[c * N + s] = S(fv[c]);
             Vo[c * N + s] = S(vv[c]);
+            v2 += double(vv[c]) * double(vv[c]);
         }
     } else {
         double fd[C], vd[C];
@@ -135,12 +138,14 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
             for (int c = 0; c < C; ++c)
                 if (c < nsky) vd[c] -= lm * fd[c];
         }
+        v2 = 0.0;
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             const S hi = S(fd[c]);
             Fo[c * N + s] = hi;
             Flo_out[c * N + s] = S(fd[c] - double(hi));
             Vo[c * N + s] = S(vd[c]);
+            v2 += double(S(vd[c])) * double(S(vd[c]));
         }
     }
 }
@@ -152,7 +157,7 @@ __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __r
                                               const S* __restrict__ L1, const S* __restrict__ L2,
                                               const S* __restrict__ L3, const T (&g)[C], T dtt, int nsky,
                                               int unit_length, S* __restrict__ Fo, S* __restrict__ Flo_out,
-                                              S* __restrict__ Vo) {
+                                              S* __restrict__ Vo, double& v2) {
     T f0[C], flo[C], v0[C], a1[C], a2[C], a3[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
@@ -165,7 +170,7 @@ __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __r
         a3[c] = T(L3[j]);
     }
     finalize_vals<T, S, C>(s, N, f0, flo, Flo_in != nullptr, v0, a1, a2, a3, g, dtt, nsky, unit_length, Fo, Flo_out,
-                           Vo);
+                           Vo, v2);
 }
 
 // Tile loader for X = F + a V + b L (V and/or L optional).
@@ -234,7 +239,7 @@ __global__ void __launch_bounds__(Shape::NTHREADS)
         __syncthreads();
         StencilCoef<T> k;
         k.init(p);
-        KSum esum{0.0, 0.0}, bsum{0.0, 0.0};
+        KSum esum{0.0, 0.0}, bsum{0.0, 0.0}, ksum{0.0, 0.0};
         double gmx = -1.0e300, gab = 0.0;
         const int z = z0 + threadIdx.x, y = y0 + threadIdx.y;
         if (z < p.Z && y < p.Y) {
@@ -283,8 +288,10 @@ __global__ void __launch_bounds__(Shape::NTHREADS)
                         gmx = fmax(gmx, gd);
                         gab = fmax(gab, fabs(gd));
                     }
+                    double v2;
                     finalize_site<T, S, C>(s, N, F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2], g, dtt, p.nsky,
-                                           p.unit_length, in.F[parity ^ 1], in.Flo[parity ^ 1], in.V[parity ^ 1]);
+                                           p.unit_length, in.F[parity ^ 1], in.Flo[parity ^ 1], in.V[parity ^ 1], v2);
+                    ksum_add(ksum, 0.5 * p.vol * v2);
                 }
             }
         }
@@ -299,9 +306,12 @@ __global__ void __launch_bounds__(Shape::NTHREADS)
         if (STAGE == 4) {
             const double a = block_max(gmx, shm);
             const double b = block_max(gab, shm);
+            const KSum kk = block_ksum(ksum, shk);
             if (threadIdx.x == 0 && threadIdx.y == 0) {
-                in.gpart[2 * lt] = a;
-                in.gpart[2 * lt + 1] = b;
+                in.gpart[4 * lt] = a;
+                in.gpart[4 * lt + 1] = b;
+                in.gpart[4 * lt + 2] = kk.s;
+                in.gpart[4 * lt + 3] = kk.c;
             }
         }
     }
@@ -324,16 +334,18 @@ __global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict_
     InstDesc<S>& in = insts[ii];
     if (!in.active) return;
     const int tid = threadIdx.x;
-    KSum e{0.0, 0.0}, b{0.0, 0.0};
+    KSum e{0.0, 0.0}, b{0.0, 0.0}, kin{0.0, 0.0};
     double gm = -1.0e300, ga = 0.0;
     for (int t = tid; t < in.ntiles; t += blockDim.x) {
         ksum_merge(e, in.epart[t]);
         ksum_merge(b, in.bpart[t]);
-        gm = fmax(gm, in.gpart[2 * t]);
-        ga = fmax(ga, in.gpart[2 * t + 1]);
+        gm = fmax(gm, in.gpart[4 * t]);
+        ga = fmax(ga, in.gpart[4 * t + 1]);
+        ksum_merge(kin, KSum{in.gpart[4 * t + 2], in.gpart[4 * t + 3]});
     }
     KSum E = block_ksum(e, shk);
     KSum B = block_ksum(b, shk);
+    KSum K = block_ksum(kin, shk);
     const double GM = block_max(gm, shm);
     const double GA = block_max(ga, shm);
     if (tid == 0) {
@@ -349,6 +361,7 @@ __global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict_
         st.baryon = B.s + B.c;
         if (mode != 2) {  // a resume keeps the step's gradient statistics
             st.err = (n > 0) ? GM : 0.0;
+            st.kinetic = (n > 0) ? K.s + K.c : 0.0;
             st.gabs = (n > 0) ? GA : 0.0;
         }
         st.arrested = arrest;
@@ -385,6 +398,8 @@ struct EngineEpi {
     int nsky;
     int unit_length;
     double gmx, gab;
+    double hvol;  // h^3 / 2
+    KSum kin;     // (1/2) h^3 sum |V'|^2 over the sites of the tile
     template <int C, int NT>
     __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g)[C],
                                                const T* __restrict__ fin) {
@@ -409,8 +424,10 @@ struct EngineEpi {
             a2[c] = fin[(4 * C + c) * NT];
             a3[c] = fin[(5 * C + c) * NT];
         }
+        double v2;
         finalize_vals<T, T, C>(s, N, f0, flo, fin_src[1] != nullptr, v0, a1, a2, a3, g, dtt, nsky, unit_length,
-                               out0, Flo_out, out1);
+                               out0, Flo_out, out1, v2);
+        ksum_add(kin, hvol * v2);
     }
 };
 
@@ -442,7 +459,7 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
                                 STAGE < 4 ? in.L[STAGE - 1] : in.F[parity ^ 1],
                                 STAGE < 4 ? nullptr : in.V[parity ^ 1],
                                 in.Flo[parity ^ 1],
-                                dtt, p.nsky, p.unit_length, -1.0e300, 0.0};
+                                dtt, p.nsky, p.unit_length, -1.0e300, 0.0, 0.5 * p.vol, KSum{0.0, 0.0}};
         KSum es{0.0, 0.0}, bs{0.0, 0.0};
         march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE>, LO>(sm, p, src, a, b, xa, xe, y0, z0, epi, es,
                                                                          bs);
@@ -457,9 +474,12 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
         if (STAGE == 4) {
             const double ga = block_max(epi.gmx, shm);
             const double gb = block_max(epi.gab, shm);
+            const KSum kk = block_ksum(epi.kin, shk);
             if (threadIdx.x == 0 && threadIdx.y == 0) {
-                in.gpart[2 * lt] = ga;
-                in.gpart[2 * lt + 1] = gb;
+                in.gpart[4 * lt] = ga;
+                in.gpart[4 * lt + 1] = gb;
+                in.gpart[4 * lt + 2] = kk.s;
+                in.gpart[4 * lt + 3] = kk.c;
             }
         }
     }

@@ -33,6 +33,7 @@ class StepStats:
     arrested: bool    # velocity zeroed for the next step
     step: int
     precision: str = ""
+    kinetic: float = 0.0   # (1/2) h^3 sum |V'|^2 after the step (before any arrest)
 
 
 def _theory_id(theory) -> int:
@@ -161,10 +162,10 @@ class Engine:
         return int(self._lib.sky_engine_stream(self._h) or 0)
 
     def stats(self, iid: int, step: int = -1) -> StepStats:
-        out = (ctypes.c_double * 6)()
-        self._call("sky_engine_stats", int(iid), int(step), out)
+        out = (ctypes.c_double * 8)()
+        self._call("sky_engine_stats_ex", int(iid), int(step), out)
         return StepStats(out[0], out[1], out[2], out[3], bool(out[4]), int(out[5]),
-                         self.meta.get(iid, {}).get("precision", ""))
+                         PRECISION_NAMES.get(int(out[7]), ""), out[6])
 
     def stats_all(self) -> dict:
         cap = max(1, len(self.meta))

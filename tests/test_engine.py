@@ -248,3 +248,27 @@ def test_fp32c_keeps_moving_below_fp32_resolution():
     assert np.max(np.abs(fb - fc)) <= 0.1 * moved_fp64 + 1e-13
     # plain FP32: the sub-ulp updates are rounded away (normalisation noise aside)
     assert np.max(np.abs((fa - f0) - (fc - F))) > np.max(np.abs(fb - fc))
+
+
+@pytest.mark.parametrize("name", ["nuclear", "coulomb"])
+def test_rk4_dynamics_and_kinetic_energy(engine, name):
+    """killkinen = 0 (RK4 dynamics, no arrest): trajectory and kinetic energy (1/2) h^3 sum |V|^2 vs the oracle."""
+    d, F, V, p_i, p_f = _inputs(name)
+    p_i = p_i.copy()
+    p_i[8] = 0
+    ref = _oracle_steps(name, F, V, p_i, p_f, 3)
+    iid = engine.add(name, (p_i, p_f), F, V, precision="fp64")
+    try:
+        vol = float(p_f[6])
+        for n in range(1, 4):
+            engine.step(1)
+            st = engine.stats(iid)
+            Fr, Vr, Er, _ = ref[n - 1]
+            assert not st.arrested
+            assert abs(st.energy - Er) <= FP64_TOL * abs(Er)
+            kin = 0.5 * vol * float(np.sum(Vr * Vr))
+            assert abs(st.kinetic - kin) <= FP64_TOL * kin
+        f, v = engine.read(iid)
+        assert G.rel_err(f, ref[2][0]) <= FP64_TOL and G.rel_err(v, ref[2][1]) <= FP64_TOL
+    finally:
+        engine.remove(iid)
