@@ -675,11 +675,11 @@ def main():
     ap.add_argument("--max-steps", type=int, default=240000)
     ap.add_argument("--out", default=None)
     ap.add_argument("--serve", action="store_true", help="serving stream: continuous batching vs serial plain FP64")
-    ap.add_argument("--requests", type=int, default=16)
+    ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--mix", default="nuclear:1")
-    ap.add_argument("--bmax", type=int, default=4)
+    ap.add_argument("--bmax", type=int, default=1)
     ap.add_argument("--max-side", type=int, default=64)
     args = ap.parse_args()
     if args.calibrate:

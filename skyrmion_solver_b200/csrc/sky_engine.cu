@@ -102,7 +102,7 @@ static int stage_setup_b(int* per_sm_out) {
         if constexpr (uses_march<Th>()) {
             using M = MShape<Th, T>;
             auto kern = k_march_stage<Th, M, T, STAGE, MINB>;
-            const size_t smem = M::template smem_bytes<T>(stage_nsrc<STAGE>(), false, STAGE == 4 ? 6 : 0);
+            const size_t smem = M::template smem_bytes<T>(stage_nsrc<STAGE>());
             rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                             "cudaFuncSetAttribute(march stage)", __LINE__);
             if (rc) return rc;
@@ -144,7 +144,7 @@ static int launch_stage_b(const Group& g, int t_begin, int t_end, cudaStream_t s
     InstDesc<T>* d = reinterpret_cast<InstDesc<T>*>(g.d_desc);
     if constexpr (uses_march<Th>()) {
         using M = MShape<Th, T>;
-        const size_t smem = M::template smem_bytes<T>(stage_nsrc<STAGE>(), false, STAGE == 4 ? 6 : 0);
+        const size_t smem = M::template smem_bytes<T>(stage_nsrc<STAGE>());
         k_march_stage<Th, M, T, STAGE, MINB><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(d, g.d_tile_inst, t_begin,
                                                                                       t_end);
     } else {

@@ -388,8 +388,9 @@ __global__ void k_engine_advance(InstDesc<S>* __restrict__ insts, int ninst) {
 // ---------------------------------------------------------------------------
 template <typename T, int STAGE>
 struct EngineEpi {
-    // stage 4 prefetches F, F_lo, V, l1, l2, l3 of the next site into shared memory
-    static constexpr int NFIN = STAGE == 4 ? 6 : 0;
+    // no shared-memory prefetch of the epilogue inputs: prefetching F, V, l1..l3 of the
+    // next site with cp.async measured slower (more instructions, more shared memory)
+    static constexpr int NFIN = 0;
     const T* fin_src[6];  // F, F_lo (null unless compensated), V (null when arrested), l1, l2, l3
     T* out0;              // l_STAGE (stages 1-3) or F' (stage 4)
     T* out1;              // V' (stage 4)
@@ -414,19 +415,9 @@ struct EngineEpi {
             gmx = fmax(gmx, gd);
             gab = fmax(gab, fabs(gd));
         }
-        T f0[C], flo[C], v0[C], a1[C], a2[C], a3[C];
-#pragma unroll
-        for (int c = 0; c < C; ++c) {
-            f0[c] = fin[(0 * C + c) * NT];
-            flo[c] = fin[(1 * C + c) * NT];
-            v0[c] = fin[(2 * C + c) * NT];
-            a1[c] = fin[(3 * C + c) * NT];
-            a2[c] = fin[(4 * C + c) * NT];
-            a3[c] = fin[(5 * C + c) * NT];
-        }
         double v2;
-        finalize_vals<T, T, C>(s, N, f0, flo, fin_src[1] != nullptr, v0, a1, a2, a3, g, dtt, nsky, unit_length,
-                               out0, Flo_out, out1, v2);
+        finalize_site<T, T, C>(s, N, fin_src[0], fin_src[1], fin_src[2], fin_src[3], fin_src[4], fin_src[5], g, dtt,
+                               nsky, unit_length, out0, Flo_out, out1, v2);
         ksum_add(kin, hvol * v2);
     }
 };
