@@ -52,9 +52,6 @@ const char* sky_last_error(void);
  * gradient (sky_gradient_step / sky_arrested_newton_step) for theories with at
  * most five components: 1 = marching x-plane kernels (default), 0 = 3-D tile
  * kernels.  Key 1: x-chunk of those marching launches (0 = automatic).
- * Key 2: resident blocks per SM the engine's FP32 marching stages are built
- * for, 2 (default, no register spills) or 3 (registers capped at 80); takes
- * effect for instances admitted or re-tiled afterwards.
  * Process-wide; not synchronised with launches in flight on other threads. */
 int sky_set_option(int key, int value);
 int sky_get_option(int key);

@@ -49,6 +49,7 @@ struct Group {
     int desc_cap = 0, tile_cap = 0;
     int ntiles = 0;
     bool any_comp = false;  // holds a compensated-field instance (stage 1 stages the low parts too)
+    bool all_wide = true;   // every member can use the wide-row (16-byte staged) kernels
 };
 
 struct Engine {
@@ -75,34 +76,38 @@ constexpr bool uses_march() {
     return Th<float>::C <= 5;
 }
 constexpr int kMarchBY = 8;
-template <template <typename> class Th, typename T>
-using MShape = MarchShape<Th<T>::C, kMarchBY>;
+// Wide-row (16-byte staged) or narrow-row march shape.
+template <template <typename> class Th, typename T, bool WIDE>
+using MShape = MarchShape<Th<T>::C, kMarchBY, WIDE>;
 
 template <int STAGE>
 constexpr int stage_nsrc() {
     return STAGE == 1 ? 1 : (STAGE == 2 ? 2 : 3);
 }
 
-// Minimum resident blocks per SM the FP32 marching stages are compiled for
-// (__launch_bounds__): 2 or 3, chosen at run time by option 2.  FP64 stages
-// are compiled for one block per SM (their shared memory allows no more).
+// Resident blocks per SM the marching stages are compiled for (__launch_bounds__):
+// two for FP32 (registers capped at 128, no spills for C = 5), one for FP64
+// (whose shared memory allows no more).
 template <typename T>
-constexpr int march_minb_lo() {
+constexpr int march_minb() {
     return sizeof(T) == 4 ? 2 : 1;
 }
-static int march_minb_float() { return option(2) == 3 ? 3 : 2; }
+
+// Whether every instance of a group can use the wide-row kernels: Z a multiple of
+// 16 / sizeof(T) (the buffers are cudaMalloc'd, hence 256-byte aligned).
+static bool wide_ok(int prec, int Z) { return Z % (prec ? 2 : 4) == 0; }
 
 // One-time kernel attribute setup (kept out of stream capture); returns the
 // number of resident blocks per SM.
-template <template <typename> class Th, typename T, int STAGE, int MINB>
-static int stage_setup_b(int* per_sm_out) {
+template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false>
+static int stage_setup_w(int* per_sm_out) {
     static int per_sm = 0;
     if (per_sm == 0) {
         int rc, n = 0;
         if constexpr (uses_march<Th>()) {
-            using M = MShape<Th, T>;
-            auto kern = k_march_stage<Th, M, T, STAGE, MINB>;
-            const size_t smem = M::template smem_bytes<T>(stage_nsrc<STAGE>());
+            using M = MShape<Th, T, WIDE>;
+            auto kern = k_march_stage<Th, M, T, STAGE, march_minb<T>(), LO>;
+            const size_t smem = M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
             rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                             "cudaFuncSetAttribute(march stage)", __LINE__);
             if (rc) return rc;
@@ -127,26 +132,23 @@ static int stage_setup_b(int* per_sm_out) {
 
 template <template <typename> class Th, typename T, int STAGE>
 static int stage_setup(int* per_sm_out) {
-    if constexpr (sizeof(T) == 4 && uses_march<Th>()) {
-        if (march_minb_float() == 3) return stage_setup_b<Th, T, STAGE, 3>(per_sm_out);
-    }
-    return stage_setup_b<Th, T, STAGE, march_minb_lo<T>()>(per_sm_out);
+    return stage_setup_w<Th, T, STAGE, true>(per_sm_out);
 }
 
-template <template <typename> class Th, typename T, int STAGE, int MINB>
-static int launch_stage_b(const Group& g, int t_begin, int t_end, cudaStream_t st) {
+template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false>
+static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t st) {
     int per_sm = 1;
-    int rc = stage_setup_b<Th, T, STAGE, MINB>(&per_sm);
+    int rc = stage_setup_w<Th, T, STAGE, WIDE, LO>(&per_sm);
     if (rc) return rc;
     int n = t_end - t_begin;
     if (n <= 0) return SKY_OK;
     const int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
     InstDesc<T>* d = reinterpret_cast<InstDesc<T>*>(g.d_desc);
     if constexpr (uses_march<Th>()) {
-        using M = MShape<Th, T>;
-        const size_t smem = M::template smem_bytes<T>(stage_nsrc<STAGE>());
-        k_march_stage<Th, M, T, STAGE, MINB><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(d, g.d_tile_inst, t_begin,
-                                                                                      t_end);
+        using M = MShape<Th, T, WIDE>;
+        const size_t smem = M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
+        k_march_stage<Th, M, T, STAGE, march_minb<T>(), LO><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(
+            d, g.d_tile_inst, t_begin, t_end);
     } else {
         using Shape = EShape<Th, T>;
         const size_t smem = Shape::template smem_bytes<T>();
@@ -156,43 +158,19 @@ static int launch_stage_b(const Group& g, int t_begin, int t_end, cudaStream_t s
     return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
 }
 
-// Stage 1 of a group that holds compensated-field instances: the low parts are
-// staged beside the high parts so the FP64 densities see hi + lo.
-template <template <typename> class Th, int MINB>
-static int launch_stage1_lo(const Group& g, int t_begin, int t_end, cudaStream_t st) {
-    using M = MShape<Th, float>;
-    auto kern = k_march_stage<Th, M, float, 1, MINB, true>;
-    const size_t smem = M::template smem_bytes<float>(2, true);
-    static int per_sm = 0;
-    if (per_sm == 0) {
-        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                            "cudaFuncSetAttribute(march stage 1, compensated)", __LINE__);
-        if (rc) return rc;
-        int n = 0;
-        rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem), "occupancy",
-                        __LINE__);
-        if (rc) return rc;
-        per_sm = n < 1 ? 1 : n;
-    }
-    const int n = t_end - t_begin;
-    if (n <= 0) return SKY_OK;
-    const int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
-    kern<<<blocks, dim3(M::BZ, M::BY), smem, st>>>(reinterpret_cast<InstDesc<float>*>(g.d_desc), g.d_tile_inst,
-                                                   t_begin, t_end);
-    return check_cuda(cudaGetLastError(), "launch march stage 1 (compensated)", __LINE__);
-}
-
 template <template <typename> class Th, typename T, int STAGE>
 static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
-    if constexpr (STAGE == 1 && sizeof(T) == 4 && uses_march<Th>()) {
-        if (g.any_comp)
-            return march_minb_float() == 3 ? launch_stage1_lo<Th, 3>(g, t_begin, t_end, st)
-                                           : launch_stage1_lo<Th, 2>(g, t_begin, t_end, st);
+    if constexpr (uses_march<Th>()) {
+        // stage 1 of a group with compensated-field instances stages the low parts too
+        // (narrow rows: the second ring would not leave room for two blocks per SM)
+        if constexpr (STAGE == 1 && sizeof(T) == 4) {
+            if (g.any_comp) return launch_stage_w<Th, T, 1, false, true>(g, t_begin, t_end, st);
+        }
+        if (g.all_wide) return launch_stage_w<Th, T, STAGE, true>(g, t_begin, t_end, st);
+        return launch_stage_w<Th, T, STAGE, false>(g, t_begin, t_end, st);
+    } else {
+        return launch_stage_w<Th, T, STAGE, false>(g, t_begin, t_end, st);
     }
-    if constexpr (sizeof(T) == 4 && uses_march<Th>()) {
-        if (march_minb_float() == 3) return launch_stage_b<Th, T, STAGE, 3>(g, t_begin, t_end, st);
-    }
-    return launch_stage_b<Th, T, STAGE, march_minb_lo<T>()>(g, t_begin, t_end, st);
 }
 
 template <template <typename> class Th, typename T>
@@ -384,6 +362,7 @@ static int rebuild_group_t(Engine& e, Group& g) {
     std::vector<int> tile_inst;
     int tb = 0;
     g.any_comp = false;
+    g.all_wide = true;
     for (size_t k = 0; k < g.members.size(); ++k) {
         HostInst& h = e.insts[g.members[k]];
         InstDesc<S> d = make_desc<S>(h, tb);
@@ -396,6 +375,7 @@ static int rebuild_group_t(Engine& e, Group& g) {
         }
         h.group_slot = (int)k;
         if (h.comp) g.any_comp = true;
+        if (!wide_ok(h.prec, h.p.Z)) g.all_wide = false;
         descs.push_back(d);
         for (int t = 0; t < h.ntiles; ++t) tile_inst.push_back((int)k);
         tb += h.ntiles;

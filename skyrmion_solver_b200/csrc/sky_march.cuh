@@ -21,14 +21,24 @@
 // array once per site plus the halo.
 #pragma once
 
+#include <type_traits>
+
 #include "sky_kernels.cuh"
 
 namespace sky {
 
-template <int C_, int BY_>
+// A row of a staged plane holds z = z0 - ZOFF .. z0 - ZOFF + HZ - 1.  Narrow rows
+// (36 values: z0-2 .. z0+33) are filled element by element; wide rows (40 values:
+// z0-4 .. z0+35) are filled with 16-byte copies, which needs Z to be a multiple of
+// 16 / sizeof(T) so that every 16-byte chunk of a row starts on a 16-byte boundary
+// and lies wholly inside or (as the first chunk at z0 = 0) wholly outside the lattice
+// in z; a chunk crossing z = Z copies its in-lattice part and zero-fills the rest.
+template <int C_, int BY_, bool WIDE_ = false>
 struct MarchShape {
     static constexpr int C = C_, BY = BY_, BZ = 32;
-    static constexpr int HY = BY + 4, HZ = BZ + 4;
+    static constexpr bool WIDE = WIDE_;
+    static constexpr int HY = BY + 4, HZ = WIDE ? BZ + 8 : BZ + 4;
+    static constexpr int ZOFF = WIDE ? 4 : 2;
     static constexpr int PLANE = HY * HZ;  // one component of one plane, with halo
     static constexpr int SLOT = C * PLANE;  // all components of one plane
     static constexpr int RING = 5;
@@ -53,6 +63,11 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool vali
     asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem), "n"(BYTES), "r"(n)
                  : "memory");
 }
+// 16-byte copy of `nbytes` (0..16) bytes, zero-filling the rest of the 16.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int nbytes) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(nbytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -73,12 +88,87 @@ struct PlaneOffsets {
             const int zz = idx - row * M::HZ;
             const int c = row / M::HY;
             const int yy = row - c * M::HY;
-            const int gy = y0 - 2 + yy, gz = z0 - 2 + zz;
+            const int gy = y0 - 2 + yy, gz = z0 - M::ZOFF + zz;
             const bool ok = idx < M::SLOT && gy >= 0 && gy < p.Y && gz >= 0 && gz < p.Z;
             off[k] = ok ? static_cast<int>(c * N + (int64_t)gy * p.Z + gz) : -1;
         }
     }
 };
+
+// Wide rows: per-thread 16-byte chunks of the haloed plane.  Chunk k of thread tid
+// is ci = tid + k*NTHREADS; its global element offset within the x-plane and the
+// number of its bytes inside the lattice (0 when outside or past the slot).
+template <class M, typename T>
+struct PlaneChunks {
+    static constexpr int VW = 16 / int(sizeof(T));
+    static constexpr int CPR = M::HZ / VW;
+    static constexpr int NCHS = M::C * M::HY * CPR;
+    static constexpr int NCH = (NCHS + M::NTHREADS - 1) / M::NTHREADS;
+    int off[NCH];
+    int nb[NCH];
+    __device__ __forceinline__ void init(const Params& p, int64_t N, int y0, int z0) {
+        static_assert(M::WIDE && M::HZ % VW == 0, "16-byte chunks need the wide row layout");
+        const int tid = threadIdx.x + M::BZ * threadIdx.y;
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) {
+            const int ci = tid + k * M::NTHREADS;
+            const int row = ci / CPR;
+            const int cz = ci - row * CPR;
+            const int c = row / M::HY;
+            const int yy = row - c * M::HY;
+            const int gy = y0 - 2 + yy, gz0 = z0 - M::ZOFF + cz * VW;
+            const bool ok = ci < NCHS && gy >= 0 && gy < p.Y && gz0 >= 0 && gz0 < p.Z;
+            off[k] = ok ? static_cast<int>(c * N + (int64_t)gy * p.Z + gz0) : 0;
+            nb[k] = ok ? int(sizeof(T)) * min(VW, p.Z - gz0) : 0;
+        }
+    }
+};
+
+template <class M, int NSRC, typename T>
+__device__ __forceinline__ void plane_issue_wide(T* __restrict__ stage, const PlaneChunks<M, T>& pc,
+                                                 const T* const (&src)[3], int64_t plane_base, bool xok) {
+    using PC = PlaneChunks<M, T>;
+    const int tid = threadIdx.x + M::BZ * threadIdx.y;
+#pragma unroll
+    for (int k = 0; k < PC::NCH; ++k) {
+        const int ci = tid + k * M::NTHREADS;
+        if (PC::NCHS % M::NTHREADS == 0 || ci < PC::NCHS) {
+#pragma unroll
+            for (int s = 0; s < NSRC; ++s) {
+                const T* g = src[s];
+                const int n = (xok && g != nullptr) ? pc.nb[k] : 0;
+                cp_async16(stage + s * M::SLOT + ci * PC::VW, n ? (const void*)(g + plane_base + pc.off[k])
+                                                                : (const void*)src[0], n);
+            }
+        }
+    }
+    cp_async_commit();
+}
+
+template <class M, int NSRC, typename T>
+__device__ __forceinline__ void plane_combine_wide(T* __restrict__ slot, const T* __restrict__ stage, T a, T b) {
+    using PC = PlaneChunks<M, T>;
+    const int tid = threadIdx.x + M::BZ * threadIdx.y;
+#pragma unroll
+    for (int k = 0; k < PC::NCH; ++k) {
+        const int ci = tid + k * M::NTHREADS;
+        if (PC::NCHS % M::NTHREADS == 0 || ci < PC::NCHS) {
+            T v[PC::VW];
+#pragma unroll
+            for (int e = 0; e < PC::VW; ++e) v[e] = stage[ci * PC::VW + e];
+            if (NSRC > 1) {
+#pragma unroll
+                for (int e = 0; e < PC::VW; ++e) v[e] += a * stage[M::SLOT + ci * PC::VW + e];
+            }
+            if (NSRC > 2) {
+#pragma unroll
+                for (int e = 0; e < PC::VW; ++e) v[e] += b * stage[2 * M::SLOT + ci * PC::VW + e];
+            }
+#pragma unroll
+            for (int e = 0; e < PC::VW; ++e) slot[ci * PC::VW + e] = v[e];
+        }
+    }
+}
 
 // Issue the cp.async copies of one x-plane (element offset plane_base) of the
 // NSRC source arrays into the staging slots; a null source reads as zero.
@@ -155,7 +245,7 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                                            int xa, int xe, int y0, int z0, Epi& epi, KSum& esum, KSum& bsum) {
     constexpr int C = M::C;
     static_assert(Th<T>::C == C, "component count mismatch");
-    static_assert(!LO || (DENS && NSRC == 2), "low-part ring only for the stage-1 density");
+    static_assert(!LO || (DENS && NSRC == 2 && !M::WIDE), "low-part ring only for the narrow stage-1 density");
     T* ring = sm;
     T* stage = sm + M::RING * M::SLOT;
     T* ring_lo = stage + NSRC * M::SLOT;
@@ -168,7 +258,9 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     const bool own = (y < p.Y) && (z < p.Z);
     StencilCoef<T> k;
     k.init(p);
-    PlaneOffsets<M> po;
+    // element offsets (narrow rows) or 16-byte chunks (wide rows) of the haloed plane
+    using PO = typename std::conditional<M::WIDE, PlaneChunks<M, T>, PlaneOffsets<M>>::type;
+    PO po;
     po.init(p, N, y0, z0);
     T uq[C][5], wq[C][5];  // uy / uz queues for planes x-2 .. x+2
 #pragma unroll
@@ -176,18 +268,26 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
 #pragma unroll
         for (int m = 0; m < 5; ++m) uq[c][m] = wq[c][m] = T(0);
     const int q0 = xa - 2, q1 = xe + 1;
-    const int lofs = (ty + 2) * M::HZ + (tx + 2);  // thread's site within a component plane
+    const int lofs = (ty + 2) * M::HZ + (tx + M::ZOFF);  // thread's site within a component plane
+    auto issue = [&](int64_t base, bool xok) {
+        if constexpr (M::WIDE)
+            plane_issue_wide<M, NSRC, T>(stage, po, src, base, xok);
+        else
+            plane_issue<M, NSRC, T>(stage, po, src, base, xok);
+    };
     __syncthreads();
-    plane_issue<M, NSRC, T>(stage, po, src, (int64_t)q0 * YZ, q0 >= 0 && q0 < p.X);
+    issue((int64_t)q0 * YZ, q0 >= 0 && q0 < p.X);
     int slot = 0;  // ring slot of plane q
     for (int q = q0; q <= q1; ++q) {
         cp_async_wait_all();
         __syncthreads();  // (A) every thread finished the previous centre: slot `slot` is free
-        if (LO)
+        if constexpr (LO)
             plane_split<M, T>(ring + slot * M::SLOT, ring_lo + slot * M::SLOT, stage);
+        else if constexpr (M::WIDE)
+            plane_combine_wide<M, NSRC, T>(ring + slot * M::SLOT, stage, a, b);
         else
             plane_combine<M, NSRC, T>(ring + slot * M::SLOT, stage, a, b);
-        if (q < q1) plane_issue<M, NSRC, T>(stage, po, src, (int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X);
+        if (q < q1) issue((int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X);
         __syncthreads();  // (B) slot complete
         // arrival: first-difference sums of plane q at (y, z)
         {

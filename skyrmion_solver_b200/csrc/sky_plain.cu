@@ -286,17 +286,16 @@ int choose_xc(int X, int tiles_yz, int resident) {
 
 // Library options (sky_set_option): key 0 = kernel family of the
 // reference-layout gradient (1 = marching kernels for C <= 5, 0 = 3-D tile
-// kernels); key 1 = x-chunk of those marching launches (0 = automatic); key 2
-// = resident blocks per SM the engine's FP32 marching stages are compiled for.
-static int g_options[4] = {1, 0, 2, 0};
+// kernels); key 1 = x-chunk of those marching launches (0 = automatic).
+static int g_options[4] = {1, 0, 0, 0};
 int option(int key) { return (key >= 0 && key < 4) ? g_options[key] : 0; }
 
 // ---------------------------------------------------------------------------
 // templated launchers
 // ---------------------------------------------------------------------------
-template <template <typename> class Th, typename T>
+template <template <typename> class Th, typename T, bool WIDE>
 int launch_gradient_march(const Params& p, const T* field, T* eg, T* l, cudaStream_t st) {
-    using M = MarchShape<Th<T>::C, 8>;
+    using M = MarchShape<Th<T>::C, 8, WIDE>;
     auto kern = k_march_plain<Th, M, T>;
     const size_t smem = M::template smem_bytes<T>(1);
     static int per_sm = 0;
@@ -381,8 +380,12 @@ int launch_density(const Params& p, const S* field, double* dens, double* scratc
 template <template <typename> class Th>
 int grad64(const Params& p, const double* f, double* eg, double* l, cudaStream_t st) {
     if constexpr (Th<double>::C <= 5) {
-        if (option(0) == 1 && (int64_t)p.C * n_sites(p) < ((int64_t)1 << 31))
-            return launch_gradient_march<Th, double>(p, f, eg, l, st);
+        if (option(0) == 1 && (int64_t)p.C * n_sites(p) < ((int64_t)1 << 31)) {
+            // 16-byte staging needs a 16-byte aligned field and Z a multiple of two doubles
+            if (p.Z % 2 == 0 && (reinterpret_cast<uintptr_t>(f) & 15) == 0)
+                return launch_gradient_march<Th, double, true>(p, f, eg, l, st);
+            return launch_gradient_march<Th, double, false>(p, f, eg, l, st);
+        }
     }
     return launch_gradient<Th, double, double>(p, f, eg, l, st);
 }
@@ -476,8 +479,7 @@ const char* sky_version(void) { return "skyrmion_b200 0.2 (sm_100a)"; }
 int sky_set_option(int key, int value) {
     if (key == 0 && value != 0 && value != 1) return invalid("option 0 takes 0 (tile kernels) or 1 (marching kernels)");
     if (key == 1 && value < 0) return invalid("option 1 (x-chunk) must be >= 0");
-    if (key == 2 && value != 2 && value != 3) return invalid("option 2 (FP32 stage blocks per SM) takes 2 or 3");
-    if (key < 0 || key > 2) return invalid("unknown option key");
+    if (key < 0 || key > 1) return invalid("unknown option key");
     g_options[key] = value;
     return SKY_OK;
 }
