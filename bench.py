@@ -370,35 +370,40 @@ def run_ours(args):
     eng64_ms = a0.elapsed_time(a1) / max(8, min(64, K))
     e64.close()
 
-    # end to end through the public API: pinned host field in, per-step (E, B, err) out, field out,
-    # for both phases of the schedule (compensated FP32, then FP64 after set_precision)
+    # end to end through the public API, one solve's worth: admission from a pinned host FP64 field,
+    # per-step host read of (E, B, err) in both phases, the precision switch, and the final field
+    # download into pinned host memory; each piece timed, then combined over the calibrated steps
     host = torch.empty(C * N, dtype=torch.float64, pin_memory=True)
     host.copy_(field)
     host_np = host.numpy().reshape((C, L, L, L))
-    out_np = np.empty_like(host_np)
-    K64 = max(8, min(64, K))
+    out_pin = torch.empty(C * N, dtype=torch.float64, pin_memory=True)
+    out_np = out_pin.numpy().reshape((C, L, L, L))
+    K64 = max(8, min(256, K))
     barrier()
-    tw0 = time.perf_counter()
+    tw = [time.perf_counter()]
     ee = Engine(local)
     j = ee.add("omega", (p_i, p_f), host_np, None, precision=FAST)
+    tw.append(time.perf_counter())                       # admission
     for _ in range(K):
         ee.step(1)
         ee.stats(j)
-    tw1 = time.perf_counter()
+    tw.append(time.perf_counter())                       # K fp32c steps
     ee.set_precision(j, "fp64")
-    tw2 = time.perf_counter()
+    tw.append(time.perf_counter())                       # switch
     for _ in range(K64):
         ee.step(1)
         ee.stats(j)
+    tw.append(time.perf_counter())                       # K64 FP64 steps
     ee._call("sky_engine_read", j, __import__("ctypes").c_void_p(out_np.ctypes.data), None, 0)
-    tw3 = time.perf_counter()
+    tw.append(time.perf_counter())                       # download
     ee.close()
-    e2e = torch.tensor([tw1 - tw0, tw3 - tw2], dtype=torch.float64)
+    e2e = torch.tensor([tw[i + 1] - tw[i] for i in range(5)], dtype=torch.float64)
     if pg is not None:
         e2e = e2e.to(dev)
         pg.all_reduce(e2e, op=pg.ReduceOp.MAX)
-    e2e32_ms = float(e2e[0]) * 1e3 / K          # includes the admission upload
-    e2e64_ms = float(e2e[1]) * 1e3 / K64         # includes the final field download
+    t_up, t32, t_sw, t64, t_down = (float(v) for v in e2e)
+    e2e32_ms = t32 * 1e3 / K
+    e2e64_ms = t64 * 1e3 / K64
     field_bytes = C * N * 8
     s32 = cal.get("mixed_fp32_steps") if cal else None
     s64p = cal.get("mixed_fp64_steps") if cal else None
@@ -407,7 +412,7 @@ def run_ours(args):
 
     solve_s = (s32 * ms_step + s64p * eng64_ms) * 1e-3 if have else None
     value = world / solve_s if have else None
-    e2e_solve_s = (s32 * e2e32_ms + s64p * e2e64_ms) * 1e-3 if have else None
+    e2e_solve_s = (t_up + s32 * e2e32_ms * 1e-3 + t_sw + s64p * e2e64_ms * 1e-3 + t_down) if have else None
     e2e_value = world / e2e_solve_s if have else None
     plain_value = world / (s64 * plain_ms * 1e-3) if s64 else None
     eng64_value = world / (s64 * eng64_ms * 1e-3) if s64 else None
@@ -435,11 +440,14 @@ def run_ours(args):
         "plain_fp64": {"ms_per_step": plain_ms, "solves_per_s": plain_value, "steps_to_converge": s64,
                        "engine_fp64_ms_per_step": eng64_ms, "engine_fp64_solves_per_s": eng64_value,
                        "speedup": (value / plain_value) if (value and plain_value) else None},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": field_bytes / (K + K64),
-                "d2h_bytes_per_step": (48 * (K + K64) + field_bytes) / (K + K64),
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": field_bytes / (s32 + s64p) if have else None,
+                "d2h_bytes_per_step": (48 * (s32 + s64p) + field_bytes) / (s32 + s64p) if have else None,
                 "ms_per_step": {"fp32c": e2e32_ms, "fp64": e2e64_ms},
-                "path": "Engine.add(pinned host FP64 field) + K x (Engine.step(1) + Engine.stats) + "
-                        "set_precision(fp64) + K64 x (step + stats) + field read"},
+                "seconds": {"admit": t_up, "switch": t_sw, "download": t_down, "solve": e2e_solve_s},
+                "path": "Engine.add(pinned host FP64 field) + S32 x (Engine.step(1) + Engine.stats) + "
+                        "set_precision(fp64) + S64 x (step + stats) + field read into pinned memory; "
+                        "per-step times from K and K64 timed steps"},
         "gpu_launches": launches,
         "clocks": clk,
         "final": {"energy": st.energy, "baryon": st.baryon, "max_abs_gradient": st.gabs, "step": st.step},
@@ -610,7 +618,7 @@ def run_serve(args):
             r.field = t.cpu().numpy().reshape(r.field.shape)
     # 1. continuous batching on the resident engine
     with Engine(0) as eng:
-        srv = Server(eng, chunk=64)
+        srv = Server(eng, chunk=64, fp32_mode=args.schedule)
         for r, _, _ in reqs:
             srv.submit(r)
         torch.cuda.synchronize()
@@ -649,7 +657,9 @@ def run_serve(args):
     line = {"mode": "serve", "metric": METRIC, "unit": UNIT,
             "config": {"workload": "poisson_stream", "requests": args.requests, "rate_per_s": args.rate,
                        "mix": mix, "B": f"1..{args.bmax}", "max_side": args.max_side, "h": 0.2, "dt": "0.2 h",
-                       "tol_max_abs_gradient": GRAD_TOL, "schedule": "fp32c until the gradient floor, then fp64"},
+                       "tol_max_abs_gradient": GRAD_TOL,
+                       "schedule": "fp64 throughout" if args.schedule == "fp64" else
+                       f"{args.schedule} until twice the FP32 gradient floor, then fp64"},
             "served": summ,
             "serial_plain_fp64": {"converged": n_serial, "seconds": t_all, "solves_per_s": serial_sps},
             "speedup_solves_per_s": (summ["solves_per_s"] / serial_sps) if (summ["solves_per_s"] and serial_sps)
@@ -806,6 +816,8 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--mix", default="nuclear:1")
     ap.add_argument("--bmax", type=int, default=1)
+    ap.add_argument("--schedule", choices=("fp32c", "fp32", "fp64"), default="fp32c",
+                    help="serving precision schedule: FP32 phase then FP64, or FP64 throughout")
     ap.add_argument("--max-side", type=int, default=64)
     ap.add_argument("--batch", action="store_true", help="48 mixed pion / rho instances in one engine")
     ap.add_argument("--instances", type=int, default=48)

@@ -130,7 +130,7 @@ class Server:
         self.plateau_chunks = int(plateau_chunks)
         self.plateau_gain = float(plateau_gain)
         self.polish = polish
-        self.fp32_mode = fp32_mode   # "fp32c" (compensated field, default) or "fp32"
+        self.fp32_mode = fp32_mode   # "fp32c" (compensated field, default), "fp32", or "fp64" (no FP32 phase)
         self.tune_cache = tune_cache  # autotune.TuneCache: re-tile admitted instances with cached choices
         self.keep_fields = keep_fields
         self.clock = clock
@@ -172,7 +172,7 @@ class Server:
             if self.tune_cache is not None:
                 from .autotune import apply
                 apply(self.engine, iid, req.theory, self.fp32_mode, req.p_i, self.tune_cache, self.engine.device)
-            self.live[iid] = _Live(req, iid, "fp32", t,
+            self.live[iid] = _Live(req, iid, "fp64" if self.fp32_mode == "fp64" else "fp32", t,
                                    rule=PlateauRule(self._switch_tol(req), self.plateau_chunks * self.chunk,
                                                     self.plateau_gain))
 
