@@ -173,7 +173,12 @@ int sky_engine_destroy(void* engine);
  * 1 = FP64, 2 = FP32 stage arithmetic with a compensated field (stored as an
  * unevaluated FP32 sum hi + lo and updated in FP64 at the end of each step, so
  * that near convergence updates far below one FP32 ulp still accumulate; the
- * stencils read hi only).  field / velocity are FP64 in the reference layout (host pointers,
+ * stencils read hi only), 3 = as 2 with a defect-corrected gradient: every 16
+ * steps an FP64 gradient of hi + lo is evaluated and the difference to the FP32
+ * gradient of the same field is added to every stage's FP32 gradient until the
+ * next refresh, so the flow's fixed point is the FP64 one while the stencils stay
+ * FP32 (theories with at most five components; rho runs 3 as 2).  field / velocity
+ * are FP64 in the reference layout (host pointers,
  * or device pointers when on_device != 0); velocity may be NULL (zero).  The
  * energy of the admitted field is evaluated immediately (stats record 0). */
 int sky_engine_add(void* engine, int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
@@ -182,7 +187,7 @@ int sky_engine_add(void* engine, int theory, const int32_t* p_i, int32_t n_pi, c
 /* Retire an instance and free its memory. */
 int sky_engine_remove(void* engine, int id);
 
-/* Change an instance's precision (0, 1 or 2 as for sky_engine_add) in place,
+/* Change an instance's precision (0..3 as for sky_engine_add) in place,
  * e.g. to FP64 for the polishing phase; the field, velocity, step count and
  * pending arrest decision carry over. */
 int sky_engine_set_precision(void* engine, int id, int precision);
@@ -210,7 +215,7 @@ int sky_engine_stats(void* engine, int id, int64_t step, double* out6);
 /* As sky_engine_stats, with out8 = [energy, baryon, err, max|g|, arrested, step,
  * kinetic energy (1/2) h^3 sum |V|^2 of the velocity the step produced (before any
  * arrest; with killkinen = 0 this is the RK4 dynamics' kinetic energy),
- * precision (0, 1 or 2)]. */
+ * precision (0..3)]. */
 int sky_engine_stats_ex(void* engine, int id, int64_t step, double* out8);
 
 /* Latest statistics of up to `cap` instances: ids_out[k] and out7[7k..7k+6] =
@@ -225,7 +230,8 @@ int sky_engine_read(void* engine, int id, double* field, double* velocity, int o
 
 /* Run nsteps steps without graph capture, timing each launch kind with CUDA
  * events on the engine stream; ms_out[6] = average milliseconds per step spent
- * in [stage 1, stage 2, stage 3, stage 4 + update, control, advance]. */
+ * in [stage 1 (with the defect refresh, if any), stage 2, stage 3, stage 4 +
+ * update, control, advance]. */
 int sky_engine_time_stages(void* engine, int nsteps, double* ms_out);
 
 /* Kernel launches one step issues (6 per non-empty (theory, precision) group). */

@@ -20,12 +20,14 @@ struct HostInst {
     int id = -1;
     int theory = 0;
     int prec = 0;  // storage: 0 = FP32 storage/arithmetic, 1 = FP64
-    int comp = 0;  // FP32 storage with a compensated (hi + lo) field
+    int comp = 0;    // FP32 storage with a compensated (hi + lo) field
+    int defect = 0;  // ... and a defect-corrected gradient (precision 3; marching theories only)
     Params p{};
     int64_t N = 0;
     int C = 0;
     void* F[2] = {nullptr, nullptr};
     void* Flo[2] = {nullptr, nullptr};
+    void* Dlt = nullptr;
     void* V[2] = {nullptr, nullptr};
     void* L[3] = {nullptr, nullptr, nullptr};
     KSum* epart = nullptr;
@@ -50,6 +52,7 @@ struct Group {
     int ntiles = 0;
     bool any_comp = false;  // holds a compensated-field instance (stage 1 stages the low parts too)
     bool all_wide = true;   // every member can use the wide-row (16-byte staged) kernels
+    bool any_defect = false;  // holds a defect-corrected instance (launch the defect refresh)
 };
 
 struct Engine {
@@ -278,6 +281,55 @@ static int launch_advance(const Group& g, cudaStream_t st) {
     return check_cuda(cudaGetLastError(), "launch engine advance", __LINE__);
 }
 
+// Defect refresh of the group's defect-corrected FP32 instances (those whose
+// refresh flag the advance kernel just set; the others' tiles are skipped).
+template <template <typename> class Th, bool WIDE>
+static int launch_defect_t(const Group& g, cudaStream_t st) {
+    if constexpr (uses_march<Th>()) {
+        using M = MarchShape<Th<double>::C, kMarchBY, WIDE>;
+        auto kern = k_march_defect<Th, M>;
+        const size_t smem = M::template smem_bytes<double, float>(2);
+        static int per_sm = 0;
+        if (per_sm == 0) {
+            int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                                "cudaFuncSetAttribute(defect)", __LINE__);
+            if (rc) return rc;
+            int n = 0;
+            rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem), "occupancy",
+                            __LINE__);
+            if (rc) return rc;
+            per_sm = n < 1 ? 1 : n;
+        }
+        const int n = g.ntiles;
+        if (n <= 0) return SKY_OK;
+        const int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
+        kern<<<blocks, dim3(M::BZ, M::BY), smem, st>>>(reinterpret_cast<InstDesc<float>*>(g.d_desc), g.d_tile_inst, 0,
+                                                       n);
+        return check_cuda(cudaGetLastError(), "launch defect refresh", __LINE__);
+    } else {
+        (void)g;
+        (void)st;
+        return SKY_OK;
+    }
+}
+
+template <template <typename> class Th>
+static int launch_defect_w(const Group& g, cudaStream_t st) {
+    return g.all_wide ? launch_defect_t<Th, true>(g, st) : launch_defect_t<Th, false>(g, st);
+}
+
+static int launch_defect(const Group& g, cudaStream_t st) {
+    if (g.prec || !g.any_defect) return SKY_OK;
+    switch (g.theory) {
+        case SKY_THEORY_NUCLEAR: return launch_defect_w<Nuclear>(g, st);
+        case SKY_THEORY_OMEGA: return launch_defect_w<Omega>(g, st);
+        case SKY_THEORY_COULOMB: return launch_defect_w<Coulomb>(g, st);
+        case SKY_THEORY_BERGER: return launch_defect_w<Berger>(g, st);
+        case SKY_THEORY_LIGHTLY_BOUND: return launch_defect_w<LightlyBound>(g, st);
+        default: return SKY_OK;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // conversion kernels (FP64 reference layout <-> engine storage)
 // ---------------------------------------------------------------------------
@@ -326,6 +378,7 @@ static InstDesc<S> make_desc(const HostInst& h, int tile_begin) {
     for (int i = 0; i < 2; ++i) {
         d.F[i] = reinterpret_cast<S*>(h.F[i]);
         d.Flo[i] = reinterpret_cast<S*>(h.Flo[i]);
+        d.Dlt = reinterpret_cast<S*>(h.Dlt);
         d.V[i] = reinterpret_cast<S*>(h.V[i]);
     }
     for (int i = 0; i < 3; ++i) d.L[i] = reinterpret_cast<S*>(h.L[i]);
@@ -363,6 +416,7 @@ static int rebuild_group_t(Engine& e, Group& g) {
     int tb = 0;
     g.any_comp = false;
     g.all_wide = true;
+    g.any_defect = false;
     for (size_t k = 0; k < g.members.size(); ++k) {
         HostInst& h = e.insts[g.members[k]];
         InstDesc<S> d = make_desc<S>(h, tb);
@@ -375,6 +429,7 @@ static int rebuild_group_t(Engine& e, Group& g) {
         }
         h.group_slot = (int)k;
         if (h.comp) g.any_comp = true;
+        if (h.defect) g.any_defect = true;
         if (!wide_ok(h.prec, h.p.Z)) g.all_wide = false;
         descs.push_back(d);
         for (int t = 0; t < h.ntiles; ++t) tile_inst.push_back((int)k);
@@ -413,12 +468,13 @@ static int rebuild_group(Engine& e, Group& g) {
 }
 
 static void free_inst(HostInst& h) {
-    void* ptrs[] = {h.F[0], h.F[1], h.Flo[0], h.Flo[1], h.V[0], h.V[1], h.L[0], h.L[1], h.L[2],
+    void* ptrs[] = {h.F[0], h.F[1], h.Flo[0], h.Flo[1], h.Dlt, h.V[0], h.V[1], h.L[0], h.L[1], h.L[2],
                     h.epart, h.bpart, h.gpart, h.stats};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     memset(h.F, 0, sizeof(h.F));
     memset(h.Flo, 0, sizeof(h.Flo));
+    h.Dlt = nullptr;
     memset(h.V, 0, sizeof(h.V));
     memset(h.L, 0, sizeof(h.L));
     h.epart = h.bpart = nullptr;
@@ -470,9 +526,17 @@ static int alloc_inst(Engine& e, HostInst& h) {
             cudaMemsetAsync(h.Flo[i], 0, fb, e.stream);
         }
     }
+    if (h.defect) {
+        if (cudaMalloc(&h.Dlt, fb) != cudaSuccess) {
+            cudaGetLastError();
+            free_inst(h);
+            return SKY_ERR_NOMEM;
+        }
+        cudaMemsetAsync(h.Dlt, 0, fb, e.stream);
+    }
     cudaMemsetAsync(h.gpart, 0, sizeof(double) * 4 * h.ntiles, e.stream);
     cudaMemsetAsync(h.stats, 0, sizeof(StepStats) * kStatsCap, e.stream);
-    h.bytes = (h.comp ? 9 : 7) * fb + (sizeof(KSum) * 2 + sizeof(double) * 4) * h.ntiles +
+    h.bytes = (h.comp ? 9 : 7) * fb + (h.defect ? fb : 0) + (sizeof(KSum) * 2 + sizeof(double) * 4) * h.ntiles +
               sizeof(StepStats) * kStatsCap;
     return SKY_OK;
 }
@@ -525,10 +589,11 @@ static int init_instance(Engine& e, HostInst& h, int mode) {
     return check_cuda(cudaStreamSynchronize(e.stream), "sync", __LINE__);
 }
 
-// Launch kinds of one step, in order: stage 2, 3, 4 (+ update), advance,
-// stage 1 (on the updated field), control.  Groups are independent, so each
-// kind is issued for every non-empty group before the next kind.
-enum { kKindS2 = 0, kKindS3, kKindS4, kKindAdvance, kKindS1, kKindControl, kNumKinds };
+// Launch kinds of one step, in order: stage 2, 3, 4 (+ update), advance, the
+// defect refresh (groups with defect-corrected instances only), stage 1 (on the
+// updated field), control.  Groups are independent, so each kind is issued for
+// every non-empty group before the next kind.
+enum { kKindS2 = 0, kKindS3, kKindS4, kKindAdvance, kKindDefect, kKindS1, kKindControl, kNumKinds };
 
 static int launch_kind(Engine& e, int kind) {
     for (int t = 0; t < 6; ++t)
@@ -541,6 +606,7 @@ static int launch_kind(Engine& e, int kind) {
                 case kKindS3: rc = launch_stage_group(3, g, 0, g.ntiles, e.stream); break;
                 case kKindS4: rc = launch_stage_group(4, g, 0, g.ntiles, e.stream); break;
                 case kKindAdvance: rc = launch_advance(g, e.stream); break;
+                case kKindDefect: rc = launch_defect(g, e.stream); break;
                 case kKindS1: rc = launch_stage_group(1, g, 0, g.ntiles, e.stream); break;
                 default: rc = launch_control(g, 0, (int)g.members.size(), 0, e.stream); break;
             }
@@ -561,7 +627,8 @@ static int count_launches(Engine& e) {
     int n = 0;
     for (int t = 0; t < 6; ++t)
         for (int pr = 0; pr < 2; ++pr)
-            if (!e.groups[t][pr].members.empty()) n += kNumKinds;
+            if (!e.groups[t][pr].members.empty())
+                n += kNumKinds - ((pr == 0 && e.groups[t][pr].any_defect) ? 0 : 1);
     return n;
 }
 
@@ -658,8 +725,9 @@ int sky_engine_add(void* handle, int theory, const int32_t* p_i, int32_t n_pi, c
                    int precision, const double* field, const double* velocity, int on_device, int* id_out) {
     Engine* e = reinterpret_cast<Engine*>(handle);
     if (!e || !id_out || !field) return invalid("null argument");
-    if (precision < 0 || precision > 2)
-        return invalid("precision must be 0 (FP32), 1 (FP64) or 2 (FP32 with a compensated field)");
+    if (precision < 0 || precision > 3)
+        return invalid("precision must be 0 (FP32), 1 (FP64), 2 (FP32 with a compensated field) or 3 "
+                       "(compensated and defect-corrected FP32)");
     cudaSetDevice(e->device);
     HostInst h;
     int rc = pack_params(theory, p_i, n_pi, p_f, n_pf, &h.p);
@@ -667,7 +735,8 @@ int sky_engine_add(void* handle, int theory, const int32_t* p_i, int32_t n_pi, c
     h.id = e->next_id++;
     h.theory = theory;
     h.prec = precision == 1 ? 1 : 0;
-    h.comp = precision == 2 ? 1 : 0;
+    h.comp = precision >= 2 ? 1 : 0;
+    h.defect = (precision == 3 && theory_components(theory) <= 5) ? 1 : 0;
     h.N = n_sites(h.p);
     h.C = h.p.C;
     if ((rc = alloc_inst(*e, h))) return rc;
@@ -709,8 +778,11 @@ int sky_engine_set_precision(void* handle, int id, int precision) {
     if (!e) return invalid("null engine");
     HostInst* hp = find(e, id);
     if (!hp) return invalid("unknown instance id");
-    if (precision < 0 || precision > 2) return invalid("precision must be 0, 1 or 2");
-    if ((hp->comp ? 2 : hp->prec) == precision) return SKY_OK;
+    if (precision < 0 || precision > 3) return invalid("precision must be 0, 1, 2 or 3");
+    const int defect_new = (precision == 3 && theory_components(hp->theory) <= 5) ? 1 : 0;
+    if ((hp->comp ? 2 + hp->defect : hp->prec) == precision ||
+        (precision == 3 && hp->comp && !defect_new))
+        return SKY_OK;
     cudaSetDevice(e->device);
     cudaStreamSynchronize(e->stream);
     HostInst& h = *hp;
@@ -733,7 +805,9 @@ int sky_engine_set_precision(void* handle, int id, int precision) {
     }
     HostInst nh = h;
     nh.prec = precision == 1 ? 1 : 0;
-    nh.comp = precision == 2 ? 1 : 0;
+    nh.comp = precision >= 2 ? 1 : 0;
+    nh.defect = defect_new;
+    nh.Dlt = nullptr;
     nh.group_slot = -1;
     for (int i = 0; i < 2; ++i) nh.F[i] = nh.Flo[i] = nh.V[i] = nullptr;
     for (int i = 0; i < 3; ++i) nh.L[i] = nullptr;
@@ -750,6 +824,8 @@ int sky_engine_set_precision(void* handle, int id, int precision) {
         const bool fieldk = k == 0;
         if (nh.prec == h.prec) {  // FP32 <-> compensated FP32: the high part carries over
             cudaMemcpyAsync(dsts[k], srcs[k], fb, cudaMemcpyDeviceToDevice, e->stream);
+            if (fieldk && h.comp && nh.comp)
+                cudaMemcpyAsync(nh.Flo[0], h.Flo[cur], fb, cudaMemcpyDeviceToDevice, e->stream);
         } else if (nh.prec) {     // FP32 (+ low part) -> FP64
             if (fieldk && h.comp)
                 k_f32c_to_f64<<<ew_blocks(n), 256, 0, e->stream>>>(n, (const float*)srcs[k], (const float*)h.Flo[cur],
@@ -942,7 +1018,7 @@ int sky_engine_stats_ex(void* handle, int id, int64_t step, double* out8) {
     out8[4] = st.arrested;
     out8[5] = st.step;
     out8[6] = st.kinetic;
-    out8[7] = h->comp ? 2 : h->prec;
+    out8[7] = h->comp ? 2 + h->defect : h->prec;
     return SKY_OK;
 }
 
@@ -974,7 +1050,7 @@ int sky_engine_stats_all(void* handle, int* ids_out, double* out7, int cap, int*
             o[3] = st[i].gabs;
             o[4] = st[i].arrested;
             o[5] = st[i].step;
-            o[6] = hs[i]->comp ? 2 : hs[i]->prec;
+            o[6] = hs[i]->comp ? 2 + hs[i]->defect : hs[i]->prec;
         }
     }
     *count_out = k;
@@ -1056,7 +1132,7 @@ int sky_engine_time_stages(void* handle, int nsteps, double* ms_out) {
     for (auto& kv : e->insts)
         if (kv.second.active) kv.second.steps += nsteps;
     // report in the order stage 1, 2, 3, 4, control, advance
-    ms_out[0] = acc[kKindS1] / nsteps;
+    ms_out[0] = (acc[kKindS1] + acc[kKindDefect]) / nsteps;  // stage 1 with the defect refresh
     ms_out[1] = acc[kKindS2] / nsteps;
     ms_out[2] = acc[kKindS3] / nsteps;
     ms_out[3] = acc[kKindS4] / nsteps;

@@ -44,6 +44,7 @@ struct InstDesc {
     Params p;
     S* F[2];           // ping-pong field
     S* Flo[2];         // ping-pong low parts of a compensated FP32 field (null otherwise)
+    S* Dlt;            // defect correction g64 - g32 of a defect-corrected FP32 instance (null otherwise)
     S* V[2];           // ping-pong velocity
     S* L[3];           // stage slopes l1, l2, l3
     KSum* epart;       // per-tile energy partials (stage 1)
@@ -61,6 +62,7 @@ struct InstDesc {
     int arrested;      // arrest flag for the current step
     int active;        // 0 = skip (retired / paused)
     int cur;           // which half of the F / V ping-pong pairs is current
+    int refresh;       // this step's stage 1 refreshes the defect correction
 };
 
 // RK4 update of one site (core/integrator.py:163-175): V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,
@@ -371,13 +373,18 @@ __global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict_
     }
 }
 
-// Flip the ping-pong halves and advance the step counter (after stage 4).
+// Steps between refreshes of the defect correction of an FP32 instance.
+constexpr int kDefectRefresh = 16;
+
+// Flip the ping-pong halves and advance the step counter (after stage 4); flag the
+// defect refresh of the step that now begins.
 template <typename S>
 __global__ void k_engine_advance(InstDesc<S>* __restrict__ insts, int ninst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < ninst && insts[i].active) {
         insts[i].step += 1;
         insts[i].cur ^= 1;
+        insts[i].refresh = (insts[i].Dlt != nullptr && insts[i].step % kDefectRefresh == 0) ? 1 : 0;
     }
 }
 
@@ -388,9 +395,8 @@ __global__ void k_engine_advance(InstDesc<S>* __restrict__ insts, int ninst) {
 // ---------------------------------------------------------------------------
 template <typename T, int STAGE>
 struct EngineEpi {
-    // no shared-memory prefetch of the epilogue inputs: prefetching F, V, l1..l3 of the
-    // next site with cp.async measured slower (more instructions, more shared memory)
-    static constexpr int NFIN = 0;
+    // inputs of the stage-4 update, read from global memory at the site (prefetching them
+    // into shared memory with cp.async measured slower: more instructions and shared memory)
     const T* fin_src[6];  // F, F_lo (null unless compensated), V (null when arrested), l1, l2, l3
     T* out0;              // l_STAGE (stages 1-3) or F' (stage 4)
     T* out1;              // V' (stage 4)
@@ -401,9 +407,27 @@ struct EngineEpi {
     double gmx, gab;
     double hvol;  // h^3 / 2
     KSum kin;     // (1/2) h^3 sum |V'|^2 over the sites of the tile
-    template <int C, int NT>
-    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g)[C],
-                                               const T* __restrict__ fin) {
+    T* dlt;       // defect correction (null unless defect-corrected)
+    int refresh;  // stage 1 of a refresh step: dlt holds g64 of the field; replace it by g64 - g32
+    template <int C>
+    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g32)[C]) {
+        T g[C];
+        if (dlt) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const int64_t j = c * N + s;
+                const T d = dlt[j];
+                if (STAGE == 1 && refresh) {   // d = g64(F): the correction becomes g64 - g32(F)
+                    dlt[j] = d - g32[c];
+                    g[c] = d;
+                } else {
+                    g[c] = g32[c] + d;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < C; ++c) g[c] = g32[c];
+        }
         if (STAGE < 4) {
 #pragma unroll
             for (int c = 0; c < C; ++c) out0[c * N + s] = -dtt * g[c];
@@ -450,7 +474,8 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
                                 STAGE < 4 ? in.L[STAGE - 1] : in.F[parity ^ 1],
                                 STAGE < 4 ? nullptr : in.V[parity ^ 1],
                                 in.Flo[parity ^ 1],
-                                dtt, p.nsky, p.unit_length, -1.0e300, 0.0, 0.5 * p.vol, KSum{0.0, 0.0}};
+                                dtt, p.nsky, p.unit_length, -1.0e300, 0.0, 0.5 * p.vol, KSum{0.0, 0.0},
+                                in.Dlt, in.refresh};
         KSum es{0.0, 0.0}, bs{0.0, 0.0};
         march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE>, LO>(sm, p, src, a, b, xa, xe, y0, z0, epi, es,
                                                                          bs);
@@ -473,6 +498,43 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
                 in.gpart[4 * lt + 3] = kk.c;
             }
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Defect refresh: for every defect-corrected FP32 instance whose refresh flag is
+// set, the FP64 gradient of its compensated field hi + lo (staged from the FP32
+// arrays into an FP64 ring) is written to Dlt; the following stage 1 turns it
+// into the correction g64 - g32.
+// ---------------------------------------------------------------------------
+struct DefectEpi {
+    float* dlt;
+    template <int C>
+    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const double (&)[C], const double (&g)[C]) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) dlt[c * N + s] = float(g[c]);
+    }
+};
+
+template <template <typename> class Th, class M>
+__global__ void __launch_bounds__(M::NTHREADS, 1)
+    k_march_defect(InstDesc<float>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double* sm = reinterpret_cast<double*>(smraw);
+    for (int t = t_begin + blockIdx.x; t < t_end; t += gridDim.x) {
+        const int ii = __ldg(tile_inst + t);
+        const InstDesc<float>& in = insts[ii];
+        if (!in.active || !in.refresh || in.Dlt == nullptr) continue;  // uniform across the block
+        const Params p = in.p;
+        const int lt = t - in.tile_begin;
+        const MarchGrid mg{in.tiles_nz, in.tiles_ny, in.tiles_nx, in.xc};
+        int xa, xe, y0, z0;
+        march_origin(mg, lt, M::BY, xa, xe, y0, z0, p.X);
+        const float* const src[3] = {in.F[in.cur], in.Flo[in.cur], nullptr};
+        DefectEpi epi{in.Dlt};
+        KSum es{0.0, 0.0}, bs{0.0, 0.0};
+        march_tile<Th, M, double, 2, false, DefectEpi, false, float>(sm, p, src, 1.0, 0.0, xa, xe, y0, z0, epi, es,
+                                                                     bs);
     }
 }
 

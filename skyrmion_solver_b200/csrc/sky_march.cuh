@@ -44,11 +44,11 @@ struct MarchShape {
     static constexpr int RING = 5;
     static constexpr int NTHREADS = BZ * BY;
     static constexpr int NPER = (SLOT + NTHREADS - 1) / NTHREADS;  // plane elements per thread
-    // ring + staging (+ a second ring for the low parts of a compensated field)
-    // + nfin per-thread values of C components for the epilogue
-    template <typename T>
-    static constexpr size_t smem_bytes(int nsrc, bool lo = false, int nfin = 0) {
-        return ((size_t(RING) * (lo ? 2 : 1) + size_t(nsrc)) * SLOT + size_t(nfin) * C * NTHREADS) * sizeof(T);
+    // ring + staging (+ a second ring for the low parts of a compensated field);
+    // the staging area holds values of the source type S
+    template <typename T, typename S = T>
+    static constexpr size_t smem_bytes(int nsrc, bool lo = false) {
+        return size_t(RING) * (lo ? 2 : 1) * SLOT * sizeof(T) + size_t(nsrc) * SLOT * sizeof(S);
     }
 };
 
@@ -145,9 +145,9 @@ __device__ __forceinline__ void plane_issue_wide(T* __restrict__ stage, const Pl
     cp_async_commit();
 }
 
-template <class M, int NSRC, typename T>
-__device__ __forceinline__ void plane_combine_wide(T* __restrict__ slot, const T* __restrict__ stage, T a, T b) {
-    using PC = PlaneChunks<M, T>;
+template <class M, int NSRC, typename T, typename S = T>
+__device__ __forceinline__ void plane_combine_wide(T* __restrict__ slot, const S* __restrict__ stage, T a, T b) {
+    using PC = PlaneChunks<M, S>;
     const int tid = threadIdx.x + M::BZ * threadIdx.y;
 #pragma unroll
     for (int k = 0; k < PC::NCH; ++k) {
@@ -155,14 +155,14 @@ __device__ __forceinline__ void plane_combine_wide(T* __restrict__ slot, const T
         if (PC::NCHS % M::NTHREADS == 0 || ci < PC::NCHS) {
             T v[PC::VW];
 #pragma unroll
-            for (int e = 0; e < PC::VW; ++e) v[e] = stage[ci * PC::VW + e];
+            for (int e = 0; e < PC::VW; ++e) v[e] = T(stage[ci * PC::VW + e]);
             if (NSRC > 1) {
 #pragma unroll
-                for (int e = 0; e < PC::VW; ++e) v[e] += a * stage[M::SLOT + ci * PC::VW + e];
+                for (int e = 0; e < PC::VW; ++e) v[e] += a * T(stage[M::SLOT + ci * PC::VW + e]);
             }
             if (NSRC > 2) {
 #pragma unroll
-                for (int e = 0; e < PC::VW; ++e) v[e] += b * stage[2 * M::SLOT + ci * PC::VW + e];
+                for (int e = 0; e < PC::VW; ++e) v[e] += b * T(stage[2 * M::SLOT + ci * PC::VW + e]);
             }
 #pragma unroll
             for (int e = 0; e < PC::VW; ++e) slot[ci * PC::VW + e] = v[e];
@@ -175,6 +175,7 @@ __device__ __forceinline__ void plane_combine_wide(T* __restrict__ slot, const T
 template <class M, int NSRC, typename T>
 __device__ __forceinline__ void plane_issue(T* __restrict__ stage, const PlaneOffsets<M>& po, const T* const (&src)[3],
                                             int64_t plane_base, bool xok) {
+    // T here is the source (staging) type
     const int tid = threadIdx.x + M::BZ * threadIdx.y;
 #pragma unroll
     for (int k = 0; k < M::NPER; ++k) {
@@ -207,17 +208,18 @@ __device__ __forceinline__ void plane_split(T* __restrict__ slot, T* __restrict_
     }
 }
 
-// Combine the thread's own staged elements into a ring slot: X = F + a V + b L.
-template <class M, int NSRC, typename T>
-__device__ __forceinline__ void plane_combine(T* __restrict__ slot, const T* __restrict__ stage, T a, T b) {
+// Combine the thread's own staged elements (source type S) into a ring slot of
+// type T: X = F + a V + b L.
+template <class M, int NSRC, typename T, typename S = T>
+__device__ __forceinline__ void plane_combine(T* __restrict__ slot, const S* __restrict__ stage, T a, T b) {
     const int tid = threadIdx.x + M::BZ * threadIdx.y;
 #pragma unroll
     for (int k = 0; k < M::NPER; ++k) {
         const int idx = tid + k * M::NTHREADS;
         if (M::SLOT % M::NTHREADS == 0 || idx < M::SLOT) {
-            T v = stage[idx];
-            if (NSRC > 1) v += a * stage[M::SLOT + idx];
-            if (NSRC > 2) v += b * stage[2 * M::SLOT + idx];
+            T v = T(stage[idx]);
+            if (NSRC > 1) v += a * T(stage[M::SLOT + idx]);
+            if (NSRC > 2) v += b * T(stage[2 * M::SLOT + idx]);
             slot[idx] = v;
         }
     }
@@ -235,22 +237,22 @@ __device__ __forceinline__ T diff5(const T* f, int st) {
 // [xa, xe).  DENS adds the FP64 energy / baryon densities of the stage input
 // to esum / bsum (compensated).  LO (with DENS, NSRC = 2): src[1] holds the low
 // parts of a compensated field; the stencils see the high parts and the FP64
-// densities use hi + lo (a null src[1] reads as zero).  When Epi::NFIN > 0 the
-// epilogue's per-site inputs Epi::fin_src[0..NFIN) (C components each; null
-// reads as zero) of site x+1 are copied with cp.async into a per-thread
-// shared-memory area while site x is computed, and handed to the epilogue.
+// densities use hi + lo (a null src[1] reads as zero).
 // ---------------------------------------------------------------------------
-template <template <typename> class Th, class M, typename T, int NSRC, bool DENS, class Epi, bool LO = false>
-__device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, const T* const (&src)[3], T a, T b,
+// S: type of the source arrays and of the staging area (S = T, or float sources
+// staged for an FP64 ring).
+template <template <typename> class Th, class M, typename T, int NSRC, bool DENS, class Epi, bool LO = false,
+          typename S = T>
+__device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, const S* const (&src)[3], T a, T b,
                                            int xa, int xe, int y0, int z0, Epi& epi, KSum& esum, KSum& bsum) {
     constexpr int C = M::C;
     static_assert(Th<T>::C == C, "component count mismatch");
     static_assert(!LO || (DENS && NSRC == 2 && !M::WIDE), "low-part ring only for the narrow stage-1 density");
+    static_assert(!LO || sizeof(S) == sizeof(T), "low-part ring needs same-type sources");
     T* ring = sm;
-    T* stage = sm + M::RING * M::SLOT;
-    T* ring_lo = stage + NSRC * M::SLOT;
-    constexpr int NFIN = Epi::NFIN;
-    T* fin = (LO ? ring_lo + M::RING * M::SLOT : ring_lo) + (threadIdx.x + M::BZ * threadIdx.y);
+    S* stage = reinterpret_cast<S*>(sm + M::RING * M::SLOT);
+    T* ring_lo = reinterpret_cast<T*>(stage + NSRC * M::SLOT);
+
     const int64_t N = n_sites(p);
     const int64_t YZ = (int64_t)p.Y * p.Z;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -259,7 +261,7 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     StencilCoef<T> k;
     k.init(p);
     // element offsets (narrow rows) or 16-byte chunks (wide rows) of the haloed plane
-    using PO = typename std::conditional<M::WIDE, PlaneChunks<M, T>, PlaneOffsets<M>>::type;
+    using PO = typename std::conditional<M::WIDE, PlaneChunks<M, S>, PlaneOffsets<M>>::type;
     PO po;
     po.init(p, N, y0, z0);
     T uq[C][5], wq[C][5];  // uy / uz queues for planes x-2 .. x+2
@@ -271,9 +273,9 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     const int lofs = (ty + 2) * M::HZ + (tx + M::ZOFF);  // thread's site within a component plane
     auto issue = [&](int64_t base, bool xok) {
         if constexpr (M::WIDE)
-            plane_issue_wide<M, NSRC, T>(stage, po, src, base, xok);
+            plane_issue_wide<M, NSRC, S>(stage, po, src, base, xok);
         else
-            plane_issue<M, NSRC, T>(stage, po, src, base, xok);
+            plane_issue<M, NSRC, S>(stage, po, src, base, xok);
     };
     __syncthreads();
     issue((int64_t)q0 * YZ, q0 >= 0 && q0 < p.X);
@@ -282,11 +284,11 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
         cp_async_wait_all();
         __syncthreads();  // (A) every thread finished the previous centre: slot `slot` is free
         if constexpr (LO)
-            plane_split<M, T>(ring + slot * M::SLOT, ring_lo + slot * M::SLOT, stage);
+            plane_split<M, T>(ring + slot * M::SLOT, ring_lo + slot * M::SLOT, reinterpret_cast<const T*>(stage));
         else if constexpr (M::WIDE)
-            plane_combine_wide<M, NSRC, T>(ring + slot * M::SLOT, stage, a, b);
+            plane_combine_wide<M, NSRC, T, S>(ring + slot * M::SLOT, stage, a, b);
         else
-            plane_combine<M, NSRC, T>(ring + slot * M::SLOT, stage, a, b);
+            plane_combine<M, NSRC, T, S>(ring + slot * M::SLOT, stage, a, b);
         if (q < q1) issue((int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X);
         __syncthreads();  // (B) slot complete
         // arrival: first-difference sums of plane q at (y, z)
@@ -342,7 +344,7 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
             }
             Th<T>::gradient(phi, D, Sd, p, g);
             const int64_t s = (int64_t)x * YZ + (int64_t)y * p.Z + z;
-            epi.template operator()<C, M::NTHREADS>(s, N, phi, g, fin);
+            epi(s, N, phi, g);
             if (DENS) {
                 // FP64 energy and baryon densities of the stage input (stage 1: the field itself),
                 // evaluated after the gradient so their registers do not overlap
@@ -368,21 +370,6 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                 ksum_add(esum, Th<double>::energy(phd, Dd, p));
                 ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
             }
-        }
-        if constexpr (NFIN > 0) {
-          if (own && x + 1 >= xa && x + 1 < xe) {
-            // epilogue inputs of the next site, in flight during the next plane's work
-            const int64_t sn = (int64_t)(x + 1) * YZ + (int64_t)y * p.Z + z;
-#pragma unroll
-            for (int k = 0; k < NFIN; ++k) {
-                const T* g0 = epi.fin_src[k];
-#pragma unroll
-                for (int c = 0; c < C; ++c)
-                    cp_async<sizeof(T)>(fin + (k * C + c) * M::NTHREADS,
-                                        g0 ? (const void*)(g0 + c * N + sn) : (const void*)src[0], g0 != nullptr);
-            }
-            cp_async_commit();
-          }
         }
         slot = (slot + 1) % 5;
     }
@@ -424,12 +411,11 @@ __device__ __forceinline__ void march_origin(const MarchGrid& g, int t, int by, 
 // ---------------------------------------------------------------------------
 template <typename T>
 struct PlainEpi {
-    static constexpr int NFIN = 0;
     T* eg;
     T* l;
     T mdt;
-    template <int C, int NT>
-    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g)[C], const T*) {
+    template <int C>
+    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g)[C]) {
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             eg[c * N + s] = g[c];

@@ -8,7 +8,11 @@ with compensated summation, takes the arrest decision on the device and
 replays the per-step launches from a CUDA graph.  Instances are FP32
 (``precision="fp32"``, stage arithmetic and state in FP32), FP32 with a
 compensated field (``"fp32c"``: the field is an unevaluated FP32 sum hi + lo
-updated in FP64, so sub-ulp updates near convergence are not lost) or FP64.
+updated in FP64, so sub-ulp updates near convergence are not lost), FP32 with a
+compensated field and a defect-corrected gradient (``"fp32d"``: every 16 steps the
+FP64 gradient of the field is evaluated and its difference to the FP32 one is
+added to the FP32 stage gradients, so the solve converges to the FP64 fixed
+point at FP32 cost) or FP64.
 """
 from __future__ import annotations
 
@@ -20,7 +24,7 @@ import numpy as np
 from . import _lib
 from ._lib import THEORY_IDS, f64p, i32p
 
-PRECISIONS = {"fp32": 0, "fp64": 1, "fp32c": 2}
+PRECISIONS = {"fp32": 0, "fp64": 1, "fp32c": 2, "fp32d": 3}
 PRECISION_NAMES = {v: k for k, v in PRECISIONS.items()}
 
 

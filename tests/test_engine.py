@@ -272,3 +272,47 @@ def test_rk4_dynamics_and_kinetic_energy(engine, name):
         assert G.rel_err(f, ref[2][0]) <= FP64_TOL and G.rel_err(v, ref[2][1]) <= FP64_TOL
     finally:
         engine.remove(iid)
+
+
+def test_fp32d_tracks_fp64(engine):
+    d, F, V, p_i, p_f = _inputs("omega")
+    a = engine.add("omega", (p_i, p_f), F, V, precision="fp64")
+    b = engine.add("omega", (p_i, p_f), F, V, precision="fp32d")
+    try:
+        engine.step(20)        # crosses a defect refresh at step 16
+        sa, sb = engine.stats(a), engine.stats(b)
+        assert sb.precision == "fp32d"
+        assert abs(sa.energy - sb.energy) <= FP32_ENERGY_TOL * abs(sa.energy)
+        fa, _ = engine.read(a)
+        fb, _ = engine.read(b)
+        assert G.rel_err(fb, fa) <= FP32_FIELD_TOL
+    finally:
+        engine.remove(a)
+        engine.remove(b)
+
+
+def test_fp32d_converges_to_the_fp64_fixed_point():
+    """FP32 stencils with the defect correction reach max|g| = 1e-6 and the FP64 energy;
+    the FP32 gradient alone stalls near its noise floor (~2e-5 at h = 0.2)."""
+    from skyrmion_solver_b200.engine import Engine
+    from tests.test_march import inputs, params_for
+    dims = (24, 24, 24)
+    th, p_i, p_f = params_for("nuclear", dims, h=(0.2, 0.2, 0.2))
+    p_f = p_f.copy()
+    p_f[7] = 0.04
+    F, _ = inputs(4, dims, h=(0.2, 0.2, 0.2), seed=9)
+    with Engine(0) as eng:
+        i64 = eng.add("nuclear", (p_i, p_f), F, None, precision="fp64")
+        i32 = eng.add("nuclear", (p_i, p_f), F, None, precision="fp32c")
+        idd = eng.add("nuclear", (p_i, p_f), F, None, precision="fp32d")
+        n = 0
+        while n < 40000 and eng.stats(i64).gabs > 1e-6:
+            eng.step(256)
+            n += 256
+        s64 = eng.stats(i64)
+        assert s64.gabs <= 1e-6, s64
+        eng.step(max(2048, n // 2))      # give the FP32 instances some extra steps
+        sd, sc = eng.stats(idd), eng.stats(i32)
+    assert sd.gabs <= 2e-6, sd
+    assert abs(sd.energy - s64.energy) <= 1e-8 * abs(s64.energy), (sd.energy, s64.energy)
+    assert sc.gabs > sd.gabs
