@@ -473,9 +473,12 @@ def run_ours(args):
 def run_calibrate(args):
     """Steps to converge: the plain FP64 solve and the mixed schedule the engine serves with.
 
-    fp64:  FP64 engine steps until max|g| <= GRAD_TOL; its final energy is E*.
-    mixed: compensated FP32 until max|g| stops improving (the serving loop's
-           plateau rule), then FP64 until max|g| <= GRAD_TOL.
+    fp64:   FP64 engine steps until max|g| <= GRAD_TOL; its final energy is E*.
+    mixed:  compensated FP32 until max|g| reaches twice the FP32 gradient floor (or
+            stops improving), then FP64 until max|g| <= GRAD_TOL.
+    defect: compensated, defect-corrected FP32 until max|g| <= GRAD_TOL (or stalls),
+            then FP64 until max|g| <= GRAD_TOL (a check that is short when the
+            corrected phase has converged).
     For each, the step after which |E - E*| <= REL_ENERGY_TOL |E*| holds to the end.
     """
     import torch
@@ -488,11 +491,13 @@ def run_calibrate(args):
     chunk = 200
     res = {"workload": WORKLOAD, "chunk": chunk, "grad_tol": GRAD_TOL, "rel_energy_tol": REL_ENERGY_TOL}
     hist = {}
-    for sched in ("fp64", "mixed"):
+    first = {"fp64": "fp64", "mixed": "fp32c", "defect": "fp32d"}
+    for sched in ("fp64", "mixed", "defect"):
         eng = Engine(0)
-        iid = eng.add("omega", (p_i, p_f), field, None, precision="fp64" if sched == "fp64" else "fp32c")
-        rule = PlateauRule(2.0 * fp32_gradient_floor(p_f))
-        prec = "fp64" if sched == "fp64" else "fp32c"
+        prec = first[sched]
+        iid = eng.add("omega", (p_i, p_f), field, None, precision=prec)
+        # the defect-corrected phase can go to the tolerance itself; the plain FP32 phase stops near its floor
+        rule = PlateauRule(GRAD_TOL if sched == "defect" else 2.0 * fp32_gradient_floor(p_f))
         switch = None
         h = [(0, eng.stats(iid).energy, float("inf"), prec)]
         t0 = time.perf_counter()
@@ -535,18 +540,19 @@ def run_calibrate(args):
                 s = None
         return s
 
-    for sched in ("fp64", "mixed"):
+    for sched in ("fp64", "mixed", "defect"):
         s = settle(hist[sched])
         res[f"{sched}_steps_to_converge"] = s
         res[f"{sched}_final_rel_energy_error"] = abs(res[f"{sched}_final_energy"] - e_star) / abs(e_star)
-    sw = res["mixed_switch_step"]
-    s_mix = res["mixed_steps_to_converge"]
-    if s_mix is not None:
-        res["mixed_fp32_steps"] = min(s_mix, sw) if sw is not None else s_mix
-        res["mixed_fp64_steps"] = max(0, s_mix - sw) if sw is not None else 0
+        if sched == "fp64":
+            continue
+        sw = res[f"{sched}_switch_step"]
+        if s is not None:
+            res[f"{sched}_fp32_steps"] = min(s, sw) if sw is not None else s
+            res[f"{sched}_fp64_steps"] = max(0, s - sw) if sw is not None else 0
     res["fp64_reached_grad_tol"] = res["fp64_final_max_abs_gradient"] <= GRAD_TOL
     res["history_every"] = chunk * 10
-    for sched in ("fp64", "mixed"):
+    for sched in ("fp64", "mixed", "defect"):
         res[f"{sched}_history"] = hist[sched][::10]
     res["command"] = "python bench.py --calibrate"
     os.makedirs(os.path.dirname(CALIBRATION), exist_ok=True)
@@ -816,7 +822,7 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--mix", default="nuclear:1")
     ap.add_argument("--bmax", type=int, default=1)
-    ap.add_argument("--schedule", choices=("fp32c", "fp32", "fp64"), default="fp32c",
+    ap.add_argument("--schedule", choices=("fp32d", "fp32c", "fp32", "fp64"), default="fp32d",
                     help="serving precision schedule: FP32 phase then FP64, or FP64 throughout")
     ap.add_argument("--max-side", type=int, default=64)
     ap.add_argument("--batch", action="store_true", help="48 mixed pion / rho instances in one engine")

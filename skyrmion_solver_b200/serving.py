@@ -121,7 +121,7 @@ class Server:
                  switch_tol: float | None = None, plateau_chunks: int = 256, plateau_gain: float = 0.99,
                  polish: bool = True,
                  keep_fields: bool = True, free_bytes=None, clock=time.perf_counter, sleep=time.sleep,
-                 fp32_mode: str = "fp32c", tune_cache=None):
+                 fp32_mode: str = "fp32d", tune_cache=None):
         self.engine = engine
         self.mem_cap = float(mem_cap_bytes)
         self.reserve = float(reserve_bytes)
@@ -130,7 +130,8 @@ class Server:
         self.plateau_chunks = int(plateau_chunks)
         self.plateau_gain = float(plateau_gain)
         self.polish = polish
-        self.fp32_mode = fp32_mode   # "fp32c" (compensated field, default), "fp32", or "fp64" (no FP32 phase)
+        # "fp32d" (compensated, defect-corrected), "fp32c" (compensated), "fp32", or "fp64" (no FP32 phase)
+        self.fp32_mode = fp32_mode
         self.tune_cache = tune_cache  # autotune.TuneCache: re-tile admitted instances with cached choices
         self.keep_fields = keep_fields
         self.clock = clock
@@ -179,6 +180,8 @@ class Server:
     def _switch_tol(self, req: Request) -> float:
         if self.switch_tol is not None:
             return float(self.switch_tol)
+        if self.fp32_mode == "fp32d":      # the corrected gradient reaches the tolerance itself
+            return req.tol
         return 2.0 * fp32_gradient_floor(req.p_f)
 
     def _retire(self, lv: _Live, st, status: str):
