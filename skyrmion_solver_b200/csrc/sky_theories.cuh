@@ -52,30 +52,41 @@ __device__ __forceinline__ void project(T* g, const T* phi, int nsky) {
 }
 
 // Quartic Skyrme variation summed over ordered pairs i != j
-// (th/nuclear_skyrme/kernels.py:1109-1138); coef multiplies each bracket.
+// (th/nuclear_skyrme/kernels.py:1109-1138):
+//   g_a -= coef sum_{i != j} [ 2 (F_j.S_ij) F_ia + n_j S_ii,a - (S_ii.F_j + F_i.S_ij) F_ja - (F_i.F_j) S_ij,a ]
+// regrouped per unordered pair {i, j} (k = ij):
+//   (F_j.S_k - S_jj.F_i) F_ia + (F_i.S_k - S_ii.F_j) F_ja - 2 (F_i.F_j) S_k,a
+// plus sum_i (sum_j n_j - n_i) S_ii,a.  Same sum, fewer operations; only the
+// rounding order differs from the reference.
 template <typename T, int C>
 __device__ __forceinline__ void skyrme_quartic(T* g, const T (&D)[3][C], const T (&S)[6][C], T coef) {
-    T norm[3];
+    T nrm[3];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) norm[i] = D[i][0] * D[i][0] + D[i][1] * D[i][1] + D[i][2] * D[i][2] + D[i][3] * D[i][3];
+    for (int i = 0; i < 3; ++i) nrm[i] = D[i][0] * D[i][0] + D[i][1] * D[i][1] + D[i][2] * D[i][2] + D[i][3] * D[i][3];
+    const T ntot = nrm[0] + nrm[1] + nrm[2];
+    T acc[4];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
+    for (int a = 0; a < 4; ++a)
+        acc[a] = (ntot - nrm[0]) * S[0][a] + (ntot - nrm[1]) * S[1][a] + (ntot - nrm[2]) * S[2][a];
+    const int pi[3] = {0, 0, 1}, pj[3] = {1, 2, 2};
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            if (i == j) continue;
-            const int ij = sidx(i, j);
-            T dn = T(0), dd = T(0), dot = T(0);
+    for (int q = 0; q < 3; ++q) {
+        const int i = pi[q], j = pj[q], k = sidx(i, j);
+        T dot = T(0), tij = T(0), tji = T(0), sij = T(0), sji = T(0);
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                dn += T(2) * D[j][b] * S[ij][b];
-                dd += S[i][b] * D[j][b] + D[i][b] * S[ij][b];
-                dot += D[i][b] * D[j][b];
-            }
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-                g[a] -= coef * (dn * D[i][a] + norm[j] * S[i][a] - dd * D[j][a] - dot * S[ij][a]);
+        for (int b = 0; b < 4; ++b) {
+            dot += D[i][b] * D[j][b];
+            tij += D[j][b] * S[k][b];
+            tji += D[i][b] * S[k][b];
+            sij += S[i][b] * D[j][b];
+            sji += S[j][b] * D[i][b];
         }
+        const T ci = tij - sji, cj = tji - sij, ck = T(2) * dot;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) acc[a] += ci * D[i][a] + cj * D[j][a] - ck * S[k][a];
     }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) g[a] -= coef * acc[a];
 }
 
 // sum_{ijk} eps_ijk d_i(aux) det[e_mu, phi, d_j phi, d_k phi] for mu = 0..3.
