@@ -669,8 +669,9 @@ def run_serve(args):
             "config": {"workload": "poisson_stream", "requests": args.requests, "rate_per_s": args.rate,
                        "mix": mix, "B": f"1..{args.bmax}", "max_side": args.max_side, "h": 0.2, "dt": "0.2 h",
                        "tol_max_abs_gradient": GRAD_TOL,
-                       "schedule": "fp64 throughout" if args.schedule == "fp64" else
-                       f"{args.schedule} until twice the FP32 gradient floor, then fp64"},
+                       "schedule": {"fp64": "fp64 throughout",
+                                    "fp32d": "fp32d until max|g| <= tol or a stall, then fp64"}.get(
+                           args.schedule, f"{args.schedule} until twice the FP32 gradient floor, then fp64")},
             "served": summ,
             "serial_plain_fp64": {"converged": n_serial, "seconds": t_all, "solves_per_s": serial_sps},
             "speedup_solves_per_s": (summ["solves_per_s"] / serial_sps) if (summ["solves_per_s"] and serial_sps)

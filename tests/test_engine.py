@@ -306,13 +306,18 @@ def test_fp32d_converges_to_the_fp64_fixed_point():
         i32 = eng.add("nuclear", (p_i, p_f), F, None, precision="fp32c")
         idd = eng.add("nuclear", (p_i, p_f), F, None, precision="fp32d")
         n = 0
-        while n < 40000 and eng.stats(i64).gabs > 1e-6:
+        while True:               # record 0 carries no gradient statistics: step first
             eng.step(256)
             n += 256
+            if eng.stats(i64).gabs <= 1e-6 or n >= 40000:
+                break
         s64 = eng.stats(i64)
         assert s64.gabs <= 1e-6, s64
-        eng.step(max(2048, n // 2))      # give the FP32 instances some extra steps
+        m = 0
+        while eng.stats(idd).gabs > 1e-6 and m < 3 * n:   # the corrected FP32 solve, up to 4x the FP64 steps
+            eng.step(256)
+            m += 256
         sd, sc = eng.stats(idd), eng.stats(i32)
-    assert sd.gabs <= 2e-6, sd
+    assert sd.gabs <= 1e-6, (sd, n, m)
     assert abs(sd.energy - s64.energy) <= 1e-8 * abs(s64.energy), (sd.energy, s64.energy)
     assert sc.gabs > sd.gabs
