@@ -278,6 +278,7 @@ def run_ours(args):
     import torch
     from skyrmion_solver_b200.core.simulation import Simulation
     from skyrmion_solver_b200.engine import Engine
+    from skyrmion_solver_b200.replicas import max_over_ranks
 
     rank, world, local = dist_env()
     if not torch.cuda.is_available():
@@ -320,10 +321,7 @@ def run_ours(args):
     barrier()
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
-    if pg is not None:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks([ms], device=dev)[0]      # the job is as slow as its slowest GPU
     ms_step = ms / K
     steps_per_s = 1e3 / ms_step
     launches = eng.launches_per_step * K
@@ -400,11 +398,7 @@ def run_ours(args):
     ee._call("sky_engine_read", j, __import__("ctypes").c_void_p(out_np.ctypes.data), None, 0)
     tw.append(time.perf_counter())                       # download
     ee.close()
-    e2e = torch.tensor([tw[i + 1] - tw[i] for i in range(5)], dtype=torch.float64)
-    if pg is not None:
-        e2e = e2e.to(dev)
-        pg.all_reduce(e2e, op=pg.ReduceOp.MAX)
-    t_up, t32, t_sw, t64, t_down = (float(v) for v in e2e)
+    t_up, t32, t_sw, t64, t_down = max_over_ranks([tw[i + 1] - tw[i] for i in range(5)], device=dev)
     e2e32_ms = t32 * 1e3 / K
     e2e64_ms = t64 * 1e3 / K64
     field_bytes = C * N * 8
