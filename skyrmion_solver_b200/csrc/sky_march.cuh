@@ -241,13 +241,18 @@ __device__ __forceinline__ T diff5(const T* f, int st) {
 // ---------------------------------------------------------------------------
 // S: type of the source arrays and of the staging area (S = T, or float sources
 // staged for an FP64 ring).
-template <template <typename> class Th, class M, typename T, int NSRC, bool DENS, class Epi, bool LO = false,
-          typename S = T>
+// GRAD = false: density-only walk (no second derivatives, no gradient, no
+// epilogue); the ring may then hold just the first M::C <= Th::C components
+// (the baryon density needs phi_0..3 only) and each site's FP64 density (energy
+// when DENS & 1, else baryon) is passed to epi.density(s, value).
+template <template <typename> class Th, class M, typename T, int NSRC, int DENS, class Epi, bool LO = false,
+          typename S = T, bool GRAD = true>
 __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, const S* const (&src)[3], T a, T b,
                                            int xa, int xe, int y0, int z0, Epi& epi, KSum& esum, KSum& bsum) {
     constexpr int C = M::C;
-    static_assert(Th<T>::C == C, "component count mismatch");
-    static_assert(!LO || (DENS && NSRC == 2 && !M::WIDE), "low-part ring only for the narrow stage-1 density");
+    constexpr int CT = Th<double>::C;  // components of the theory
+    static_assert(GRAD ? Th<T>::C == C : C <= CT, "component count mismatch");
+    static_assert(!LO || (DENS != 0 && NSRC == 2 && !M::WIDE), "low-part ring only for the narrow stage-1 density");
     static_assert(!LO || sizeof(S) == sizeof(T), "low-part ring needs same-type sources");
     T* ring = sm;
     S* stage = reinterpret_cast<S*>(sm + M::RING * M::SLOT);
@@ -292,7 +297,7 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
         if (q < q1) issue((int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X);
         __syncthreads();  // (B) slot complete
         // arrival: first-difference sums of plane q at (y, z)
-        {
+        if constexpr (GRAD) {
             const T* P = ring + slot * M::SLOT + lofs;
 #pragma unroll
             for (int c = 0; c < C; ++c) {
@@ -314,6 +319,8 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
             const T* Pp1 = ring + ((slot + 4) % 5) * M::SLOT + lofs;
             const T* Pp2 = ring + slot * M::SLOT + lofs;
             const Mask mk = site_mask(p, x, y, z);
+            const int64_t s = (int64_t)x * YZ + (int64_t)y * p.Z + z;
+            if constexpr (GRAD) {
             T phi[C], D[3][C], Sd[6][C], g[C];
 #pragma unroll
             for (int c = 0; c < C; ++c) {
@@ -343,14 +350,16 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                 Sd[5][c] = (mk.my && mk.mz) ? k.mix[2] * mixed16<T>(f, M::HZ, 1) : T(0);
             }
             Th<T>::gradient(phi, D, Sd, p, g);
-            const int64_t s = (int64_t)x * YZ + (int64_t)y * p.Z + z;
             epi(s, N, phi, g);
+            }
             if (DENS) {
                 // FP64 energy and baryon densities of the stage input (stage 1: the field itself),
                 // evaluated after the gradient so their registers do not overlap
                 StencilCoef<double> kd;
                 kd.init(p);
-                double phd[C], Dd[3][C];
+                double phd[CT], Dd[3][CT];
+#pragma unroll
+                for (int c = C; c < CT; ++c) phd[c] = Dd[0][c] = Dd[1][c] = Dd[2][c] = 0.0;
                 // tap value in FP64: hi, or hi + lo for a compensated field
                 const ptrdiff_t dlo = ring_lo - ring;
                 auto tap = [&](const T* q) -> double { return LO ? double(q[0]) + double(q[dlo]) : double(q[0]); };
@@ -367,8 +376,14 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                     Dd[1][c] = mk.py ? kd.d1a[1] * yd - kd.d1b[1] * yd2 : 0.0;
                     Dd[2][c] = mk.pz ? kd.d1a[2] * zd - kd.d1b[2] * zd2 : 0.0;
                 }
-                ksum_add(esum, Th<double>::energy(phd, Dd, p));
-                ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
+                if constexpr (GRAD) {
+                    ksum_add(esum, Th<double>::energy(phd, Dd, p));
+                    ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
+                } else {
+                    const double v = (DENS & 1) ? Th<double>::energy(phd, Dd, p) : Th<double>::baryon(phd, Dd, p);
+                    ksum_add(esum, v);
+                    epi.density(s, v);
+                }
             }
         }
         slot = (slot + 1) % 5;
@@ -423,6 +438,38 @@ struct PlainEpi {
         }
     }
 };
+
+// ---------------------------------------------------------------------------
+// Reference-layout FP64 density (drop-in for compute_energy_kernel /
+// compute_skyrmion_number_kernel): per-site e h^3 or b h^3 (optional) and its
+// compensated sum finished by the last block (deterministic for a given grid).
+// MODE 0: energy (all components), 1: baryon (phi_0..3; M::C = 4).
+// ---------------------------------------------------------------------------
+struct DensEpi {
+    double* dens;
+    __device__ __forceinline__ void density(int64_t s, double v) {
+        if (dens) dens[s] = v;
+    }
+};
+
+template <template <typename> class Th, class M, int MODE>
+__global__ void __launch_bounds__(M::NTHREADS) k_march_density(Params p, MarchGrid mg, const double* __restrict__ field,
+                                                               double* __restrict__ dens, double* __restrict__ scratch,
+                                                               double* __restrict__ out_dev) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double* sm = reinterpret_cast<double*>(smraw);
+    __shared__ KSum shk[32];
+    DensEpi epi{dens};
+    const double* const src[3] = {field, nullptr, nullptr};
+    KSum es{0.0, 0.0}, unused{0.0, 0.0};
+    for (int t = blockIdx.x; t < mg.count(); t += gridDim.x) {
+        int xa, xe, y0, z0;
+        march_origin(mg, t, M::BY, xa, xe, y0, z0, p.X);
+        march_tile<Th, M, double, 1, (MODE == 0 ? 1 : 2), DensEpi, false, double, false>(sm, p, src, 0.0, 0.0, xa, xe,
+                                                                                         y0, z0, epi, es, unused);
+    }
+    if (scratch) finish_ksum(es, scratch, out_dev, shk);
+}
 
 template <template <typename> class Th, class M, typename T>
 __global__ void __launch_bounds__(M::NTHREADS) k_march_plain(Params p, MarchGrid mg, const T* __restrict__ field,

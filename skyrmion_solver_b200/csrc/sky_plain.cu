@@ -389,9 +389,54 @@ int grad64(const Params& p, const double* f, double* eg, double* l, cudaStream_t
     }
     return launch_gradient<Th, double, double>(p, f, eg, l, st);
 }
+// Marching FP64 density with its fused compensated sum (energy: all C <= 5
+// components; baryon: phi_0..3 of any theory).
+template <template <typename> class Th, int MODE, bool WIDE>
+int launch_density_march(const Params& p, const double* field, double* dens, double* scratch, double* out_dev,
+                         cudaStream_t st) {
+    using M = MarchShape<(MODE == 0 ? Th<double>::C : 4), 8, WIDE>;
+    auto kern = k_march_density<Th, M, MODE>;
+    const size_t smem = M::template smem_bytes<double>(1);
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(march density)", __LINE__);
+        if (rc) return rc;
+        int n = 0;
+        rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem), "occupancy",
+                        __LINE__);
+        if (rc) return rc;
+        per_sm = n < 1 ? 1 : n;
+    }
+    int resident = num_sms() * per_sm;
+    if (resident > kMaxRedBlocks) resident = kMaxRedBlocks;
+    const MarchGrid g0 = march_grid<M>(p, p.X);
+    const MarchGrid mg = march_grid<M>(p, choose_xc(p.X, g0.nz * g0.ny, resident));
+    const int blocks = mg.count() < resident ? mg.count() : resident;
+    if (scratch) {
+        int rc = check_cuda(cudaMemsetAsync(scratch + 2 * kMaxRedBlocks + 1, 0, sizeof(double), st), "memset",
+                            __LINE__);
+        if (rc) return rc;
+    }
+    kern<<<blocks, dim3(M::BZ, M::BY), smem, st>>>(p, mg, field, dens, scratch, out_dev);
+    return check_cuda(cudaGetLastError(), "launch march density", __LINE__);
+}
+
+template <template <typename> class Th, int MODE>
+int density_march(const Params& p, const double* f, double* dens, double* scratch, double* out_dev, cudaStream_t st) {
+    if (p.Z % 2 == 0 && (reinterpret_cast<uintptr_t>(f) & 15) == 0)
+        return launch_density_march<Th, MODE, true>(p, f, dens, scratch, out_dev, st);
+    return launch_density_march<Th, MODE, false>(p, f, dens, scratch, out_dev, st);
+}
+
 template <template <typename> class Th>
 int dens64(const Params& p, int mode, const double* f, double* dens, double* scratch, double* out_dev,
            cudaStream_t st) {
+    const bool march = option(0) == 1 && (int64_t)p.C * n_sites(p) < ((int64_t)1 << 31);
+    if (march && mode == 1) return density_march<Th, 1>(p, f, dens, scratch, out_dev, st);
+    if constexpr (Th<double>::C <= 5) {
+        if (march) return density_march<Th, 0>(p, f, dens, scratch, out_dev, st);
+    }
     return mode == 0 ? launch_density<Th, 0, double>(p, f, dens, scratch, out_dev, st)
                      : launch_density<Th, 1, double>(p, f, dens, scratch, out_dev, st);
 }

@@ -152,3 +152,40 @@ def test_engine_fp32_tiling_invariance():
         fb, _ = b.read(ib)
         assert np.array_equal(fa, fb)
         assert a.stats(ia).energy == pytest.approx(b.stats(ib).energy, rel=1e-13)
+
+
+def _plain_density(name, F, p_i, p_f, fn):
+    import ctypes
+    import torch
+    from skyrmion_solver_b200 import _lib
+    from skyrmion_solver_b200._lib import THEORY_IDS, f64p, i32p
+    from skyrmion_solver_b200.core.utils import scratch_doubles
+    t = torch.from_numpy(F.ravel().copy()).cuda()
+    en = torch.zeros(int(p_i[6]), dtype=torch.float64, device="cuda")
+    _lib.call(fn, THEORY_IDS[name], i32p(p_i), len(p_i), f64p(p_f), len(p_f), _lib.dptr(en), _lib.dptr(t),
+              _lib.stream_ptr())
+    scratch = torch.zeros(scratch_doubles(), dtype=torch.float64, device="cuda")
+    tot = ctypes.c_double()
+    _lib.call(fn.replace("_density", "").replace("sky_energy", "sky_total_energy").replace("sky_baryon",
+                                                                                          "sky_total_baryon"),
+              THEORY_IDS[name], i32p(p_i), len(p_i), f64p(p_f), len(p_f), _lib.dptr(t), _lib.dptr(scratch),
+              scratch.numel(), ctypes.byref(tot), _lib.stream_ptr())
+    torch.cuda.synchronize()
+    return en.cpu().numpy().reshape(F.shape[1:]), tot.value
+
+
+@pytest.mark.parametrize("name", ["nuclear", "omega", "coulomb", "rho", "berger"])
+@pytest.mark.parametrize("dims", [(37, 21, 70), (9, 33, 5)])
+def test_plain_density_geometry(options, name, dims):
+    th, p_i, p_f = params_for(name, dims)
+    F, _ = inputs(int(p_i[5]), dims, seed=sum(dims) + 1)
+    thd = O.THEORIES[name]
+    for mode in (1, 0):
+        _set_option(0, mode)
+        e, E = _plain_density(name, F, p_i, p_f, "sky_energy_density")
+        b, Bn = _plain_density(name, F, p_i, p_f, "sky_baryon_density")
+        ref_e = O.energy_density(thd, F, p_i, p_f)
+        ref_b = O.baryon_density(thd, F, p_i, p_f)
+        assert G.rel_err(e, ref_e) <= GRAD_TOL and G.rel_err(b, ref_b) <= GRAD_TOL
+        assert abs(E - O.total_energy(thd, F, p_i, p_f)) <= 1e-12 * abs(E)
+        assert abs(Bn - O.total_baryon(thd, F, p_i, p_f)) <= 1e-12 * max(1.0, abs(Bn))
