@@ -822,7 +822,7 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--mix", default="nuclear:1")
     ap.add_argument("--bmax", type=int, default=1)
-    ap.add_argument("--schedule", choices=("fp32d", "fp32c", "fp32", "fp64"), default="fp32d",
+    ap.add_argument("--schedule", choices=("fp32d", "fp32c", "fp32", "fp64"), default="fp64",
                     help="serving precision schedule: FP32 phase then FP64, or FP64 throughout")
     ap.add_argument("--max-side", type=int, default=64)
     ap.add_argument("--batch", action="store_true", help="48 mixed pion / rho instances in one engine")
