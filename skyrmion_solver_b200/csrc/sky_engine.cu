@@ -73,10 +73,12 @@ template <template <typename> class Th, typename T>
 using EShape = typename GradTile<Th<T>::C, T>::type;
 
 // Theories with at most five components run the marching kernels
-// (sky_march.cuh); the 13-component rho variant keeps the 3-D tile kernel.
-template <template <typename> class Th>
+// (sky_march.cuh) in both precisions; the 13-component rho variant runs them in
+// FP32 (one block of 200 KB per SM) and keeps the 3-D tile kernel in FP64, whose
+// planes would need 400 KB of shared memory.
+template <template <typename> class Th, typename T = float>
 constexpr bool uses_march() {
-    return Th<float>::C <= 5;
+    return Th<float>::C <= 5 || sizeof(T) == 4;
 }
 constexpr int kMarchBY = 8;
 // Wide-row (16-byte staged) or narrow-row march shape.
@@ -91,9 +93,9 @@ constexpr int stage_nsrc() {
 // Resident blocks per SM the marching stages are compiled for (__launch_bounds__):
 // two for FP32 (registers capped at 128, no spills for C = 5), one for FP64
 // (whose shared memory allows no more).
-template <typename T>
+template <template <typename> class Th, typename T>
 constexpr int march_minb() {
-    return sizeof(T) == 4 ? 2 : 1;
+    return (sizeof(T) == 4 && Th<float>::C <= 5) ? 2 : 1;
 }
 
 // Whether every instance of a group can use the wide-row kernels: Z a multiple of
@@ -107,9 +109,9 @@ static int stage_setup_w(int* per_sm_out) {
     static int per_sm = 0;
     if (per_sm == 0) {
         int rc, n = 0;
-        if constexpr (uses_march<Th>()) {
+        if constexpr (uses_march<Th, T>()) {
             using M = MShape<Th, T, WIDE>;
-            auto kern = k_march_stage<Th, M, T, STAGE, march_minb<T>(), LO>;
+            auto kern = k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO>;
             const size_t smem = M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
             rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                             "cudaFuncSetAttribute(march stage)", __LINE__);
@@ -147,10 +149,10 @@ static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t s
     if (n <= 0) return SKY_OK;
     const int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
     InstDesc<T>* d = reinterpret_cast<InstDesc<T>*>(g.d_desc);
-    if constexpr (uses_march<Th>()) {
+    if constexpr (uses_march<Th, T>()) {
         using M = MShape<Th, T, WIDE>;
         const size_t smem = M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
-        k_march_stage<Th, M, T, STAGE, march_minb<T>(), LO><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(
+        k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(
             d, g.d_tile_inst, t_begin, t_end);
     } else {
         using Shape = EShape<Th, T>;
@@ -163,10 +165,12 @@ static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t s
 
 template <template <typename> class Th, typename T, int STAGE>
 static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
-    if constexpr (uses_march<Th>()) {
+    if constexpr (uses_march<Th, T>()) {
         // stage 1 of a group with compensated-field instances stages the low parts too
-        // (narrow rows: the second ring would not leave room for two blocks per SM)
-        if constexpr (STAGE == 1 && sizeof(T) == 4) {
+        // (narrow rows: the second ring would not leave room for two blocks per SM);
+        // rho's 13 components leave no room for the second ring at all: its FP64
+        // densities use the high parts
+        if constexpr (STAGE == 1 && sizeof(T) == 4 && Th<float>::C <= 5) {
             if (g.any_comp) return launch_stage_w<Th, T, 1, false, true>(g, t_begin, t_end, st);
         }
         if (g.all_wide) return launch_stage_w<Th, T, STAGE, true>(g, t_begin, t_end, st);
@@ -235,19 +239,18 @@ static int launch_stage_group(int stage, const Group& g, int tb, int te, cudaStr
 template <template <typename> class Th>
 static int shape_of(int prec, int& bz, int& by, int& tx, int& per_sm) {
     per_sm = 1;
-    if constexpr (uses_march<Th>()) {
-        bz = 32, by = kMarchBY, tx = 0;
-        return prec ? stage_setup<Th, double, 4>(&per_sm) : stage_setup<Th, float, 4>(&per_sm);
-    } else {
-        if (prec) {
+    if (prec) {
+        if constexpr (uses_march<Th, double>()) {
+            bz = 32, by = kMarchBY, tx = 0;
+            return stage_setup<Th, double, 4>(&per_sm);
+        } else {
             using S = EShape<Th, double>;
             bz = S::BZ, by = S::BY, tx = S::TX;
-        } else {
-            using S = EShape<Th, float>;
-            bz = S::BZ, by = S::BY, tx = S::TX;
+            return SKY_OK;
         }
-        return SKY_OK;
     }
+    bz = 32, by = kMarchBY, tx = 0;   // every theory marches in FP32
+    return stage_setup<Th, float, 4>(&per_sm);
 }
 
 static int tile_shape(int theory, int prec, int& bz, int& by, int& tx, int& per_sm) {
@@ -285,7 +288,7 @@ static int launch_advance(const Group& g, cudaStream_t st) {
 // refresh flag the advance kernel just set; the others' tiles are skipped).
 template <template <typename> class Th, bool WIDE>
 static int launch_defect_t(const Group& g, cudaStream_t st) {
-    if constexpr (uses_march<Th>()) {
+    if constexpr (uses_march<Th, double>()) {
         using M = MarchShape<Th<double>::C, kMarchBY, WIDE>;
         auto kern = k_march_defect<Th, M>;
         const size_t smem = M::template smem_bytes<double, float>(2);

@@ -251,6 +251,10 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                                            int xa, int xe, int y0, int z0, Epi& epi, KSum& esum, KSum& bsum) {
     constexpr int C = M::C;
     constexpr int CT = Th<double>::C;  // components of the theory
+    // register queues of the y / z first-difference sums for C <= 5; with more
+    // components (rho, C = 13) they would not fit the registers, and the mixed
+    // derivatives d_x d_y, d_x d_z take 16 taps across the ring planes instead
+    constexpr bool QUEUE = GRAD && C <= 5;
     static_assert(GRAD ? Th<T>::C == C : C <= CT, "component count mismatch");
     static_assert(!LO || (DENS != 0 && NSRC == 2 && !M::WIDE), "low-part ring only for the narrow stage-1 density");
     static_assert(!LO || sizeof(S) == sizeof(T), "low-part ring needs same-type sources");
@@ -269,9 +273,10 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     using PO = typename std::conditional<M::WIDE, PlaneChunks<M, S>, PlaneOffsets<M>>::type;
     PO po;
     po.init(p, N, y0, z0);
-    T uq[C][5], wq[C][5];  // uy / uz queues for planes x-2 .. x+2
+    constexpr int CQ = QUEUE ? C : 1;
+    T uq[CQ][5], wq[CQ][5];  // uy / uz queues for planes x-2 .. x+2
 #pragma unroll
-    for (int c = 0; c < C; ++c)
+    for (int c = 0; c < CQ; ++c)
 #pragma unroll
         for (int m = 0; m < 5; ++m) uq[c][m] = wq[c][m] = T(0);
     const int q0 = xa - 2, q1 = xe + 1;
@@ -297,7 +302,7 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
         if (q < q1) issue((int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X);
         __syncthreads();  // (B) slot complete
         // arrival: first-difference sums of plane q at (y, z)
-        if constexpr (GRAD) {
+        if constexpr (QUEUE) {
             const T* P = ring + slot * M::SLOT + lofs;
 #pragma unroll
             for (int c = 0; c < C; ++c) {
@@ -343,8 +348,16 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                     D[2][c] = mk.pz ? k.d1a[2] * (fp1 - fm1) - k.d1b[2] * (fp2 - fm2) : T(0);
                     Sd[2][c] = mk.pz ? k.d2a[2] * (fp1 + fm1) - k.d2b[2] * (fp2 + fm2) - k.d2c[2] * f0 : T(0);
                 }
-                const T sxy = (uq[c][0] - uq[c][4]) + T(8) * (uq[c][3] - uq[c][1]);
-                const T sxz = (wq[c][0] - wq[c][4]) + T(8) * (wq[c][3] - wq[c][1]);
+                T sxy, sxz;
+                if constexpr (QUEUE) {
+                    sxy = (uq[c][0] - uq[c][4]) + T(8) * (uq[c][3] - uq[c][1]);
+                    sxz = (wq[c][0] - wq[c][4]) + T(8) * (wq[c][3] - wq[c][1]);
+                } else {
+                    sxy = (diff5<T>(Pm2 + co, M::HZ) - diff5<T>(Pp2 + co, M::HZ)) +
+                          T(8) * (diff5<T>(Pp1 + co, M::HZ) - diff5<T>(Pm1 + co, M::HZ));
+                    sxz = (diff5<T>(Pm2 + co, 1) - diff5<T>(Pp2 + co, 1)) +
+                          T(8) * (diff5<T>(Pp1 + co, 1) - diff5<T>(Pm1 + co, 1));
+                }
                 Sd[3][c] = (mk.mx && mk.my) ? k.mix[0] * sxy : T(0);
                 Sd[4][c] = (mk.mx && mk.mz) ? k.mix[1] * sxz : T(0);
                 Sd[5][c] = (mk.my && mk.mz) ? k.mix[2] * mixed16<T>(f, M::HZ, 1) : T(0);

@@ -136,15 +136,44 @@ def test_engine_fp64_chunked(name):
             assert G.rel_err(v, ref[1][1]) <= STEP_TOL
 
 
-def test_engine_fp32_tiling_invariance():
+@pytest.mark.parametrize("xc", [0, 4])
+def test_engine_rho_fp32_marching(xc):
+    """rho (13 components) marches in FP32 without register queues (mixed x-derivatives
+    from taps across the ring planes): two steps against the FP64 oracle, FP32 tolerance."""
+    from skyrmion_solver_b200.engine import Engine
+    dims = (29, 19, 45)
+    th, p_i, p_f = params_for("rho", dims)
+    F, V = inputs(13, dims, seed=7)
+    thd = O.THEORIES["rho"]
+    Fr, Vr, E = F, V, O.total_energy(thd, F, p_i, p_f)
+    ref = []
+    for _ in range(2):
+        Fr, Vr, E, err, _ = O.arrested_newton_step(thd, Fr, Vr, p_i, p_f, E)
+        ref.append((Fr, E))
+    with Engine(0) as eng:
+        iid = eng.add("rho", (p_i, p_f), F, V, precision="fp32")
+        if xc:
+            eng.retile(iid, xc)
+            assert eng.xc(iid) == xc
+        assert eng.xc(iid) > 0
+        for n in range(2):
+            eng.step(1)
+            st = eng.stats(iid)
+            assert abs(st.energy - ref[n][1]) <= 2e-5 * abs(ref[n][1]), (n, st.energy, ref[n][1])
+        f, _ = eng.read(iid)
+    assert G.rel_err(f, ref[1][0]) <= 2e-5
+
+
+@pytest.mark.parametrize("name", ["omega", "rho"])
+def test_engine_fp32_tiling_invariance(name):
     """Re-tiling changes only the order of the per-tile energy partials: the trajectory is unchanged."""
     from skyrmion_solver_b200.engine import Engine
     dims = (40, 24, 36)
-    th, p_i, p_f = params_for("omega", dims)
-    F, V = inputs(5, dims, seed=5)
+    th, p_i, p_f = params_for(name, dims)
+    F, V = inputs(int(p_i[5]), dims, seed=5)
     with Engine(0) as a, Engine(0) as b:
-        ia = a.add("omega", (p_i, p_f), F, V, precision="fp32")
-        ib = b.add("omega", (p_i, p_f), F, V, precision="fp32")
+        ia = a.add(name, (p_i, p_f), F, V, precision="fp32")
+        ib = b.add(name, (p_i, p_f), F, V, precision="fp32")
         b.retile(ib, 4)
         a.step(6)
         b.step(6)
