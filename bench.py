@@ -47,7 +47,8 @@ METRIC = "converged solves/s and p99 latency at 1e-6 rel. energy vs plain FP64; 
 UNIT = "solves/s"
 WORKLOAD = "omega_B4_rational_map_128^3_h0.15"
 CALIBRATION = os.path.join(ROOT, "profiles", "convergence_omega_B4_128.json")
-TRAFFIC = os.path.join(ROOT, "profiles", "ncu_engine_stages_omega128_fp32.md")
+TRAFFIC = [os.path.join(ROOT, "profiles", f) for f in ("ncu_stage1_fp32d_omega128.md",
+                                                        "ncu_engine_stages_omega128_fp32.md")]
 L = 128
 H = 0.15
 FAST = "fp32d"   # precision of the timed steps (the FP32 phase of the schedule)
@@ -59,6 +60,20 @@ REL_ENERGY_TOL = 1e-6
 GRAD_TOL = 1e-6
 # passes over one C-component field per stage launch (reads + writes)
 STAGE_PASSES = {"stage1": 2, "stage2": 3, "stage3": 4, "stage4": 7}
+
+
+def stage_passes(stage, precision):
+    """Field-sized passes (reads + writes of one C-component FP32 array) of one stage launch.
+    Compensated field (fp32c, fp32d): stage 1 also reads the low parts (FP64 densities of hi + lo),
+    stage 4 reads and writes them.  fp32d: every stage reads the correction; every 16th step the
+    defect kernel reads hi and lo and writes it, and stage 1 rewrites it (4/16 per step, counted
+    with stage 1, whose timing includes the defect kernel)."""
+    n = STAGE_PASSES[stage]
+    if precision in ("fp32c", "fp32d"):
+        n += {"stage1": 1, "stage4": 2}.get(stage, 0)
+    if precision == "fp32d":
+        n += 1 + (4 / 16 if stage == "stage1" else 0)
+    return n
 
 
 # ---------------------------------------------------------------------------
@@ -94,11 +109,13 @@ def load_calibration():
 
 def load_traffic(stage):
     """Per-launch DRAM bytes (read + write) of one stage kernel from the committed ncu summary, or None."""
-    if not os.path.exists(TRAFFIC):
-        return None
     import re
-    m = re.search(r"traffic_bytes_per_launch\[%s\]:\s*([0-9.eE+]+)" % stage, open(TRAFFIC).read())
-    return float(m.group(1)) if m else None
+    for path in TRAFFIC:
+        if os.path.exists(path):
+            m = re.search(r"traffic_bytes_per_launch\[%s\]:\s*([0-9.eE+]+)" % stage, open(path).read())
+            if m:
+                return float(m.group(1))
+    return None
 
 
 def measured_peaks():
@@ -330,12 +347,10 @@ def run_ours(args):
     # per-launch-kind timing (CUDA events on the engine stream, un-captured launches)
     stages = eng.time_stages(max(5, min(50, K)))
     dom = max(("stage1", "stage2", "stage3", "stage4"), key=lambda k: stages[k])
-    # passes per launch: the stage's own, + the low parts of the field in stage 4, + the defect correction read
-    extra = (2 if dom == "stage4" else 0) + (1 if FAST == "fp32d" else 0)
-    alg_bytes = (STAGE_PASSES[dom] + extra) * C * 4 * N
+    alg_bytes = stage_passes(dom, FAST) * C * 4 * N
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (stages[dom] * 1e-3) / 1e9
-    step_bytes = (18 + (4 if FAST == "fp32d" else 0)) * C * 4 * N   # 16 passes + low parts (+ correction reads)
+    step_bytes = sum(stage_passes(k, FAST) for k in STAGE_PASSES) * C * 4 * N
     traffic = load_traffic(dom)
 
     # plain FP64 drop-in path (reference layout, sky_arrested_newton_step) on the same field
@@ -432,7 +447,7 @@ def run_ours(args):
                       "the same time; the serving mode (--serve) reports p50/p99 over a request stream"},
         "site_steps_per_s": world * N * steps_per_s,
         "hbm_gbs_step": step_bytes / (ms_step * 1e-3) / 1e9,
-        "roofline": {"bound": "hbm", "kernel": f"k_engine_stage<Omega,float,{dom[-1]}>", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": f"k_march_stage<Omega,float,{dom[-1]}>" + (" + k_march_defect" if dom == "stage1" and FAST == "fp32d" else ""), "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
                      "launch_ms": stages[dom], "stage_ms": stages},
@@ -442,7 +457,7 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": field_bytes / (s32 + s64p) if have else None,
                 "d2h_bytes_per_step": (48 * (s32 + s64p) + field_bytes) / (s32 + s64p) if have else None,
-                "ms_per_step": {"fp32c": e2e32_ms, "fp64": e2e64_ms},
+                "ms_per_step": {FAST: e2e32_ms, "fp64": e2e64_ms},
                 "seconds": {"admit": t_up, "switch": t_sw, "download": t_down, "solve": e2e_solve_s},
                 "path": "Engine.add(pinned host FP64 field) + S32 x (Engine.step(1) + Engine.stats) + "
                         "set_precision(fp64) + S64 x (step + stats) + field read into pinned memory; "
@@ -746,9 +761,10 @@ def run_batch(args):
 def run_dynamics(args):
     """Two B=2 toroidal (z^2 rational map) skyrmions at x = -/+3, the second isorotated by a seeded
     Haar-random SU(2) element, combined by quaternion product, boosted toward each other at relative
-    velocity 0.3 (V = -u(x) d_x phi projected orthogonal to phi, u = 0.15 tanh(-x)), Coulomb variant,
-    side^3 sites with h = 0.15, dt = 0.1 h, killkinen = 0 (RK4 dynamics), compensated FP32.  Every 50
-    steps the FP64 energy audit reads E (potential, FP64 compensated) and K = (1/2) h^3 sum |V|^2."""
+    velocity 0.3 (V = -u(x) d_x phi projected orthogonal to phi, u = 0.15 tanh(-x)), Coulomb variant
+    (or --theory), side^3 sites with h = 0.15, dt = 0.1 h, killkinen = 0 (RK4 dynamics), compensated
+    FP32 (or --precision).  Every 50 steps the FP64 energy audit (sky_engine_audit) evaluates the
+    potential Phi that the kernels integrate and K = (1/2) h^3 sum_c s_c |V_c|^2; H = Phi + K."""
     import numpy as np
     import torch
     from skyrmion_solver_b200.engine import Engine
@@ -756,10 +772,11 @@ def run_dynamics(args):
     from skyrmion_solver_b200 import theories as T
     torch.cuda.set_device(0)
     L, h = args.side, 0.15
-    th = T.by_short_name("coulomb")
+    name = args.theory
+    th = T.by_short_name(name)
     prm = th.params.default_params(xlen=L, ylen=L, zlen=L, lsx=h, lsy=h, lsz=h, xsize=h * (L - 1),
                                    ysize=h * (L - 1), zsize=h * (L - 1), time_step=0.1 * h, killkinen=False,
-                                   **SERVE_THEORIES["coulomb"])
+                                   **SERVE_THEORIES[name])
     p_i, p_f = th.params.pack_device_params(prm.resolved())
     p_i, p_f = np.asarray(p_i, np.int32), np.asarray(p_f, np.float64)
     rng = np.random.default_rng(args.seed)
@@ -772,20 +789,26 @@ def run_dynamics(args):
     dphi = np.gradient(phi, h, axis=1)
     V = -(0.15 * np.tanh(-x))[None] * dphi
     V -= (V * phi).sum(axis=0) * phi
-    F = ini.with_extra_components(phi, 5)
-    Vf = ini.with_extra_components(V, 5)
+    C = int(p_i[5])
+    F = ini.with_extra_components(phi, C)
+    Vf = ini.with_extra_components(V, C)
     ini.vacuum_shell(F, 2)
     Vf[:, :2] = Vf[:, -2:] = 0.0
     Vf[:, :, :2] = Vf[:, :, -2:] = 0.0
     Vf[:, :, :, :2] = Vf[:, :, :, -2:] = 0.0
     with Engine(0) as eng:
-        i = eng.add("coulomb", (p_i, p_f), F, Vf, precision=FAST)
+        i = eng.add(name, (p_i, p_f), F, Vf, precision=args.precision)
         audit = []
-        st = eng.stats(i)
-        audit.append((0, st.energy, 0.5 * float(p_f[6]) * float((Vf * Vf).sum()), st.baryon))
+
+        def record(n):
+            st = eng.stats(i)
+            a = eng.audit(i)
+            audit.append((n, a["potential"], a["kinetic"], st.energy, st.baryon))
+
+        record(0)
         stream = torch.cuda.ExternalStream(eng.stream)
         torch.cuda.synchronize()
-        t_dev = 0.0
+        t_dev = t_audit = 0.0
         for n in range(50, args.steps + 1, 50):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
@@ -793,16 +816,22 @@ def run_dynamics(args):
             b.record(stream)
             b.synchronize()
             t_dev += a.elapsed_time(b)
-            st = eng.stats(i)
-            audit.append((n, st.energy, st.kinetic, st.baryon))
-    H = [e + k for _, e, k, _ in audit]
-    emit({"mode": "dynamics", "sites": L ** 3, "steps": args.steps, "ms_per_step": t_dev / args.steps,
-          "site_steps_per_s": L ** 3 * args.steps / (t_dev * 1e-3), "precision": FAST,
-          "H0": H[0], "H_final": H[-1], "max_rel_H_drift": max(abs(v - H[0]) for v in H) / abs(H[0]),
-          "baryon": [audit[0][3], audit[-1][3]],
-          "audit_every_50": [dict(step=n, E=e, K=k) for n, e, k, _ in audit[:: max(1, len(audit) // 20)]],
-          "note": "E is the variant's coded energy (reference compute_energy); for the Coulomb variant the "
-                  "integrated force is not its exact gradient, so H = E + K is an audit, not an invariant"})
+            t0 = time.perf_counter()
+            record(n)
+            t_audit += time.perf_counter() - t0
+    H = [phi + k for _, phi, k, _, _ in audit]
+    drift = [abs(v - H[0]) / abs(H[0]) for v in H]
+    emit({"mode": "dynamics", "theory": name, "sites": L ** 3, "steps": args.steps,
+          "ms_per_step": t_dev / args.steps,
+          "site_steps_per_s": L ** 3 * args.steps / (t_dev * 1e-3), "precision": args.precision,
+          "audit_ms": 1e3 * t_audit / max(1, len(audit) - 1),
+          "H0": H[0], "H_final": H[-1], "max_rel_H_drift": max(drift),
+          "baryon": [audit[0][4], audit[-1][4]],
+          "audit_every_50": [dict(step=n, Phi=phi, K=k, E_coded=e) for n, phi, k, e, _ in
+                             audit[:: max(1, len(audit) // 20)]],
+          "note": "H = Phi + K from sky_engine_audit (FP64): Phi is the potential whose (anti-)gradient the "
+                  "kernels integrate, K the kinetic term with the auxiliary field's negative sign (omega, "
+                  "Coulomb); E_coded is the variant's coded energy (reference compute_energy)"})
     return 0
 
 
@@ -829,6 +858,10 @@ def main():
     ap.add_argument("--instances", type=int, default=48)
     ap.add_argument("--dynamics", action="store_true", help="RK4 dynamics of two boosted tori with energy audit")
     ap.add_argument("--side", type=int, default=192)
+    ap.add_argument("--theory", choices=("coulomb", "nuclear", "omega"), default="coulomb",
+                    help="dynamics: theory variant")
+    ap.add_argument("--precision", choices=("fp32c", "fp32", "fp32d", "fp64"), default="fp32c",
+                    help="dynamics: engine precision")
     args = ap.parse_args()
     if args.batch:
         return run_batch(args)

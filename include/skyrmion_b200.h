@@ -192,12 +192,25 @@ int sky_engine_remove(void* engine, int id);
  * pending arrest decision carry over. */
 int sky_engine_set_precision(void* engine, int id, int precision);
 
-/* Re-tile an instance of a marching-kernel theory (C <= 5): x-chunk `xc`
- * planes per block (0 = automatic choice from the grid and the SM count).  The
- * state and the pending arrest decision carry over. */
+/* Re-tile an instance that runs the marching kernels (every theory in FP32,
+ * C <= 5 in FP64): x-chunk `xc` planes per block (0 = automatic choice from the
+ * grid and the SM count).  The state and the pending arrest decision carry
+ * over. */
 int sky_engine_retile(void* engine, int id, int xc);
-/* Current x-chunk of an instance (0 for tile-kernel theories, -1 if unknown). */
+/* Current x-chunk of an instance (0 for the 3-D tile kernels, -1 if unknown). */
 int sky_engine_get_xc(void* engine, int id);
+
+/* Energy audit of the RK4 dynamics (killkinen = 0) of an instance's current
+ * state, in FP64 (synchronous).  out2 = [Phi, K]: Phi is the potential whose
+ * (anti-)gradient the kernels integrate and K = (1/2) h^3 sum_c s_c |V_c|^2;
+ * H = Phi + K is conserved up to the O(h^4) gap between the force and energy
+ * stencils.  For the nuclear, rho, Berger and lightly-bound variants Phi is
+ * the coded energy and s_c = 1; for omega, Phi = E_pion - E_omega -
+ * c_omega omega B0, and for Coulomb, Phi = E_pion/2 - (kappa/2)|grad A0|^2 +
+ * kappa A0 B0, both with s_4 = -1 (the auxiliary field is the time component
+ * of a vector field).  No reference counterpart: the reference's dynamics
+ * reports only the coded energy (core/simulation.py:287-308). */
+int sky_engine_audit(void* engine, int id, double* out2);
 
 /* Pause (0) or resume (1) an instance. */
 int sky_engine_set_active(void* engine, int id, int active);

@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <cmath>
 #include <map>
 #include <vector>
 
@@ -166,12 +167,20 @@ static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t s
 template <template <typename> class Th, typename T, int STAGE>
 static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
     if constexpr (uses_march<Th, T>()) {
-        // stage 1 of a group with compensated-field instances stages the low parts too
-        // (narrow rows: the second ring would not leave room for two blocks per SM);
-        // rho's 13 components leave no room for the second ring at all: its FP64
-        // densities use the high parts
+        // stage 1 of a group with compensated-field instances stages the low parts too,
+        // in wide rows when two blocks per SM still fit (the two six-slot rings take
+        // 112.5 KB per block for C = 5), else in narrow rows; rho's 13 components leave
+        // no room for the second ring at all: its FP64 densities use the high parts
         if constexpr (STAGE == 1 && sizeof(T) == 4 && Th<float>::C <= 5) {
-            if (g.any_comp) return launch_stage_w<Th, T, 1, false, true>(g, t_begin, t_end, st);
+            if (g.any_comp) {
+                if (g.all_wide) {
+                    int n = 0;
+                    const int rc = stage_setup_w<Th, T, 1, true, true>(&n);
+                    if (rc) return rc;
+                    if (n >= 2) return launch_stage_w<Th, T, 1, true, true>(g, t_begin, t_end, st);
+                }
+                return launch_stage_w<Th, T, 1, false, true>(g, t_begin, t_end, st);
+            }
         }
         if (g.all_wide) return launch_stage_w<Th, T, STAGE, true>(g, t_begin, t_end, st);
         return launch_stage_w<Th, T, STAGE, false>(g, t_begin, t_end, st);
@@ -201,6 +210,10 @@ static int setup_all() {
     if ((rc = stage_setup<Th, T, 1>(&n)) || (rc = stage_setup<Th, T, 2>(&n)) || (rc = stage_setup<Th, T, 3>(&n)) ||
         (rc = stage_setup<Th, T, 4>(&n)))
         return rc;
+    if constexpr (sizeof(T) == 4 && Th<float>::C <= 5) {  // stage 1 with the low parts
+        if ((rc = stage_setup_w<Th, T, 1, true, true>(&n)) || (rc = stage_setup_w<Th, T, 1, false, true>(&n)))
+            return rc;
+    }
     return SKY_OK;
 }
 
@@ -683,6 +696,61 @@ static int remove_from_group(Engine& e, HostInst& h) {
 
 using namespace sky;
 
+// ---------------------------------------------------------------------------
+// energy audit of the RK4 dynamics (k_engine_audit)
+// ---------------------------------------------------------------------------
+constexpr int kAuditBY = 4;  // 4-row tiles: a 13-component FP64 ring still fits
+
+template <template <typename> class Th, typename S>
+static int audit_t(Engine& e, const HostInst& h, double* out2) {
+    using M = MarchShape<Th<double>::C, kAuditBY, false>;
+    constexpr int NSRC = std::is_same<S, double>::value ? 1 : 2;
+    auto kern = k_engine_audit<Th, M, S>;
+    const size_t smem = M::template smem_bytes<double, S>(NSRC);
+    static bool configured = false;
+    if (!configured) {
+        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(audit)", __LINE__);
+        if (rc) return rc;
+        configured = true;
+    }
+    const MarchGrid mg = march_grid<M>(h.p, h.p.X < 16 ? h.p.X : 16);
+    const int blocks = mg.count() < num_sms() ? mg.count() : num_sms();
+    double* parts = nullptr;
+    int rc = check_cuda(cudaMalloc(&parts, sizeof(double) * 4 * blocks), "cudaMalloc(audit)", __LINE__);
+    if (rc) return rc;
+    const Group& g = e.groups[h.theory][h.prec];
+    const InstDesc<S>* d = reinterpret_cast<const InstDesc<S>*>(g.d_desc) + h.group_slot;
+    kern<<<blocks, dim3(M::BZ, M::BY), smem, e.stream>>>(d, mg, parts);
+    rc = check_cuda(cudaGetLastError(), "launch audit", __LINE__);
+    std::vector<double> hp(4 * (size_t)blocks);
+    if (!rc)
+        rc = check_cuda(cudaMemcpyAsync(hp.data(), parts, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, e.stream),
+                        "read audit", __LINE__);
+    if (!rc) rc = check_cuda(cudaStreamSynchronize(e.stream), "sync audit", __LINE__);
+    cudaFree(parts);
+    if (rc) return rc;
+    // fixed-order compensated sum of the block partials
+    for (int q = 0; q < 2; ++q) {
+        double sum = 0.0, comp = 0.0;
+        for (int b = 0; b < blocks; ++b) {
+            for (int k = 0; k < 2; ++k) {
+                const double v = hp[4 * b + 2 * q + k];
+                const double t = sum + v;
+                comp += (std::fabs(sum) >= std::fabs(v)) ? ((sum - t) + v) : ((v - t) + sum);
+                sum = t;
+            }
+        }
+        out2[q] = sum + comp;
+    }
+    return SKY_OK;
+}
+
+template <template <typename> class Th>
+static int audit_prec(Engine& e, const HostInst& h, double* out2) {
+    return h.prec ? audit_t<Th, double>(e, h, out2) : audit_t<Th, float>(e, h, out2);
+}
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -921,6 +989,24 @@ int sky_engine_retile(void* handle, int id, int xc) {
     Group& g = e->groups[h.theory][h.prec];
     if ((rc = rebuild_group(*e, g))) return rc;
     return init_instance(*e, h, 2);
+}
+
+int sky_engine_audit(void* handle, int id, double* out2) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return invalid("null engine");
+    if (!out2) return invalid("null output");
+    HostInst* hp = find(e, id);
+    if (!hp) return invalid("unknown instance id");
+    cudaSetDevice(e->device);
+    switch (hp->theory) {
+        case SKY_THEORY_NUCLEAR: return audit_prec<Nuclear>(*e, *hp, out2);
+        case SKY_THEORY_OMEGA: return audit_prec<Omega>(*e, *hp, out2);
+        case SKY_THEORY_COULOMB: return audit_prec<Coulomb>(*e, *hp, out2);
+        case SKY_THEORY_RHO: return audit_prec<Rho>(*e, *hp, out2);
+        case SKY_THEORY_BERGER: return audit_prec<Berger>(*e, *hp, out2);
+        case SKY_THEORY_LIGHTLY_BOUND: return audit_prec<LightlyBound>(*e, *hp, out2);
+    }
+    return invalid("unknown theory id");
 }
 
 int sky_engine_get_xc(void* handle, int id) {

@@ -89,15 +89,17 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
 #pragma unroll
         for (int c = 0; c < C; ++c) fv[c] = f0[c] + inc[c];
         if (unit_length) {
+            // one reciprocal square root instead of a square root and nsky divisions
+            // (within one unit in the last place of the quotients)
             T ss = T(0);
 #pragma unroll
             for (int c = 0; c < C; ++c)
                 if (c < nsky) ss += fv[c] * fv[c];
-            ss = sqrt(ss);
             if (ss != T(0)) {
+                const T r = rsqrt(ss);
 #pragma unroll
                 for (int c = 0; c < C; ++c)
-                    if (c < nsky) fv[c] /= ss;
+                    if (c < nsky) fv[c] *= r;
             }
             T lm = T(0);
 #pragma unroll
@@ -115,40 +117,49 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
             v2 += double(vv[c]) * double(vv[c]);
         }
     } else {
-        double fd[C], vd[C];
+        // hi + lo + inc in FP64, with the two small terms summed in FP32 first: lo and the
+        // increment are both far below hi, so their FP32 sum loses no more than the FP32
+        // increment and the FP32 low part already do (about 2^-49 of the field).  One
+        // reciprocal square root normalises.  The velocity is FP32 storage and is
+        // projected in FP32 on the rounded field.
+        double fd[C];
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
-            fd[c] = (double(f0[c]) + double(flo[c])) + double(inc[c]);
-            vd[c] = double(vv[c]);
-        }
+        for (int c = 0; c < C; ++c) fd[c] = double(f0[c]) + double(flo[c] + inc[c]);
         if (unit_length) {
             double ss = 0.0;
 #pragma unroll
             for (int c = 0; c < C; ++c)
-                if (c < nsky) ss += fd[c] * fd[c];
-            ss = sqrt(ss);
+                if (c < nsky) ss = fma(fd[c], fd[c], ss);
             if (ss != 0.0) {
+                const double r = rsqrt(ss);
 #pragma unroll
                 for (int c = 0; c < C; ++c)
-                    if (c < nsky) fd[c] /= ss;
+                    if (c < nsky) fd[c] *= r;
             }
-            double lm = 0.0;
-#pragma unroll
-            for (int c = 0; c < C; ++c)
-                if (c < nsky) lm += vd[c] * fd[c];
-#pragma unroll
-            for (int c = 0; c < C; ++c)
-                if (c < nsky) vd[c] -= lm * fd[c];
         }
-        v2 = 0.0;
+        T hi[C];
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            const S hi = S(fd[c]);
-            Fo[c * N + s] = hi;
-            Flo_out[c * N + s] = S(fd[c] - double(hi));
-            Vo[c * N + s] = S(vd[c]);
-            v2 += double(S(vd[c])) * double(S(vd[c]));
+            hi[c] = T(fd[c]);
+            Fo[c * N + s] = S(hi[c]);
+            Flo_out[c * N + s] = S(fd[c] - double(hi[c]));
         }
+        if (unit_length) {
+            T lm = T(0);
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) lm += vv[c] * hi[c];
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                if (c < nsky) vv[c] -= lm * hi[c];
+        }
+        T vs = T(0);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            Vo[c * N + s] = S(vv[c]);
+            vs += vv[c] * vv[c];
+        }
+        v2 = double(vs);
     }
 }
 
@@ -413,16 +424,20 @@ struct EngineEpi {
     __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g32)[C]) {
         T g[C];
         if (dlt) {
+            // all C loads first (one latency, not C: a store to dlt between them would
+            // keep the compiler from batching them)
+            T d[C];
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-                const int64_t j = c * N + s;
-                const T d = dlt[j];
-                if (STAGE == 1 && refresh) {   // d = g64(F): the correction becomes g64 - g32(F)
-                    dlt[j] = d - g32[c];
-                    g[c] = d;
-                } else {
-                    g[c] = g32[c] + d;
+            for (int c = 0; c < C; ++c) d[c] = dlt[c * N + s];
+            if (STAGE == 1 && refresh) {   // d = g64(F): the correction becomes g64 - g32(F)
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    dlt[c * N + s] = d[c] - g32[c];
+                    g[c] = d[c];
                 }
+            } else {
+#pragma unroll
+                for (int c = 0; c < C; ++c) g[c] = g32[c] + d[c];
             }
         } else {
 #pragma unroll
@@ -452,8 +467,8 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
     constexpr int NSRC = STAGE == 1 ? (LO ? 2 : 1) : (STAGE == 2 ? 2 : 3);
     extern __shared__ __align__(16) unsigned char smraw[];
     T* sm = reinterpret_cast<T*>(smraw);
-    __shared__ KSum shk[32];
-    __shared__ double shm[32];
+    __shared__ KSum shk[M::NTHREADS / 32];  // one entry per warp (kept small: two blocks
+    __shared__ double shm[M::NTHREADS / 32];  // per SM need all but 1 KB of shared memory)
     for (int t = t_begin + blockIdx.x; t < t_end; t += gridDim.x) {
         const int ii = __ldg(tile_inst + t);
         const InstDesc<T>& in = insts[ii];
@@ -535,6 +550,59 @@ __global__ void __launch_bounds__(M::NTHREADS, 1)
         KSum es{0.0, 0.0}, bs{0.0, 0.0};
         march_tile<Th, M, double, 2, false, DefectEpi, false, float>(sm, p, src, 1.0, 0.0, xa, xe, y0, z0, epi, es,
                                                                      bs);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Energy audit of one instance's current state (F, V), in FP64: the potential
+// Phi of the RK4 dynamics (sky_theories.cuh, Dynamics) and the signed kinetic
+// term (1/2) h^3 sum_c s_c |V_c|^2, whose sum H the dynamics conserves.  The
+// field is staged into an FP64 ring (hi + lo for a compensated field); each
+// block writes its two compensated partial sums to parts[4 * block].
+// ---------------------------------------------------------------------------
+template <template <typename> class Th, typename S>
+struct AuditEpi {
+    const S* V;  // null: the velocity is zero (arrested)
+    int64_t N;
+    double hvol;  // h^3 / 2
+    KSum kin;
+    __device__ __forceinline__ void density(int64_t s, double) {
+        if (!V) return;
+        double k = 0.0;
+#pragma unroll
+        for (int c = 0; c < Th<double>::C; ++c) {
+            const double v = double(V[c * N + s]);
+            k += Dynamics<Th>::kinetic_sign(c) * v * v;
+        }
+        ksum_add(kin, hvol * k);
+    }
+};
+
+template <template <typename> class Th, class M, typename S>
+__global__ void __launch_bounds__(M::NTHREADS, 1)
+    k_engine_audit(const InstDesc<S>* __restrict__ d, MarchGrid mg, double* __restrict__ parts) {
+    constexpr int NSRC = std::is_same<S, double>::value ? 1 : 2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double* sm = reinterpret_cast<double*>(smraw);
+    __shared__ KSum shk[M::NTHREADS / 32];
+    const Params p = d->p;
+    const int cur = d->cur;
+    const S* const src[3] = {d->F[cur], NSRC == 2 ? d->Flo[cur] : nullptr, nullptr};
+    AuditEpi<Th, S> epi{d->arrested ? nullptr : d->V[cur], n_sites(p), 0.5 * p.vol, KSum{0.0, 0.0}};
+    KSum es{0.0, 0.0}, unused{0.0, 0.0};
+    for (int t = blockIdx.x; t < mg.count(); t += gridDim.x) {
+        int xa, xe, y0, z0;
+        march_origin(mg, t, M::BY, xa, xe, y0, z0, p.X);
+        march_tile<Th, M, double, NSRC, 4, AuditEpi<Th, S>, false, S, false>(sm, p, src, 1.0, 0.0, xa, xe, y0, z0,
+                                                                             epi, es, unused);
+    }
+    const KSum pe = block_ksum(es, shk);
+    const KSum pk = block_ksum(epi.kin, shk);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        parts[4 * blockIdx.x] = pe.s;
+        parts[4 * blockIdx.x + 1] = pe.c;
+        parts[4 * blockIdx.x + 2] = pk.s;
+        parts[4 * blockIdx.x + 3] = pk.c;
     }
 }
 

@@ -124,7 +124,9 @@ struct PlaneChunks {
     }
 };
 
-template <class M, int NSRC, typename T>
+// Source s of a plane lands at stage + s * DST (DST = M::SLOT: consecutive staging
+// slots; a ring of R slots per source when the plane goes straight into the ring).
+template <class M, int NSRC, typename T, int DST = M::SLOT>
 __device__ __forceinline__ void plane_issue_wide(T* __restrict__ stage, const PlaneChunks<M, T>& pc,
                                                  const T* const (&src)[3], int64_t plane_base, bool xok) {
     using PC = PlaneChunks<M, T>;
@@ -137,7 +139,7 @@ __device__ __forceinline__ void plane_issue_wide(T* __restrict__ stage, const Pl
             for (int s = 0; s < NSRC; ++s) {
                 const T* g = src[s];
                 const int n = (xok && g != nullptr) ? pc.nb[k] : 0;
-                cp_async16(stage + s * M::SLOT + ci * PC::VW, n ? (const void*)(g + plane_base + pc.off[k])
+                cp_async16(stage + s * DST + ci * PC::VW, n ? (const void*)(g + plane_base + pc.off[k])
                                                                 : (const void*)src[0], n);
             }
         }
@@ -172,7 +174,7 @@ __device__ __forceinline__ void plane_combine_wide(T* __restrict__ slot, const S
 
 // Issue the cp.async copies of one x-plane (element offset plane_base) of the
 // NSRC source arrays into the staging slots; a null source reads as zero.
-template <class M, int NSRC, typename T>
+template <class M, int NSRC, typename T, int DST = M::SLOT>
 __device__ __forceinline__ void plane_issue(T* __restrict__ stage, const PlaneOffsets<M>& po, const T* const (&src)[3],
                                             int64_t plane_base, bool xok) {
     // T here is the source (staging) type
@@ -186,26 +188,12 @@ __device__ __forceinline__ void plane_issue(T* __restrict__ stage, const PlaneOf
             for (int s = 0; s < NSRC; ++s) {
                 const T* g = src[s];
                 const bool v = ok && g != nullptr;
-                cp_async<sizeof(T)>(stage + s * M::SLOT + idx,
+                cp_async<sizeof(T)>(stage + s * DST + idx,
                                     v ? (const void*)(g + plane_base + po.off[k]) : (const void*)src[0], v);
             }
         }
     }
     cp_async_commit();
-}
-
-// Move the thread's own staged hi / lo elements of a compensated field into two ring slots.
-template <class M, typename T>
-__device__ __forceinline__ void plane_split(T* __restrict__ slot, T* __restrict__ slot_lo, const T* __restrict__ stage) {
-    const int tid = threadIdx.x + M::BZ * threadIdx.y;
-#pragma unroll
-    for (int k = 0; k < M::NPER; ++k) {
-        const int idx = tid + k * M::NTHREADS;
-        if (M::SLOT % M::NTHREADS == 0 || idx < M::SLOT) {
-            slot[idx] = stage[idx];
-            slot_lo[idx] = stage[M::SLOT + idx];
-        }
-    }
 }
 
 // Combine the thread's own staged elements (source type S) into a ring slot of
@@ -238,13 +226,17 @@ __device__ __forceinline__ T diff5(const T* f, int st) {
 // to esum / bsum (compensated).  LO (with DENS, NSRC = 2): src[1] holds the low
 // parts of a compensated field; the stencils see the high parts and the FP64
 // densities use hi + lo (a null src[1] reads as zero).
+// When the stage input is the field itself (NSRC = 1, or the hi / lo pair of LO,
+// with S = T) the planes are copied straight into a six-slot ring, whose sixth
+// slot takes the plane in flight: no staging copy and one barrier per plane.
 // ---------------------------------------------------------------------------
 // S: type of the source arrays and of the staging area (S = T, or float sources
 // staged for an FP64 ring).
 // GRAD = false: density-only walk (no second derivatives, no gradient, no
 // epilogue); the ring may then hold just the first M::C <= Th::C components
-// (the baryon density needs phi_0..3 only) and each site's FP64 density (energy
-// when DENS & 1, else baryon) is passed to epi.density(s, value).
+// (the baryon density needs phi_0..3 only) and each site's FP64 density (the
+// potential of the RK4 dynamics when DENS & 4, else energy when DENS & 1, else
+// baryon) is passed to epi.density(s, value).
 template <template <typename> class Th, class M, typename T, int NSRC, int DENS, class Epi, bool LO = false,
           typename S = T, bool GRAD = true>
 __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, const S* const (&src)[3], T a, T b,
@@ -256,11 +248,16 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     // derivatives d_x d_y, d_x d_z take 16 taps across the ring planes instead
     constexpr bool QUEUE = GRAD && C <= 5;
     static_assert(GRAD ? Th<T>::C == C : C <= CT, "component count mismatch");
-    static_assert(!LO || (DENS != 0 && NSRC == 2 && !M::WIDE), "low-part ring only for the narrow stage-1 density");
-    static_assert(!LO || sizeof(S) == sizeof(T), "low-part ring needs same-type sources");
+    static_assert(!LO || (DENS != 0 && NSRC == 2), "low-part ring only for the stage-1 density");
+    static_assert(!LO || (std::is_same<S, T>::value && sizeof(T) == 4), "low-part ring needs FP32 sources");
+    constexpr bool DIRECT = (NSRC == 1 || LO) && std::is_same<S, T>::value;
+    constexpr int R = DIRECT ? M::RING + 1 : M::RING;  // ring slots
+    constexpr int DST = DIRECT ? R * M::SLOT : M::SLOT;  // distance between the sources' copies
+    // shared memory: DIRECT: ring (R slots) [+ low-part ring (R slots)];
+    // otherwise: ring (5 slots) + NSRC staging slots of S
     T* ring = sm;
     S* stage = reinterpret_cast<S*>(sm + M::RING * M::SLOT);
-    T* ring_lo = reinterpret_cast<T*>(stage + NSRC * M::SLOT);
+    T* ring_lo = sm + R * M::SLOT;
 
     const int64_t N = n_sites(p);
     const int64_t YZ = (int64_t)p.Y * p.Z;
@@ -281,26 +278,31 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
         for (int m = 0; m < 5; ++m) uq[c][m] = wq[c][m] = T(0);
     const int q0 = xa - 2, q1 = xe + 1;
     const int lofs = (ty + 2) * M::HZ + (tx + M::ZOFF);  // thread's site within a component plane
-    auto issue = [&](int64_t base, bool xok) {
+    auto issue = [&](int64_t base, bool xok, int dslot) {
+        S* dst = DIRECT ? reinterpret_cast<S*>(ring + dslot * M::SLOT) : stage;
         if constexpr (M::WIDE)
-            plane_issue_wide<M, NSRC, S>(stage, po, src, base, xok);
+            plane_issue_wide<M, NSRC, S, DST>(dst, po, src, base, xok);
         else
-            plane_issue<M, NSRC, S>(stage, po, src, base, xok);
+            plane_issue<M, NSRC, S, DST>(dst, po, src, base, xok);
     };
     __syncthreads();
-    issue((int64_t)q0 * YZ, q0 >= 0 && q0 < p.X);
+    issue((int64_t)q0 * YZ, q0 >= 0 && q0 < p.X, 0);
     int slot = 0;  // ring slot of plane q
     for (int q = q0; q <= q1; ++q) {
         cp_async_wait_all();
-        __syncthreads();  // (A) every thread finished the previous centre: slot `slot` is free
-        if constexpr (LO)
-            plane_split<M, T>(ring + slot * M::SLOT, ring_lo + slot * M::SLOT, reinterpret_cast<const T*>(stage));
-        else if constexpr (M::WIDE)
-            plane_combine_wide<M, NSRC, T, S>(ring + slot * M::SLOT, stage, a, b);
-        else
-            plane_combine<M, NSRC, T, S>(ring + slot * M::SLOT, stage, a, b);
-        if (q < q1) issue((int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X);
-        __syncthreads();  // (B) slot complete
+        // (A) plane q has landed for every thread, and every thread finished the
+        // previous centre: the slot of plane q - 5 (staging: the staging area) is free
+        __syncthreads();
+        if constexpr (DIRECT) {
+            if (q < q1) issue((int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X, slot + 1 == R ? 0 : slot + 1);
+        } else {
+            if constexpr (M::WIDE)
+                plane_combine_wide<M, NSRC, T, S>(ring + slot * M::SLOT, stage, a, b);
+            else
+                plane_combine<M, NSRC, T, S>(ring + slot * M::SLOT, stage, a, b);
+            if (q < q1) issue((int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X, 0);
+            __syncthreads();  // (B) slot complete
+        }
         // arrival: first-difference sums of plane q at (y, z)
         if constexpr (QUEUE) {
             const T* P = ring + slot * M::SLOT + lofs;
@@ -317,11 +319,11 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
         }
         const int x = q - 2;
         if (x >= xa && own) {
-            // plane q-j sits in slot (slot + 5 - j) % 5: x-2 = q-4, ..., x+2 = q
-            const T* Pm2 = ring + ((slot + 1) % 5) * M::SLOT + lofs;
-            const T* Pm1 = ring + ((slot + 2) % 5) * M::SLOT + lofs;
-            const T* P0 = ring + ((slot + 3) % 5) * M::SLOT + lofs;
-            const T* Pp1 = ring + ((slot + 4) % 5) * M::SLOT + lofs;
+            // plane q-j sits in slot (slot + R - j) % R: x-2 = q-4, ..., x+2 = q
+            const T* Pm2 = ring + ((slot + R - 4) % R) * M::SLOT + lofs;
+            const T* Pm1 = ring + ((slot + R - 3) % R) * M::SLOT + lofs;
+            const T* P0 = ring + ((slot + R - 2) % R) * M::SLOT + lofs;
+            const T* Pp1 = ring + ((slot + R - 1) % R) * M::SLOT + lofs;
             const T* Pp2 = ring + slot * M::SLOT + lofs;
             const Mask mk = site_mask(p, x, y, z);
             const int64_t s = (int64_t)x * YZ + (int64_t)y * p.Z + z;
@@ -373,18 +375,30 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                 double phd[CT], Dd[3][CT];
 #pragma unroll
                 for (int c = C; c < CT; ++c) phd[c] = Dd[0][c] = Dd[1][c] = Dd[2][c] = 0.0;
-                // tap value in FP64: hi, or hi + lo for a compensated field
+                // difference of two tap values in FP64.  Compensated field: the
+                // difference of the high parts is split exactly into s + e (Knuth's
+                // TwoSum, FP32), e absorbs the difference of the low parts, and only s
+                // and that remainder are converted: two conversions instead of four,
+                // with an error below 2^-47 of the field's magnitude
                 const ptrdiff_t dlo = ring_lo - ring;
-                auto tap = [&](const T* q) -> double { return LO ? double(q[0]) + double(q[dlo]) : double(q[0]); };
+                auto dif = [&](const T* u, const T* v) -> double {
+                    if constexpr (LO) {
+                        const T ua = u[0], vb = -v[0];
+                        const T s = ua + vb, bb = s - ua;
+                        const T e = (ua - (s - bb)) + (vb - bb);
+                        return double(s) + double(e + (u[dlo] - v[dlo]));
+                    } else {
+                        return double(u[0]) - double(v[0]);
+                    }
+                };
 #pragma unroll
                 for (int c = 0; c < C; ++c) {
                     const int co = c * M::PLANE;
                     const T* f = P0 + co;
-                    phd[c] = tap(f);
-                    const double xd = tap(Pp1 + co) - tap(Pm1 + co), xd2 = tap(Pp2 + co) - tap(Pm2 + co);
-                    const double yd = tap(f + M::HZ) - tap(f - M::HZ);
-                    const double yd2 = tap(f + 2 * M::HZ) - tap(f - 2 * M::HZ);
-                    const double zd = tap(f + 1) - tap(f - 1), zd2 = tap(f + 2) - tap(f - 2);
+                    phd[c] = LO ? double(f[0]) + double(f[dlo]) : double(f[0]);
+                    const double xd = dif(Pp1 + co, Pm1 + co), xd2 = dif(Pp2 + co, Pm2 + co);
+                    const double yd = dif(f + M::HZ, f - M::HZ), yd2 = dif(f + 2 * M::HZ, f - 2 * M::HZ);
+                    const double zd = dif(f + 1, f - 1), zd2 = dif(f + 2, f - 2);
                     Dd[0][c] = mk.px ? kd.d1a[0] * xd - kd.d1b[0] * xd2 : 0.0;
                     Dd[1][c] = mk.py ? kd.d1a[1] * yd - kd.d1b[1] * yd2 : 0.0;
                     Dd[2][c] = mk.pz ? kd.d1a[2] * zd - kd.d1b[2] * zd2 : 0.0;
@@ -393,13 +407,17 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                     ksum_add(esum, Th<double>::energy(phd, Dd, p));
                     ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
                 } else {
-                    const double v = (DENS & 1) ? Th<double>::energy(phd, Dd, p) : Th<double>::baryon(phd, Dd, p);
+                    double v;
+                    if constexpr ((DENS & 4) != 0)
+                        v = Dynamics<Th>::potential(phd, Dd, p);  // potential of the RK4 dynamics
+                    else
+                        v = (DENS & 1) ? Th<double>::energy(phd, Dd, p) : Th<double>::baryon(phd, Dd, p);
                     ksum_add(esum, v);
                     epi.density(s, v);
                 }
             }
         }
-        slot = (slot + 1) % 5;
+        slot = (slot + 1) % R;
     }
 }
 

@@ -500,4 +500,50 @@ struct LightlyBound {
     }
 };
 
+// ===========================================================================
+// What the RK4 dynamics (killkinen = 0) conserves.  The kernels integrate
+// phi_c'' = -g_c.  H = (1/2) h^3 sum_c s_c |phi_c'|^2 + Phi is conserved when
+// g_c = s_c dPhi/dphi_c, up to the O(h^4) gap between the force stencils and
+// the energy stencils.  For the pure Skyrme variants and rho, Phi is the coded
+// energy and every s_c = +1.  The omega and Coulomb auxiliary fields are time
+// components of vector fields: their forces are anti-gradients (s_4 = -1) of
+//   omega:   Phi = E_pion - E_omega - c_omega omega B0
+//   Coulomb: Phi = E_pion / 2 - (kappa / 2) |grad V|^2 + kappa V B0
+// (E_pion: the coded energy without the auxiliary field's terms; the Coulomb
+// pion force is half the variation of its coded energy).  Signs and factors
+// were fixed by central differences of these potentials against the coded
+// forces.  Densities include the cell volume h^3, like the energies.
+// ===========================================================================
+template <template <typename> class Th>
+struct Dynamics {
+    static constexpr int C = Th<double>::C;
+    __device__ static double potential(const double* phi, const double (&D)[3][C], const Params& p) {
+        return Th<double>::energy(phi, D, p);
+    }
+    __host__ __device__ static constexpr double kinetic_sign(int) { return 1.0; }
+};
+
+template <>
+struct Dynamics<Omega> {
+    static constexpr int C = 5;
+    __device__ static double potential(const double* phi, const double (&D)[3][C], const Params& p) {
+        const double ew = p.vol * (0.5 * phi[4] * phi[4] + 0.5 * (D[0][4] * D[0][4] + D[1][4] * D[1][4] +
+                                                                   D[2][4] * D[2][4]));
+        const double e_pion = Omega<double>::energy(phi, D, p) - ew;
+        return e_pion - ew - p.c1 * phi[4] * Omega<double>::baryon(phi, D, p);
+    }
+    __host__ __device__ static constexpr double kinetic_sign(int c) { return c == 4 ? -1.0 : 1.0; }
+};
+
+template <>
+struct Dynamics<Coulomb> {
+    static constexpr int C = 5;
+    __device__ static double potential(const double* phi, const double (&D)[3][C], const Params& p) {
+        const double ev = p.vol * 0.5 * p.c1 * (D[0][4] * D[0][4] + D[1][4] * D[1][4] + D[2][4] * D[2][4]);
+        const double e_pion = Coulomb<double>::energy(phi, D, p) - ev;
+        return 0.5 * e_pion - ev + p.c1 * phi[4] * Coulomb<double>::baryon(phi, D, p);
+    }
+    __host__ __device__ static constexpr double kinetic_sign(int c) { return c == 4 ? -1.0 : 1.0; }
+};
+
 }  // namespace sky

@@ -152,6 +152,14 @@ class Engine:
     def xc(self, iid: int) -> int:
         return int(self._lib.sky_engine_get_xc(self._h, int(iid)))
 
+    def audit(self, iid: int) -> dict:
+        """FP64 energy audit of the RK4 dynamics of `iid`'s current state: the potential
+        `potential` whose (anti-)gradient the kernels integrate, the signed kinetic term
+        `kinetic` and their sum `hamiltonian` (conserved up to the O(h^4) stencil gap)."""
+        out = np.zeros(2)
+        self._call("sky_engine_audit", int(iid), f64p(out))
+        return {"potential": float(out[0]), "kinetic": float(out[1]), "hamiltonian": float(out[0] + out[1])}
+
     def set_active(self, iid: int, active: bool):
         self._call("sky_engine_set_active", int(iid), 1 if active else 0)
 

@@ -324,3 +324,27 @@ def test_fp32d_schedule_reaches_the_fp64_fixed_point():
     assert sd.gabs <= 1e-6, (sd, n, m)
     assert abs(sd.energy - s64.energy) <= 1e-8 * abs(s64.energy), (sd.energy, s64.energy)
     assert sc.gabs > 1e-6
+
+
+@pytest.mark.parametrize("name,precision", [("coulomb", "fp64"), ("omega", "fp64"), ("coulomb", "fp32c"),
+                                            ("rho", "fp32"), ("rho", "fp64"), ("nuclear", "fp32d")])
+def test_energy_audit_matches_the_oracle(name, precision):
+    """sky_engine_audit: the dynamics potential and the signed kinetic term of the current
+    state, in FP64 (hi + lo for a compensated field), against the oracle restatement
+    (tests/_dynamics.py) on the field and velocity read back: only the summation order
+    differs, so the tolerance is 1e-10 relative."""
+    tol = 1e-10
+    from skyrmion_solver_b200.engine import Engine
+    from tests import _dynamics as DY
+    d, F, V, p_i, p_f = _inputs(name)
+    rng = np.random.default_rng(4)
+    V = rng.uniform(-0.05, 0.05, size=F.shape)
+    with Engine(0) as eng:
+        i = eng.add(name, (p_i, p_f), F, V, precision=precision)
+        a = eng.audit(i)
+        f, v = eng.read(i)
+    phi = DY.potential(name, f, p_i, p_f)
+    kin = DY.kinetic(name, v, p_f)
+    assert abs(a["potential"] - phi) <= tol * max(1.0, abs(phi)), (a, phi)
+    assert abs(a["kinetic"] - kin) <= tol * max(1.0, abs(kin)), (a, kin)
+    assert a["hamiltonian"] == pytest.approx(a["potential"] + a["kinetic"])
