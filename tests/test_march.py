@@ -107,7 +107,7 @@ def test_plain_gradient_geometry(options, name, dims):
         assert G.rel_err(l, ref_l) <= GRAD_TOL
 
 
-@pytest.mark.parametrize("name", ["nuclear", "omega", "coulomb"])
+@pytest.mark.parametrize("name", ["nuclear", "omega", "coulomb", "rho"])
 def test_engine_fp64_chunked(name):
     from skyrmion_solver_b200.engine import Engine
     dims = (29, 19, 45)
