@@ -762,7 +762,7 @@ def run_dynamics(args):
     """Two B=2 toroidal (z^2 rational map) skyrmions at x = -/+3, the second isorotated by a seeded
     Haar-random SU(2) element, combined by quaternion product, boosted toward each other at relative
     velocity 0.3 (V = -u(x) d_x phi projected orthogonal to phi, u = 0.15 tanh(-x)), Coulomb variant
-    (or --theory), side^3 sites with h = 0.15, dt = 0.1 h, killkinen = 0 (RK4 dynamics), compensated
+    (or --theory), side^3 sites with h = 0.15 (or --h), dt = 0.1 h, killkinen = 0 (RK4 dynamics), compensated
     FP32 (or --precision).  Every 50 steps the FP64 energy audit (sky_engine_audit) evaluates the
     potential Phi that the kernels integrate and K = (1/2) h^3 sum_c s_c |V_c|^2; H = Phi + K."""
     import numpy as np
@@ -771,7 +771,7 @@ def run_dynamics(args):
     from skyrmion_solver_b200 import initial as ini
     from skyrmion_solver_b200 import theories as T
     torch.cuda.set_device(0)
-    L, h = args.side, 0.15
+    L, h = args.side, args.h
     name = args.theory
     th = T.by_short_name(name)
     prm = th.params.default_params(xlen=L, ylen=L, zlen=L, lsx=h, lsy=h, lsz=h, xsize=h * (L - 1),
@@ -821,7 +821,7 @@ def run_dynamics(args):
             t_audit += time.perf_counter() - t0
     H = [phi + k for _, phi, k, _, _ in audit]
     drift = [abs(v - H[0]) / abs(H[0]) for v in H]
-    emit({"mode": "dynamics", "theory": name, "sites": L ** 3, "steps": args.steps,
+    emit({"mode": "dynamics", "theory": name, "sites": L ** 3, "h": h, "dt": 0.1 * h, "steps": args.steps,
           "ms_per_step": t_dev / args.steps,
           "site_steps_per_s": L ** 3 * args.steps / (t_dev * 1e-3), "precision": args.precision,
           "audit_ms": 1e3 * t_audit / max(1, len(audit) - 1),
@@ -860,6 +860,7 @@ def main():
     ap.add_argument("--side", type=int, default=192)
     ap.add_argument("--theory", choices=("coulomb", "nuclear", "omega"), default="coulomb",
                     help="dynamics: theory variant")
+    ap.add_argument("--h", type=float, default=0.15, help="dynamics: lattice spacing (dt = 0.1 h)")
     ap.add_argument("--precision", choices=("fp32c", "fp32", "fp32d", "fp64"), default="fp32c",
                     help="dynamics: engine precision")
     args = ap.parse_args()

@@ -73,18 +73,26 @@ struct Engine {
 template <template <typename> class Th, typename T>
 using EShape = typename GradTile<Th<T>::C, T>::type;
 
-// Theories with at most five components run the marching kernels
-// (sky_march.cuh) in both precisions; the 13-component rho variant runs them in
-// FP32 (one block of 200 KB per SM) and keeps the 3-D tile kernel in FP64, whose
-// planes would need 400 KB of shared memory.
+// Every theory runs the marching kernels (sky_march.cuh) in both precisions.
+// Tiles are 8 rows x 32 columns, except for FP64 rho (13 components): its
+// 4-row tiles keep the five-plane ring at 150 KB, narrow rows only, with two
+// of stage 3/4's three sources staged (one block per SM).
 template <template <typename> class Th, typename T = float>
 constexpr bool uses_march() {
-    return Th<float>::C <= 5 || sizeof(T) == 4;
+    return true;
 }
 constexpr int kMarchBY = 8;
+template <template <typename> class Th, typename T>
+constexpr int march_by() {
+    return (Th<float>::C > 5 && sizeof(T) == 8) ? 4 : kMarchBY;
+}
+template <template <typename> class Th, typename T>
+constexpr bool march_wide_allowed() {
+    return !(Th<float>::C > 5 && sizeof(T) == 8);
+}
 // Wide-row (16-byte staged) or narrow-row march shape.
 template <template <typename> class Th, typename T, bool WIDE>
-using MShape = MarchShape<Th<T>::C, kMarchBY, WIDE>;
+using MShape = MarchShape<Th<T>::C, march_by<Th, T>(), WIDE && march_wide_allowed<Th, T>()>;
 
 template <int STAGE>
 constexpr int stage_nsrc() {
@@ -254,7 +262,7 @@ static int shape_of(int prec, int& bz, int& by, int& tx, int& per_sm) {
     per_sm = 1;
     if (prec) {
         if constexpr (uses_march<Th, double>()) {
-            bz = 32, by = kMarchBY, tx = 0;
+            bz = 32, by = march_by<Th, double>(), tx = 0;
             return stage_setup<Th, double, 4>(&per_sm);
         } else {
             using S = EShape<Th, double>;

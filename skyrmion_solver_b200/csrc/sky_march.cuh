@@ -33,6 +33,8 @@ namespace sky {
 // 16 / sizeof(T) so that every 16-byte chunk of a row starts on a 16-byte boundary
 // and lies wholly inside or (as the first chunk at z0 = 0) wholly outside the lattice
 // in z; a chunk crossing z = Z copies its in-lattice part and zero-fills the rest.
+constexpr size_t kMaxSmemPerBlock = 232448;  // 227 KB of dynamic shared memory per block
+
 template <int C_, int BY_, bool WIDE_ = false>
 struct MarchShape {
     static constexpr int C = C_, BY = BY_, BZ = 32;
@@ -44,11 +46,19 @@ struct MarchShape {
     static constexpr int RING = 5;
     static constexpr int NTHREADS = BZ * BY;
     static constexpr int NPER = (SLOT + NTHREADS - 1) / NTHREADS;  // plane elements per thread
+    // Sources staged through shared memory: all nsrc, or only the first two when
+    // three would not fit in one block's 227 KB (FP64 rho); the third source is
+    // then read from global memory while the plane is combined.
+    template <typename T, typename S = T>
+    static constexpr int staged(int nsrc) {
+        return (nsrc == 3 && size_t(RING) * SLOT * sizeof(T) + 3 * size_t(SLOT) * sizeof(S) > kMaxSmemPerBlock) ? 2
+                                                                                                            : nsrc;
+    }
     // ring + staging (+ a second ring for the low parts of a compensated field);
     // the staging area holds values of the source type S
     template <typename T, typename S = T>
     static constexpr size_t smem_bytes(int nsrc, bool lo = false) {
-        return size_t(RING) * (lo ? 2 : 1) * SLOT * sizeof(T) + size_t(nsrc) * SLOT * sizeof(S);
+        return size_t(RING) * (lo ? 2 : 1) * SLOT * sizeof(T) + size_t(staged<T, S>(nsrc)) * SLOT * sizeof(S);
     }
 };
 
@@ -213,6 +223,24 @@ __device__ __forceinline__ void plane_combine(T* __restrict__ slot, const S* __r
     }
 }
 
+// As plane_combine for three sources of which only the first two were staged:
+// the third (src2, element offsets of the plane at plane_base) is read from
+// global memory here.
+template <class M, typename T, typename S = T>
+__device__ __forceinline__ void plane_combine_g(T* __restrict__ slot, const S* __restrict__ stage, T a, T b,
+                                                const PlaneOffsets<M>& po, const S* __restrict__ src2,
+                                                int64_t plane_base, bool xok) {
+    const int tid = threadIdx.x + M::BZ * threadIdx.y;
+#pragma unroll
+    for (int k = 0; k < M::NPER; ++k) {
+        const int idx = tid + k * M::NTHREADS;
+        if (M::SLOT % M::NTHREADS == 0 || idx < M::SLOT) {
+            const T l = (xok && src2 != nullptr && po.off[k] >= 0) ? T(__ldg(src2 + plane_base + po.off[k])) : T(0);
+            slot[idx] = T(stage[idx]) + a * T(stage[M::SLOT + idx]) + b * l;
+        }
+    }
+}
+
 // Raw first-difference sum c_m f[m*st], c = (1, -8, 0, 8, -1) for m = -2..2.
 template <typename T>
 __device__ __forceinline__ T diff5(const T* f, int st) {
@@ -251,6 +279,8 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     static_assert(!LO || (DENS != 0 && NSRC == 2), "low-part ring only for the stage-1 density");
     static_assert(!LO || (std::is_same<S, T>::value && sizeof(T) == 4), "low-part ring needs FP32 sources");
     constexpr bool DIRECT = (NSRC == 1 || LO) && std::is_same<S, T>::value;
+    constexpr int NST = M::template staged<T, S>(NSRC);  // sources staged in shared memory
+    static_assert(NST == NSRC || !M::WIDE, "the unstaged third source is read with narrow-row offsets");
     constexpr int R = DIRECT ? M::RING + 1 : M::RING;  // ring slots
     constexpr int DST = DIRECT ? R * M::SLOT : M::SLOT;  // distance between the sources' copies
     // shared memory: DIRECT: ring (R slots) [+ low-part ring (R slots)];
@@ -281,9 +311,9 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     auto issue = [&](int64_t base, bool xok, int dslot) {
         S* dst = DIRECT ? reinterpret_cast<S*>(ring + dslot * M::SLOT) : stage;
         if constexpr (M::WIDE)
-            plane_issue_wide<M, NSRC, S, DST>(dst, po, src, base, xok);
+            plane_issue_wide<M, NST, S, DST>(dst, po, src, base, xok);
         else
-            plane_issue<M, NSRC, S, DST>(dst, po, src, base, xok);
+            plane_issue<M, NST, S, DST>(dst, po, src, base, xok);
     };
     __syncthreads();
     issue((int64_t)q0 * YZ, q0 >= 0 && q0 < p.X, 0);
@@ -296,10 +326,15 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
         if constexpr (DIRECT) {
             if (q < q1) issue((int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X, slot + 1 == R ? 0 : slot + 1);
         } else {
-            if constexpr (M::WIDE)
+            if constexpr (NST < NSRC) {
+                if constexpr (!M::WIDE)
+                    plane_combine_g<M, T, S>(ring + slot * M::SLOT, stage, a, b, po, src[2], (int64_t)q * YZ,
+                                             q >= 0 && q < p.X);
+            } else if constexpr (M::WIDE) {
                 plane_combine_wide<M, NSRC, T, S>(ring + slot * M::SLOT, stage, a, b);
-            else
+            } else {
                 plane_combine<M, NSRC, T, S>(ring + slot * M::SLOT, stage, a, b);
+            }
             if (q < q1) issue((int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X, 0);
             __syncthreads();  // (B) slot complete
         }
