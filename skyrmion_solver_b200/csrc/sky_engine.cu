@@ -62,7 +62,8 @@ struct Engine {
     std::map<int, HostInst> insts;
     int next_id = 0;
     Group groups[6][2];
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;   // kGraphSteps steps
+    cudaGraphExec_t graph1 = nullptr;  // one step (the remainder of a step call)
     bool graph_valid = false;
     int64_t bytes = 0;
 };
@@ -656,28 +657,37 @@ static int count_launches(Engine& e) {
     return n;
 }
 
-static int build_graph(Engine& e) {
-    if (e.graph) {
-        cudaGraphExecDestroy(e.graph);
-        e.graph = nullptr;
+// Capture `nsteps` steps of the current instance set into *exec.
+static int capture_steps(Engine& e, int nsteps, cudaGraphExec_t* exec) {
+    if (*exec) {
+        cudaGraphExecDestroy(*exec);
+        *exec = nullptr;
     }
-    int rc = SKY_OK;
-    for (int t = 0; t < 6; ++t)
-        for (int pr = 0; pr < 2; ++pr)
-            if (!e.groups[t][pr].members.empty() && (rc = setup_group(e.groups[t][pr]))) return rc;
     cudaGraph_t graph;
-    rc = check_cuda(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal), "begin capture", __LINE__);
+    int rc = check_cuda(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal), "begin capture",
+                        __LINE__);
     if (rc) return rc;
-    for (int s = 0; s < kGraphSteps && rc == SKY_OK; ++s) rc = record_step(e);
+    for (int s = 0; s < nsteps && rc == SKY_OK; ++s) rc = record_step(e);
     cudaError_t ce = cudaStreamEndCapture(e.stream, &graph);
     if (rc) {
         if (ce == cudaSuccess) cudaGraphDestroy(graph);
         return rc;
     }
     if ((rc = check_cuda(ce, "end capture", __LINE__))) return rc;
-    rc = check_cuda(cudaGraphInstantiate(&e.graph, graph, 0), "graph instantiate", __LINE__);
+    rc = check_cuda(cudaGraphInstantiate(exec, graph, 0), "graph instantiate", __LINE__);
     cudaGraphDestroy(graph);
-    if (rc) return rc;
+    return rc;
+}
+
+// The step graphs: kGraphSteps steps, and one step for the remainder of a call.
+// Each step depends only on device-side state, so replaying them is the same as
+// launching the kernels one by one.
+static int build_graph(Engine& e) {
+    int rc = SKY_OK;
+    for (int t = 0; t < 6; ++t)
+        for (int pr = 0; pr < 2; ++pr)
+            if (!e.groups[t][pr].members.empty() && (rc = setup_group(e.groups[t][pr]))) return rc;
+    if ((rc = capture_steps(e, kGraphSteps, &e.graph)) || (rc = capture_steps(e, 1, &e.graph1))) return rc;
     e.graph_valid = true;
     return SKY_OK;
 }
@@ -789,6 +799,7 @@ int sky_engine_destroy(void* handle) {
     cudaSetDevice(e->device);
     cudaStreamSynchronize(e->stream);
     if (e->graph) cudaGraphExecDestroy(e->graph);
+    if (e->graph1) cudaGraphExecDestroy(e->graph1);
     for (auto& kv : e->insts) free_inst(kv.second);
     for (int t = 0; t < 6; ++t)
         for (int p = 0; p < 2; ++p) {
@@ -1048,15 +1059,13 @@ int sky_engine_step(void* handle, int nsteps) {
     cudaSetDevice(e->device);
     int rc;
     int done = 0;
-    if (nsteps >= kGraphSteps) {
-        if (!e->graph_valid && (rc = build_graph(*e))) return rc;
-        while (nsteps - done >= kGraphSteps) {
-            if ((rc = check_cuda(cudaGraphLaunch(e->graph, e->stream), "graph launch", __LINE__))) return rc;
-            done += kGraphSteps;
-        }
+    if (nsteps > 0 && !e->graph_valid && (rc = build_graph(*e))) return rc;
+    while (nsteps - done >= kGraphSteps) {
+        if ((rc = check_cuda(cudaGraphLaunch(e->graph, e->stream), "graph launch", __LINE__))) return rc;
+        done += kGraphSteps;
     }
     for (; done < nsteps; ++done)
-        if ((rc = record_step(*e))) return rc;
+        if ((rc = check_cuda(cudaGraphLaunch(e->graph1, e->stream), "graph launch", __LINE__))) return rc;
     for (auto& kv : e->insts)
         if (kv.second.active) kv.second.steps += nsteps;
     return SKY_OK;

@@ -225,20 +225,43 @@ __device__ __forceinline__ void plane_combine(T* __restrict__ slot, const S* __r
 
 // As plane_combine for three sources of which only the first two were staged:
 // the third (src2, element offsets of the plane at plane_base) is read from
-// global memory here.
+// global memory here, in groups of eight loads issued back to back (one memory
+// latency per group); plane_prefetch_l2 brought its lines into L2 one plane
+// earlier.
 template <class M, typename T, typename S = T>
 __device__ __forceinline__ void plane_combine_g(T* __restrict__ slot, const S* __restrict__ stage, T a, T b,
                                                 const PlaneOffsets<M>& po, const S* __restrict__ src2,
                                                 int64_t plane_base, bool xok) {
+    constexpr int G = 8;
     const int tid = threadIdx.x + M::BZ * threadIdx.y;
+    const bool any = xok && src2 != nullptr;
 #pragma unroll
-    for (int k = 0; k < M::NPER; ++k) {
-        const int idx = tid + k * M::NTHREADS;
-        if (M::SLOT % M::NTHREADS == 0 || idx < M::SLOT) {
-            const T l = (xok && src2 != nullptr && po.off[k] >= 0) ? T(__ldg(src2 + plane_base + po.off[k])) : T(0);
-            slot[idx] = T(stage[idx]) + a * T(stage[M::SLOT + idx]) + b * l;
+    for (int k0 = 0; k0 < M::NPER; k0 += G) {
+        T l[G];
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            const int k = k0 + j;
+            l[j] = T(0);
+            if (k < M::NPER && any && po.off[k] >= 0) l[j] = T(__ldg(src2 + plane_base + po.off[k]));
+        }
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            const int k = k0 + j;
+            const int idx = tid + k * M::NTHREADS;
+            if (k < M::NPER && (M::SLOT % M::NTHREADS == 0 || idx < M::SLOT))
+                slot[idx] = T(stage[idx]) + a * T(stage[M::SLOT + idx]) + b * l[j];
         }
     }
+}
+
+// L2 prefetch of the thread's elements of one plane of src (narrow-row offsets).
+template <class M, typename S>
+__device__ __forceinline__ void plane_prefetch_l2(const PlaneOffsets<M>& po, const S* src, int64_t plane_base,
+                                                  bool xok) {
+    if (!xok || src == nullptr) return;
+#pragma unroll
+    for (int k = 0; k < M::NPER; ++k)
+        if (po.off[k] >= 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(src + plane_base + po.off[k]));
 }
 
 // Raw first-difference sum c_m f[m*st], c = (1, -8, 0, 8, -1) for m = -2..2.
@@ -310,10 +333,12 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     const int lofs = (ty + 2) * M::HZ + (tx + M::ZOFF);  // thread's site within a component plane
     auto issue = [&](int64_t base, bool xok, int dslot) {
         S* dst = DIRECT ? reinterpret_cast<S*>(ring + dslot * M::SLOT) : stage;
-        if constexpr (M::WIDE)
+        if constexpr (M::WIDE) {
             plane_issue_wide<M, NST, S, DST>(dst, po, src, base, xok);
-        else
+        } else {
             plane_issue<M, NST, S, DST>(dst, po, src, base, xok);
+            if constexpr (NST < NSRC) plane_prefetch_l2<M, S>(po, src[2], base, xok);
+        }
     };
     __syncthreads();
     issue((int64_t)q0 * YZ, q0 >= 0 && q0 < p.X, 0);

@@ -285,7 +285,7 @@ int choose_xc(int X, int tiles_yz, int resident) {
 }
 
 // Library options (sky_set_option): key 0 = kernel family of the
-// reference-layout gradient (1 = marching kernels for C <= 5, 0 = 3-D tile
+// reference-layout gradient and densities (1 = marching kernels, 0 = 3-D tile
 // kernels); key 1 = x-chunk of those marching launches (0 = automatic).
 static int g_options[4] = {1, 0, 0, 0};
 int option(int key) { return (key >= 0 && key < 4) ? g_options[key] : 0; }
@@ -293,9 +293,11 @@ int option(int key) { return (key >= 0 && key < 4) ? g_options[key] : 0; }
 // ---------------------------------------------------------------------------
 // templated launchers
 // ---------------------------------------------------------------------------
-template <template <typename> class Th, typename T, bool WIDE>
+// BY = 8-row tiles, or 4 for FP64 rho (13 components), whose 8-row ring would
+// not fit in shared memory.
+template <template <typename> class Th, typename T, bool WIDE, int BY = 8>
 int launch_gradient_march(const Params& p, const T* field, T* eg, T* l, cudaStream_t st) {
-    using M = MarchShape<Th<T>::C, 8, WIDE>;
+    using M = MarchShape<Th<T>::C, BY, WIDE>;
     auto kern = k_march_plain<Th, M, T>;
     const size_t smem = M::template smem_bytes<T>(1);
     static int per_sm = 0;
@@ -386,15 +388,18 @@ int grad64(const Params& p, const double* f, double* eg, double* l, cudaStream_t
                 return launch_gradient_march<Th, double, true>(p, f, eg, l, st);
             return launch_gradient_march<Th, double, false>(p, f, eg, l, st);
         }
+    } else {
+        if (option(0) == 1 && (int64_t)p.C * n_sites(p) < ((int64_t)1 << 31))
+            return launch_gradient_march<Th, double, false, 4>(p, f, eg, l, st);
     }
     return launch_gradient<Th, double, double>(p, f, eg, l, st);
 }
-// Marching FP64 density with its fused compensated sum (energy: all C <= 5
-// components; baryon: phi_0..3 of any theory).
-template <template <typename> class Th, int MODE, bool WIDE>
+// Marching FP64 density with its fused compensated sum (energy: all components,
+// in 4-row tiles for rho; baryon: phi_0..3 of any theory).
+template <template <typename> class Th, int MODE, bool WIDE, int BY = 8>
 int launch_density_march(const Params& p, const double* field, double* dens, double* scratch, double* out_dev,
                          cudaStream_t st) {
-    using M = MarchShape<(MODE == 0 ? Th<double>::C : 4), 8, WIDE>;
+    using M = MarchShape<(MODE == 0 ? Th<double>::C : 4), BY, WIDE>;
     auto kern = k_march_density<Th, M, MODE>;
     const size_t smem = M::template smem_bytes<double>(1);
     static int per_sm = 0;
@@ -436,6 +441,8 @@ int dens64(const Params& p, int mode, const double* f, double* dens, double* scr
     if (march && mode == 1) return density_march<Th, 1>(p, f, dens, scratch, out_dev, st);
     if constexpr (Th<double>::C <= 5) {
         if (march) return density_march<Th, 0>(p, f, dens, scratch, out_dev, st);
+    } else {
+        if (march) return launch_density_march<Th, 0, false, 4>(p, f, dens, scratch, out_dev, st);
     }
     return mode == 0 ? launch_density<Th, 0, double>(p, f, dens, scratch, out_dev, st)
                      : launch_density<Th, 1, double>(p, f, dens, scratch, out_dev, st);

@@ -127,13 +127,28 @@ def test_graph_replay_equals_single_steps():
     with Engine(0) as a, Engine(0) as b:
         ia = a.add("omega", (p_i, p_f), F, V, precision="fp32")
         ib = b.add("omega", (p_i, p_f), F, V, precision="fp32")
-        a.step(16)                  # two graph replays
+        a.step(16)                  # two replays of the eight-step graph
         for _ in range(16):
-            b.step(1)               # direct launches
+            b.step(1)               # sixteen replays of the one-step graph
         fa, va = a.read(ia)
         fb, vb = b.read(ib)
         assert np.array_equal(fa, fb) and np.array_equal(va, vb)
         assert a.stats(ia).energy == b.stats(ib).energy
+
+
+def test_uncaptured_launches_equal_graph_replay():
+    """The per-stage timing pass launches each kernel outside any graph; it advances the
+    state exactly as the graph replays do."""
+    from skyrmion_solver_b200.engine import Engine
+    d, F, V, p_i, p_f = _inputs("omega")
+    with Engine(0) as a, Engine(0) as b:
+        ia = a.add("omega", (p_i, p_f), F, V, precision="fp32d")
+        ib = b.add("omega", (p_i, p_f), F, V, precision="fp32d")
+        a.step(5)
+        b.time_stages(5)
+        fa, va = a.read(ia)
+        fb, vb = b.read(ib)
+        assert np.array_equal(fa, fb) and np.array_equal(va, vb)
 
 
 def test_precision_switch_and_remove(engine):

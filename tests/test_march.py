@@ -89,7 +89,7 @@ def _plain_gradient(name, F, p_i, p_f):
     return eg.cpu().numpy().reshape(F.shape), l.cpu().numpy().reshape(F.shape)
 
 
-@pytest.mark.parametrize("name", ["nuclear", "omega", "coulomb", "berger", "lightly_bound"])
+@pytest.mark.parametrize("name", ["nuclear", "omega", "coulomb", "rho", "berger", "lightly_bound"])
 @pytest.mark.parametrize("dims", [(37, 21, 70), (9, 33, 5), (6, 6, 40)])
 def test_plain_gradient_geometry(options, name, dims):
     th, p_i, p_f = params_for(name, dims)
