@@ -109,6 +109,19 @@ int sky_set_field_zero(const int32_t* p_i, int32_t n_pi, double* field, void* st
 int sky_create_grid(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf, double* grid,
                     void* stream);
 
+/* Initial field on the device (replaces the reference's initial-configuration
+ * kernels, th/nuclear_skyrme/initial_config.py:583-627, 664-698, 941-953,
+ * 1082-1126): the normalised quaternion product, in order, of nsol <= 48
+ * solitons with profile f(r) = pi exp(-r / scale).  Soliton k has baryon
+ * number baryon[k] (1: hedgehog; 2 or 4: the rational maps z^2 and the cubic
+ * map), centre centers[3k..3k+2] and isorotation quats[4k..4k+3] (unit
+ * quaternion; quats may be NULL).  nsol = 0 gives the vacuum.  Components
+ * 4..C-1 are zeroed, and the outer vacuum_shell sites of every face are set to
+ * the vacuum.  field: device buffer of C*N doubles. */
+int sky_init_field(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf, int32_t nsol,
+                   const int32_t* baryon, const double* centers, const double* quats, double scale,
+                   int32_t vacuum_shell, double* field, void* stream);
+
 /* Replace compute_sum / compute_max (core/utils.py:201-279, 321-373):
  * deterministic FP64 reductions (compensated sum; signed max).  `scratch` is a
  * device buffer of sky_reduce_scratch_size(n) doubles; the result is written to

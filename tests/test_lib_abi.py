@@ -51,3 +51,19 @@ def test_invalid_arguments_rejected_before_launch():
     # scratch too small
     out = ctypes.c_double()
     assert lib.sky_sum(dummy, 10, dummy, 4, ctypes.byref(out), None, None) == 5
+
+
+def test_init_field_rejects_bad_soliton_lists():
+    lib = _lib.load()
+    pf = np.array([1, 1, 1, 0.2, 0.2, 0.2, 0.008, 0.1, 1.0, 1.0], dtype=np.float64)
+    dummy = ctypes.c_void_p(16)
+    b = np.ones(64, np.int32)
+    c = np.zeros(3 * 64)
+    q = np.tile([1.0, 0.0, 0.0, 0.0], 64)
+    args = (_lib.i32p(_pi()), 11, _lib.f64p(pf), 10)
+    assert lib.sky_init_field(*args, 49, _lib.i32p(b), _lib.f64p(c), _lib.f64p(q), 1.5, 0, dummy, None) == 1
+    b3 = b.copy()
+    b3[0] = 3                                         # no B = 3 rational map
+    assert lib.sky_init_field(*args, 1, _lib.i32p(b3), _lib.f64p(c), _lib.f64p(q), 1.5, 0, dummy, None) == 1
+    assert lib.sky_init_field(*args, 1, _lib.i32p(b), _lib.f64p(c), _lib.f64p(q), 0.0, 0, dummy, None) == 1
+    assert lib.sky_init_field(*args, 1, _lib.i32p(b), _lib.f64p(c), _lib.f64p(q), 1.5, 0, None, None) == 1
