@@ -207,6 +207,27 @@ class Engine:
         self._call("sky_engine_read", int(iid), _lib.dptr(field_out),
                    _lib.dptr(velocity_out) if velocity_out is not None else None, 1)
 
+    def view(self, iid: int, density: str = "baryon"):
+        """The FP64 buffers a renderer reads, materialised on the device from an instance of any
+        precision: the reference's ``sim.Field`` (reference layout, C*N values) and ``sim.en``
+        after ``compute_baryon_density()`` (b h^3 per site) or the energy kernel (e h^3), as read
+        by th/nuclear_skyrme/render_gl.py:157-222.  Returns (field, en) CUDA tensors; nothing
+        passes through the host."""
+        import torch
+        if density not in ("baryon", "energy"):
+            raise ValueError("density must be 'baryon' or 'energy'")
+        m = self.meta[iid]
+        N = int(m["p_i"][6])
+        dev = torch.device("cuda", self.device)
+        field = torch.empty(m["C"] * N, dtype=torch.float64, device=dev)
+        torch.cuda.current_stream(dev).synchronize()   # the engine writes on its own stream
+        self.read_device(iid, field)                   # synchronous on the engine's stream
+        en = torch.zeros(N, dtype=torch.float64, device=dev)
+        fn = "sky_baryon_density" if density == "baryon" else "sky_energy_density"
+        _lib.call(fn, m["theory"], i32p(m["p_i"]), len(m["p_i"]), f64p(m["p_f"]), len(m["p_f"]), _lib.dptr(en),
+                  _lib.dptr(field), _lib.stream_ptr(torch.cuda.current_stream(dev)))
+        return field, en
+
     def time_stages(self, nsteps: int) -> dict:
         """Advance nsteps un-captured steps timing each launch kind with CUDA events (ms per step)."""
         out = (ctypes.c_double * 6)()

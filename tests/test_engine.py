@@ -363,3 +363,22 @@ def test_energy_audit_matches_the_oracle(name, precision):
     assert abs(a["potential"] - phi) <= tol * max(1.0, abs(phi)), (a, phi)
     assert abs(a["kinetic"] - kin) <= tol * max(1.0, abs(kin)), (a, kin)
     assert a["hamiltonian"] == pytest.approx(a["potential"] + a["kinetic"])
+
+
+@pytest.mark.parametrize("density", ["baryon", "energy"])
+def test_renderer_view_of_a_compensated_instance(density):
+    """Engine.view materialises the renderer's FP64 buffers (field and per-site density) on the
+    device from a compensated FP32 instance; they equal the oracle's densities of the field."""
+    import torch
+    from skyrmion_solver_b200.engine import Engine
+    d, F, V, p_i, p_f = _inputs("omega")
+    with Engine(0) as eng:
+        i = eng.add("omega", (p_i, p_f), F, V, precision="fp32c")
+        eng.step(3)
+        field, en = eng.view(i, density)
+        torch.cuda.synchronize()
+        f, _ = eng.read(i)
+    assert np.array_equal(field.cpu().numpy().reshape(f.shape), f)
+    fn = O.baryon_density if density == "baryon" else O.energy_density
+    ref = fn(O.THEORIES["omega"], f, p_i, p_f)
+    assert G.rel_err(en.cpu().numpy().reshape(ref.shape), ref) <= 1e-12
