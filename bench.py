@@ -594,7 +594,6 @@ def serve_requests(n, rate, seed, mix, bmax, max_side, tol, max_steps):
     import numpy as np
     from skyrmion_solver_b200 import theories as T
     from skyrmion_solver_b200.serving import Request, poisson_arrivals
-    from skyrmion_solver_b200.theories._init_common import build_host_field
     rng = np.random.default_rng(seed)
     names = list(mix)
     w = np.array([mix[k] for k in names], dtype=np.float64)
@@ -614,8 +613,8 @@ def serve_requests(n, rate, seed, mix, bmax, max_side, tol, max_steps):
         p_i = np.asarray(p_i, np.int32)
         p_f = np.asarray(p_f, np.float64)
         cfg = {"mode": "smorgasbord", "count": B, "seed": seed * 1000 + k, "scale": 1.5, "vacuum_shell": 2}
-        f = build_host_field(name, p_i, p_f, cfg)
-        reqs.append((Request(k, name, p_i, p_f, f, float(arrivals[k]), tol, max_steps), prm, th))
+        # the field is built on the device when the request is admitted (sky_init_field)
+        reqs.append((Request(k, name, p_i, p_f, None, float(arrivals[k]), tol, max_steps, init=cfg), prm, th))
     return reqs
 
 
@@ -625,18 +624,13 @@ def run_serve(args):
     from skyrmion_solver_b200.core.simulation import Simulation
     from skyrmion_solver_b200.engine import Engine
     from skyrmion_solver_b200.serving import Server
-    from skyrmion_solver_b200.theories._init_common import seed_omega
+    from skyrmion_solver_b200.theories._init_common import build_device_field, seed_omega
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
     mix = dict(kv.split(":") for kv in args.mix.split(","))
     mix = {k: float(v) for k, v in mix.items()}
     reqs = serve_requests(args.requests, args.rate, args.seed, mix, args.bmax, args.max_side, GRAD_TOL,
                           args.max_steps)
-    for r, _, _ in reqs:           # omega: seed the omega component as -c_omega B0, on the device
-        if r.theory == "omega":
-            t = torch.from_numpy(r.field.ravel().copy()).to(dev)
-            seed_omega(t, r.p_i, r.p_f)
-            r.field = t.cpu().numpy().reshape(r.field.shape)
     # 1. continuous batching on the resident engine
     with Engine(0) as eng:
         srv = Server(eng, chunk=64, fp32_mode=args.schedule)
@@ -650,7 +644,10 @@ def run_serve(args):
     t_all = 0.0
     for r, prm, th in reqs:
         sim = Simulation(prm, th)
-        sim.Field.copy_(torch.from_numpy(r.field.ravel()).to(dev))
+        f0 = build_device_field(r.theory, r.p_i, r.p_f, r.init)      # the same field the server built
+        if r.theory == "omega":
+            seed_omega(f0, r.p_i, r.p_f)
+        sim.Field.copy_(f0)
         sim.Velocity.zero_()
         e = sim.observables()["energy"]
         torch.cuda.synchronize()

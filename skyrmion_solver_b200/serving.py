@@ -1,7 +1,8 @@
 """Continuous-batching request loop over the resident engine.
 
 Requests (one relaxation each: a theory, its packed parameters and an initial
-FP64 field) arrive open-loop.  The loop:
+FP64 field, or an initial configuration that is built on the device at
+admission) arrive open-loop.  The loop:
 
 * admits pending requests whose arrival time has passed, in arrival order,
   while the engine's device memory plus the request's estimate stays under the
@@ -38,10 +39,11 @@ class Request:
     theory: str
     p_i: np.ndarray
     p_f: np.ndarray
-    field: np.ndarray               # (C, X, Y, Z) FP64, reference layout
+    field: np.ndarray | None        # (C, X, Y, Z) FP64, reference layout; None: built from `init`
     arrival: float = 0.0            # seconds after the loop starts
     tol: float = 1e-6               # FP64 gradient max-norm at which the solve is converged
     max_steps: int = 1_000_000
+    init: dict | None = None        # initial configuration built on the device at admission
 
 
 @dataclass
@@ -165,7 +167,8 @@ class Server:
                 break                                   # wait for a retirement to free memory
             self.pending.pop(0)
             try:
-                iid = self.engine.add(req.theory, (req.p_i, req.p_f), req.field, None, precision=self.fp32_mode)
+                field = req.field if req.field is not None else self._device_field(req)
+                iid = self.engine.add(req.theory, (req.p_i, req.p_f), field, None, precision=self.fp32_mode)
             except MemoryError:
                 self.results.append(Result(req.rid, "failed", math.nan, math.nan, math.nan, 0, 0, req.arrival, t,
                                            t))
@@ -176,6 +179,15 @@ class Server:
             self.live[iid] = _Live(req, iid, "fp64" if self.fp32_mode == "fp64" else "fp32", t,
                                    rule=PlateauRule(self._switch_tol(req), self.plateau_chunks * self.chunk,
                                                     self.plateau_gain))
+
+    def _device_field(self, req: Request):
+        """The request's initial field built on the engine's device (sky_init_field), with the
+        omega component seeded as -c_omega B0 for the omega variant; no host field is made."""
+        from .theories._init_common import build_device_field, seed_omega
+        f = build_device_field(req.theory, req.p_i, req.p_f, req.init or {}, device=self.engine.device)
+        if req.theory == "omega" and (req.init or {}).get("omega_seed", True):
+            seed_omega(f, req.p_i, req.p_f)
+        return f
 
     def _switch_tol(self, req: Request) -> float:
         if self.switch_tol is not None:

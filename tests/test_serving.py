@@ -224,3 +224,33 @@ def test_autotune_picks_a_measured_chunk(tmp_path):
     assert res["xc"] in [int(k) for k in res["timings"]]
     assert res["ms_per_step"] == min(res["timings"].values())
     assert autotune.tune("omega", p_i, p_f, "fp32c", cache=cache) == res      # cached
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["nuclear", "omega"])
+def test_request_built_on_the_device(name):
+    """A request that carries an initial configuration instead of a field is built on the
+    device at admission (omega seeded there too) and relaxes to the same solution as the
+    same configuration built on the host (the two fields differ in the last bits only)."""
+    import torch
+    from skyrmion_solver_b200.engine import Engine
+    from skyrmion_solver_b200.theories._init_common import build_host_field, seed_omega
+    from tests.test_march import params_for
+    th, p_i, p_f = params_for(name, (24, 22, 26))
+    cfg = {"mode": "hedgehog", "scale": 1.0, "center": (0.1, -0.1, 0.05), "vacuum_shell": 2}
+    host = build_host_field(name, p_i, p_f, cfg)
+    if name == "omega":
+        t = torch.from_numpy(host.ravel().copy()).cuda()
+        seed_omega(t, p_i, p_f)
+        host = t.cpu().numpy().reshape(host.shape)
+    out = {}
+    for key, req in (("host", Request(0, name, p_i, p_f, host, 0.0, 2e-4, 6000)),
+                     ("device", Request(0, name, p_i, p_f, None, 0.0, 2e-4, 6000, init=cfg))):
+        with Engine(0) as eng:
+            srv = Server(eng, chunk=32, plateau_chunks=4)
+            srv.submit(req)
+            out[key] = srv.run()[0]
+    a, b = out["host"], out["device"]
+    assert a.status == b.status == "converged"
+    assert abs(a.energy - b.energy) <= 1e-8 * abs(a.energy)
+    assert np.max(np.abs(a.field - b.field)) <= 1e-6
