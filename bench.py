@@ -668,7 +668,8 @@ def run_serve(args):
         t_all += dt
         serial[r.rid] = dict(status=status, steps=n, energy=e, seconds=dt)
         del sim
-    rel = [abs(served[k].energy - serial[k]["energy"]) / abs(serial[k]["energy"]) for k in served
+    # relative to max(|E|, 1): a configuration that unwinds to the vacuum (E -> 0) compares absolutely
+    rel = [abs(served[k].energy - serial[k]["energy"]) / max(abs(serial[k]["energy"]), 1.0) for k in served
            if served[k].status == "converged" and serial[k]["status"] == "converged"]
     n_serial = sum(v["status"] == "converged" for v in serial.values())
     serial_sps = n_serial / t_all if t_all > 0 else None
@@ -686,6 +687,8 @@ def run_serve(args):
             else None,
             "max_rel_energy_diff_vs_plain_fp64": max(rel) if rel else None,
             "per_request": [dict(rid=k, theory=reqs[k][0].theory, sites=int(reqs[k][0].p_i[6]),
+                                 energy=served[k].energy, baryon=served[k].baryon,
+                                 serial_energy=serial[k]["energy"],
                                  served_steps=served[k].steps, fp32_steps=served[k].fp32_steps,
                                  latency_s=served[k].latency, status=served[k].status,
                                  serial_steps=serial[k]["steps"], serial_s=serial[k]["seconds"])
