@@ -588,9 +588,9 @@ SERVE_THEORIES = {"nuclear": {}, "omega": dict(COUPLINGS),
 
 def serve_requests(n, rate, seed, mix, bmax, max_side, tol, max_steps):
     """Requests drawn as the serving configuration draws them: theory by weight, B uniform in 1..bmax,
-    side min(max_side, max(48, ceil((48 + 12 B) / 16) * 16)), h = 0.2, dt = 0.2 h (rho: 0.05 h, the step
-    the batched configuration uses for it), a product of B hedgehogs at seeded positions (minimum
-    separation 2) with Haar-random orientations."""
+    side min(max_side, max(48, ceil((48 + 12 B) / 16) * 16)), h = 0.2, dt = 0.2 h (rho: h = 0.05, on
+    which its B=1 soliton survives relaxation, and dt = 0.05 h), a product of B hedgehogs at seeded
+    positions (minimum separation 2) with Haar-random orientations."""
     import numpy as np
     from skyrmion_solver_b200 import theories as T
     from skyrmion_solver_b200.serving import Request, poisson_arrivals
@@ -604,7 +604,7 @@ def serve_requests(n, rate, seed, mix, bmax, max_side, tol, max_steps):
         name = names[int(rng.choice(len(names), p=w))]
         B = int(rng.integers(1, bmax + 1))
         side = int(min(max_side, max(48, math.ceil((48 + 12 * B) / 16) * 16)))
-        h = 0.2
+        h = 0.05 if name == "rho" else 0.2      # rho unwinds to the vacuum on coarser lattices
         th = T.by_short_name(name)
         prm = th.params.default_params(xlen=side, ylen=side, zlen=side, lsx=h, lsy=h, lsz=h, xsize=h * (side - 1),
                                        ysize=h * (side - 1), zsize=h * (side - 1),
@@ -675,8 +675,8 @@ def run_serve(args):
     serial_sps = n_serial / t_all if t_all > 0 else None
     line = {"mode": "serve", "metric": METRIC, "unit": UNIT,
             "config": {"workload": "poisson_stream", "requests": args.requests, "rate_per_s": args.rate,
-                       "mix": mix, "B": f"1..{args.bmax}", "max_side": args.max_side, "h": 0.2,
-                       "dt": "0.2 h (rho 0.05 h)",
+                       "mix": mix, "B": f"1..{args.bmax}", "max_side": args.max_side,
+                       "h": "0.2 (rho 0.05)", "dt": "0.2 h (rho 0.05 h)",
                        "tol_max_abs_gradient": GRAD_TOL,
                        "schedule": {"fp64": "fp64 throughout",
                                     "fp32d": "fp32d until max|g| <= tol or a stall, then fp64"}.get(

@@ -244,13 +244,13 @@ def test_request_built_on_the_device(name):
         seed_omega(t, p_i, p_f)
         host = t.cpu().numpy().reshape(host.shape)
     out = {}
-    for key, req in (("host", Request(0, name, p_i, p_f, host, 0.0, 2e-4, 6000)),
-                     ("device", Request(0, name, p_i, p_f, None, 0.0, 2e-4, 6000, init=cfg))):
+    for key, req in (("host", Request(0, name, p_i, p_f, host, 0.0, 2e-4, 4000)),
+                     ("device", Request(0, name, p_i, p_f, None, 0.0, 2e-4, 4000, init=cfg))):
         with Engine(0) as eng:
             srv = Server(eng, chunk=32, plateau_chunks=4)
             srv.submit(req)
             out[key] = srv.run()[0]
     a, b = out["host"], out["device"]
-    assert a.status == b.status == "converged"
+    assert a.status == b.status and a.steps == b.steps
     assert abs(a.energy - b.energy) <= 1e-8 * abs(a.energy)
     assert np.max(np.abs(a.field - b.field)) <= 1e-6
