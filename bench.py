@@ -107,6 +107,18 @@ def load_calibration():
         return json.load(fh)
 
 
+def load_issue_active(stage):
+    """smsp__issue_active (fraction of cycles a scheduler issued) of one stage kernel from the
+    committed ncu summary, or None: the compute-side roofline of an issue-bound kernel."""
+    import re
+    for path in TRAFFIC:
+        if os.path.exists(path):
+            m = re.search(r"issue_active\[%s\]:\s*([0-9.eE+]+)" % stage, open(path).read())
+            if m:
+                return float(m.group(1))
+    return None
+
+
 def load_traffic(stage):
     """Per-launch DRAM bytes (read + write) of one stage kernel from the committed ncu summary, or None."""
     import re
@@ -450,6 +462,9 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": f"k_march_stage<Omega,float,{dom[-1]}>" + (" + k_march_defect" if dom == "stage1" and FAST == "fp32d" else ""), "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                     "issue_active": load_issue_active(dom),
+                     "note": "the stencil stages are issue-bound, not HBM-bound: issue_active is the ncu "
+                             "fraction of scheduler cycles that issued (profiles/ncu_stage1_fp32d_omega128.md)",
                      "launch_ms": stages[dom], "stage_ms": stages},
         "plain_fp64": {"ms_per_step": plain_ms, "solves_per_s": plain_value, "steps_to_converge": s64,
                        "engine_fp64_ms_per_step": eng64_ms, "engine_fp64_solves_per_s": eng64_value,
