@@ -205,12 +205,11 @@ int sky_engine_remove(void* engine, int id);
  * pending arrest decision carry over. */
 int sky_engine_set_precision(void* engine, int id, int precision);
 
-/* Re-tile an instance that runs the marching kernels (every theory in FP32,
- * C <= 5 in FP64): x-chunk `xc` planes per block (0 = automatic choice from the
- * grid and the SM count).  The state and the pending arrest decision carry
- * over. */
+/* Re-tile an instance: x-chunk `xc` planes per block of the marching kernels
+ * (0 = automatic choice from the grid and the SM count).  The state and the
+ * pending arrest decision carry over. */
 int sky_engine_retile(void* engine, int id, int xc);
-/* Current x-chunk of an instance (0 for the 3-D tile kernels, -1 if unknown). */
+/* Current x-chunk of an instance (-1 if unknown). */
 int sky_engine_get_xc(void* engine, int id);
 
 /* Energy audit of the RK4 dynamics (killkinen = 0) of an instance's current

@@ -101,12 +101,9 @@ def tune(theory, p_i, p_f, precision: str = "fp32c", field=None, device: int = 0
     with Engine(device) as eng:
         iid = eng.add(theory, (np.asarray(p_i, np.int32), np.asarray(p_f, np.float64)), field, None,
                       precision=precision)
-        if eng.xc(iid) == 0:          # tile-kernel theory: nothing to tune
-            res = {"xc": 0, "ms_per_step": None, "timings": {}}
-        else:
-            t = time_chunks(eng, iid, candidate_chunks(X), steps=steps)
-            best = min(t, key=t.get)
-            res = {"xc": int(best), "ms_per_step": float(t[best]), "timings": {str(k): v for k, v in t.items()}}
+        t = time_chunks(eng, iid, candidate_chunks(X), steps=steps)
+        best = min(t, key=t.get)
+        res = {"xc": int(best), "ms_per_step": float(t[best]), "timings": {str(k): v for k, v in t.items()}}
     cache.put(key, res)
     return res
 

@@ -71,17 +71,10 @@ struct Engine {
 // ---------------------------------------------------------------------------
 // shapes and launches per (theory, precision)
 // ---------------------------------------------------------------------------
-template <template <typename> class Th, typename T>
-using EShape = typename GradTile<Th<T>::C, T>::type;
-
 // Every theory runs the marching kernels (sky_march.cuh) in both precisions.
 // Tiles are 8 rows x 32 columns, except for FP64 rho (13 components): its
 // 4-row tiles keep the five-plane ring at 150 KB, narrow rows only, with two
 // of stage 3/4's three sources staged (one block per SM).
-template <template <typename> class Th, typename T = float>
-constexpr bool uses_march() {
-    return true;
-}
 constexpr int kMarchBY = 8;
 template <template <typename> class Th, typename T>
 constexpr int march_by() {
@@ -119,25 +112,14 @@ static int stage_setup_w(int* per_sm_out) {
     static int per_sm = 0;
     if (per_sm == 0) {
         int rc, n = 0;
-        if constexpr (uses_march<Th, T>()) {
-            using M = MShape<Th, T, WIDE>;
-            auto kern = k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO>;
-            const size_t smem = M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
-            rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                            "cudaFuncSetAttribute(march stage)", __LINE__);
-            if (rc) return rc;
-            rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem),
-                            "occupancy query", __LINE__);
-        } else {
-            using Shape = EShape<Th, T>;
-            auto kern = k_engine_stage<Th, Shape, T, T, STAGE>;
-            const size_t smem = Shape::template smem_bytes<T>();
-            rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                            "cudaFuncSetAttribute(engine stage)", __LINE__);
-            if (rc) return rc;
-            rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, Shape::NTHREADS, smem),
-                            "occupancy query", __LINE__);
-        }
+        using M = MShape<Th, T, WIDE>;
+        auto kern = k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO>;
+        const size_t smem = M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
+        rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                        "cudaFuncSetAttribute(march stage)", __LINE__);
+        if (rc) return rc;
+        rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem),
+                        "occupancy query", __LINE__);
         if (rc) return rc;
         per_sm = n < 1 ? 1 : n;
     }
@@ -159,43 +141,32 @@ static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t s
     if (n <= 0) return SKY_OK;
     const int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
     InstDesc<T>* d = reinterpret_cast<InstDesc<T>*>(g.d_desc);
-    if constexpr (uses_march<Th, T>()) {
-        using M = MShape<Th, T, WIDE>;
-        const size_t smem = M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
-        k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(
-            d, g.d_tile_inst, t_begin, t_end);
-    } else {
-        using Shape = EShape<Th, T>;
-        const size_t smem = Shape::template smem_bytes<T>();
-        k_engine_stage<Th, Shape, T, T, STAGE><<<blocks, dim3(Shape::BZ, Shape::BY), smem, st>>>(d, g.d_tile_inst,
-                                                                                                t_begin, t_end);
-    }
+    using M = MShape<Th, T, WIDE>;
+    const size_t smem = M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
+    k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(
+        d, g.d_tile_inst, t_begin, t_end);
     return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
 }
 
 template <template <typename> class Th, typename T, int STAGE>
 static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
-    if constexpr (uses_march<Th, T>()) {
-        // stage 1 of a group with compensated-field instances stages the low parts too,
-        // in wide rows when two blocks per SM still fit (the two six-slot rings take
-        // 112.5 KB per block for C = 5), else in narrow rows; rho's 13 components leave
-        // no room for the second ring at all: its FP64 densities use the high parts
-        if constexpr (STAGE == 1 && sizeof(T) == 4 && Th<float>::C <= 5) {
-            if (g.any_comp) {
-                if (g.all_wide) {
-                    int n = 0;
-                    const int rc = stage_setup_w<Th, T, 1, true, true>(&n);
-                    if (rc) return rc;
-                    if (n >= 2) return launch_stage_w<Th, T, 1, true, true>(g, t_begin, t_end, st);
-                }
-                return launch_stage_w<Th, T, 1, false, true>(g, t_begin, t_end, st);
+    // stage 1 of a group with compensated-field instances stages the low parts too,
+    // in wide rows when two blocks per SM still fit (the two six-slot rings take
+    // 112.5 KB per block for C = 5), else in narrow rows; rho's 13 components leave
+    // no room for the second ring at all: its FP64 densities use the high parts
+    if constexpr (STAGE == 1 && sizeof(T) == 4 && Th<float>::C <= 5) {
+        if (g.any_comp) {
+            if (g.all_wide) {
+                int n = 0;
+                const int rc = stage_setup_w<Th, T, 1, true, true>(&n);
+                if (rc) return rc;
+                if (n >= 2) return launch_stage_w<Th, T, 1, true, true>(g, t_begin, t_end, st);
             }
+            return launch_stage_w<Th, T, 1, false, true>(g, t_begin, t_end, st);
         }
-        if (g.all_wide) return launch_stage_w<Th, T, STAGE, true>(g, t_begin, t_end, st);
-        return launch_stage_w<Th, T, STAGE, false>(g, t_begin, t_end, st);
-    } else {
-        return launch_stage_w<Th, T, STAGE, false>(g, t_begin, t_end, st);
     }
+    if (g.all_wide) return launch_stage_w<Th, T, STAGE, true>(g, t_begin, t_end, st);
+    return launch_stage_w<Th, T, STAGE, false>(g, t_begin, t_end, st);
 }
 
 template <template <typename> class Th, typename T>
@@ -255,23 +226,17 @@ static int launch_stage_group(int stage, const Group& g, int tb, int te, cudaStr
     return invalid("unknown theory id");
 }
 
-// Tile geometry of a (theory, precision): (bz, by, tx) of the tile kernels, or
-// (32, BY, 0) for the marching kernels, whose x-chunk is chosen per instance;
-// per_sm = resident stage-4 blocks per SM.
+// Tile geometry of a (theory, precision): (bz, by, tx) = (32, BY, 0) for the
+// marching kernels, whose x-chunk is chosen per instance; per_sm = resident
+// stage-4 blocks per SM.
 template <template <typename> class Th>
 static int shape_of(int prec, int& bz, int& by, int& tx, int& per_sm) {
     per_sm = 1;
     if (prec) {
-        if constexpr (uses_march<Th, double>()) {
-            bz = 32, by = march_by<Th, double>(), tx = 0;
-            return stage_setup<Th, double, 4>(&per_sm);
-        } else {
-            using S = EShape<Th, double>;
-            bz = S::BZ, by = S::BY, tx = S::TX;
-            return SKY_OK;
-        }
+        bz = 32, by = march_by<Th, double>(), tx = 0;
+        return stage_setup<Th, double, 4>(&per_sm);
     }
-    bz = 32, by = kMarchBY, tx = 0;   // every theory marches in FP32
+    bz = 32, by = march_by<Th, float>(), tx = 0;
     return stage_setup<Th, float, 4>(&per_sm);
 }
 
@@ -310,32 +275,26 @@ static int launch_advance(const Group& g, cudaStream_t st) {
 // refresh flag the advance kernel just set; the others' tiles are skipped).
 template <template <typename> class Th, bool WIDE>
 static int launch_defect_t(const Group& g, cudaStream_t st) {
-    if constexpr (uses_march<Th, double>()) {
-        using M = MarchShape<Th<double>::C, kMarchBY, WIDE>;
-        auto kern = k_march_defect<Th, M>;
-        const size_t smem = M::template smem_bytes<double, float>(2);
-        static int per_sm = 0;
-        if (per_sm == 0) {
-            int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                                "cudaFuncSetAttribute(defect)", __LINE__);
-            if (rc) return rc;
-            int n = 0;
-            rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem), "occupancy",
-                            __LINE__);
-            if (rc) return rc;
-            per_sm = n < 1 ? 1 : n;
-        }
-        const int n = g.ntiles;
-        if (n <= 0) return SKY_OK;
-        const int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
-        kern<<<blocks, dim3(M::BZ, M::BY), smem, st>>>(reinterpret_cast<InstDesc<float>*>(g.d_desc), g.d_tile_inst, 0,
-                                                       n);
-        return check_cuda(cudaGetLastError(), "launch defect refresh", __LINE__);
-    } else {
-        (void)g;
-        (void)st;
-        return SKY_OK;
+    using M = MarchShape<Th<double>::C, kMarchBY, WIDE>;
+    auto kern = k_march_defect<Th, M>;
+    const size_t smem = M::template smem_bytes<double, float>(2);
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(defect)", __LINE__);
+        if (rc) return rc;
+        int n = 0;
+        rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem), "occupancy",
+                        __LINE__);
+        if (rc) return rc;
+        per_sm = n < 1 ? 1 : n;
     }
+    const int n = g.ntiles;
+    if (n <= 0) return SKY_OK;
+    const int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
+    kern<<<blocks, dim3(M::BZ, M::BY), smem, st>>>(reinterpret_cast<InstDesc<float>*>(g.d_desc), g.d_tile_inst, 0,
+                                                   n);
+    return check_cuda(cudaGetLastError(), "launch defect refresh", __LINE__);
 }
 
 template <template <typename> class Th>
@@ -515,15 +474,11 @@ static int alloc_inst(Engine& e, HostInst& h) {
     if (rc0) return rc0;
     h.tnz = (h.p.Z + bz - 1) / bz;
     h.tny = (h.p.Y + by - 1) / by;
-    if (tx == 0) {
-        if ((int64_t)h.C * h.N >= ((int64_t)1 << 31)) return invalid("lattice too large for the marching kernels");
-        h.xc = h.xc_request > 0 ? (h.xc_request < h.p.X ? h.xc_request : h.p.X)
-                                : choose_xc(h.p.X, h.tnz * h.tny, num_sms() * per_sm);
-        tx = h.xc;
-    } else {
-        h.xc = 0;
-    }
-    h.tnx = (h.p.X + tx - 1) / tx;
+    (void)tx;
+    if ((int64_t)h.C * h.N >= ((int64_t)1 << 31)) return invalid("lattice too large for the marching kernels");
+    h.xc = h.xc_request > 0 ? (h.xc_request < h.p.X ? h.xc_request : h.p.X)
+                            : choose_xc(h.p.X, h.tnz * h.tny, num_sms() * per_sm);
+    h.tnx = (h.p.X + h.xc - 1) / h.xc;
     h.ntiles = h.tnz * h.tny * h.tnx;
     void** bufs[] = {&h.F[0], &h.F[1], &h.V[0], &h.V[1], &h.L[0], &h.L[1], &h.L[2]};
     for (void** b : bufs) {
@@ -974,7 +929,6 @@ int sky_engine_retile(void* handle, int id, int xc) {
     int bz, by, tx, per_sm;
     int rc = tile_shape(h.theory, h.prec, bz, by, tx, per_sm);
     if (rc) return rc;
-    if (tx != 0) return SKY_OK;  // tile-kernel theory: fixed geometry
     const int tny = (h.p.Y + by - 1) / by, tnz = (h.p.Z + bz - 1) / bz;
     const int nxc = xc > 0 ? (xc < h.p.X ? xc : h.p.X) : choose_xc(h.p.X, tnz * tny, num_sms() * per_sm);
     const int ntiles = tnz * tny * ((h.p.X + nxc - 1) / nxc);

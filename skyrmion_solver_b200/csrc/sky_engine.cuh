@@ -186,150 +186,6 @@ __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __r
                            Vo, v2);
 }
 
-// Tile loader for X = F + a V + b L (V and/or L optional).
-template <class Shape, typename T, typename S>
-__device__ __forceinline__ void load_stage_tile(T* __restrict__ sm, const Params& p, int64_t N, int x0, int y0, int z0,
-                                                const S* __restrict__ F, const S* __restrict__ V,
-                                                const S* __restrict__ Lp, T a, T b) {
-    const int64_t YZ = (int64_t)p.Y * p.Z;
-    const int nrows = Shape::C * Shape::HX * Shape::HY;
-    for (int row = threadIdx.y; row < nrows; row += Shape::BY) {
-        const int c = row / (Shape::HX * Shape::HY);
-        const int r = row - c * (Shape::HX * Shape::HY);
-        const int xx = r / Shape::HY;
-        const int yy = r - xx * Shape::HY;
-        const int gx = x0 - 2 + xx;
-        const int gy = y0 - 2 + yy;
-        const bool rowok = (gx >= 0) && (gx < p.X) && (gy >= 0) && (gy < p.Y);
-        const int64_t base = (int64_t)c * N + gx * YZ + (int64_t)gy * p.Z;
-        T* dst = sm + c * Shape::VOL + xx * Shape::PLANE + yy * Shape::HZ;
-        for (int zz = threadIdx.x; zz < Shape::HZ; zz += Shape::BZ) {
-            const int gz = z0 - 2 + zz;
-            T v = T(0);
-            if (rowok && gz >= 0 && gz < p.Z) {
-                const int64_t i = base + gz;
-                v = T(F[i]);
-                if (V) v += a * T(V[i]);
-                if (Lp) v += b * T(Lp[i]);
-            }
-            dst[zz] = v;
-        }
-    }
-}
-
-__device__ __forceinline__ int find_inst(const int* __restrict__ tile_inst, int t) { return __ldg(tile_inst + t); }
-
-// ---------------------------------------------------------------------------
-// Fused stage kernel.  STAGE in 1..4.  Grid-strides over the global tile list.
-// ---------------------------------------------------------------------------
-template <template <typename> class Th, class Shape, typename T, typename S, int STAGE>
-__global__ void __launch_bounds__(Shape::NTHREADS)
-    k_engine_stage(InstDesc<S>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
-    constexpr int C = Th<T>::C;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    T* sm = reinterpret_cast<T*>(smraw);
-    __shared__ KSum shk[32];
-    __shared__ double shm[32];
-    for (int t = t_begin + blockIdx.x; t < t_end; t += gridDim.x) {
-        const int ii = find_inst(tile_inst, t);
-        InstDesc<S>& in = insts[ii];
-        if (!in.active) continue;  // uniform across the block
-        const int parity = in.cur;
-        const Params& p = in.p;
-        const int64_t N = n_sites(p);
-        const int lt = t - in.tile_begin;
-        TileGrid tg{in.tiles_nz, in.tiles_ny, in.tiles_nx};
-        int x0, y0, z0;
-        tile_origin(tg, lt, Shape::BZ, Shape::BY, Shape::TX, x0, y0, z0);
-        const S* F = in.F[parity];
-        const S* V = in.arrested ? nullptr : in.V[parity];
-        const T hdt = T(0.5 * p.dt), dtt = T(p.dt);
-        __syncthreads();
-        if (STAGE == 1) load_stage_tile<Shape, T, S>(sm, p, N, x0, y0, z0, F, nullptr, nullptr, T(0), T(0));
-        if (STAGE == 2) load_stage_tile<Shape, T, S>(sm, p, N, x0, y0, z0, F, V, nullptr, hdt, T(0));
-        if (STAGE == 3) load_stage_tile<Shape, T, S>(sm, p, N, x0, y0, z0, F, V, in.L[0], hdt, T(0.25) * dtt);
-        if (STAGE == 4) load_stage_tile<Shape, T, S>(sm, p, N, x0, y0, z0, F, V, in.L[1], dtt, T(0.5) * dtt);
-        __syncthreads();
-        StencilCoef<T> k;
-        k.init(p);
-        KSum esum{0.0, 0.0}, bsum{0.0, 0.0}, ksum{0.0, 0.0};
-        double gmx = -1.0e300, gab = 0.0;
-        const int z = z0 + threadIdx.x, y = y0 + threadIdx.y;
-        if (z < p.Z && y < p.Y) {
-#pragma unroll 1
-            for (int i = 0; i < Shape::TX; ++i) {
-                const int x = x0 + i;
-                if (x >= p.X) break;
-                const Mask m = site_mask(p, x, y, z);
-                T phi[C], D[3][C], Sd[6][C], g[C];
-#pragma unroll
-                for (int c = 0; c < C; ++c)
-                    site_derivs<Shape, T, C>(sm, c, i + 2, threadIdx.y + 2, threadIdx.x + 2, k, m, D, Sd, phi[c]);
-                const int64_t s = ((int64_t)x * p.Y + y) * p.Z + z;
-                if (STAGE == 1) {
-                    // FP64 energy and baryon density of F (the tile holds F exactly)
-                    StencilCoef<double> kd;
-                    kd.init(p);
-                    double phd[C], Dd[3][C];
-#pragma unroll
-                    for (int c = 0; c < C; ++c) {
-                        const T* f = sm + c * Shape::VOL + (i + 2) * Shape::PLANE + (threadIdx.y + 2) * Shape::HZ +
-                                     threadIdx.x + 2;
-                        const int st[3] = {Shape::PLANE, Shape::HZ, 1};
-                        const bool pm[3] = {m.px, m.py, m.pz};
-                        phd[c] = double(f[0]);
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            const double v = kd.d1a[d] * (double(f[st[d]]) - double(f[-st[d]])) -
-                                             kd.d1b[d] * (double(f[2 * st[d]]) - double(f[-2 * st[d]]));
-                            Dd[d][c] = pm[d] ? v : 0.0;
-                        }
-                    }
-                    ksum_add(esum, Th<double>::energy(phd, Dd, p));
-                    ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
-                }
-                Th<T>::gradient(phi, D, Sd, p, g);
-                if (STAGE < 4) {
-                    S* lout = in.L[STAGE - 1];
-#pragma unroll
-                    for (int c = 0; c < C; ++c) lout[c * N + s] = S(-dtt * g[c]);
-                } else {
-                    // stage-4 gradient statistics (reference `err`: signed max of EG)
-#pragma unroll
-                    for (int c = 0; c < C; ++c) {
-                        const double gd = double(g[c]);
-                        gmx = fmax(gmx, gd);
-                        gab = fmax(gab, fabs(gd));
-                    }
-                    double v2;
-                    finalize_site<T, S, C>(s, N, F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2], g, dtt, p.nsky,
-                                           p.unit_length, in.F[parity ^ 1], in.Flo[parity ^ 1], in.V[parity ^ 1], v2);
-                    ksum_add(ksum, 0.5 * p.vol * v2);
-                }
-            }
-        }
-        if (STAGE == 1) {
-            KSum be = block_ksum(esum, shk);
-            KSum bb = block_ksum(bsum, shk);
-            if (threadIdx.x == 0 && threadIdx.y == 0) {
-                in.epart[lt] = be;
-                in.bpart[lt] = bb;
-            }
-        }
-        if (STAGE == 4) {
-            const double a = block_max(gmx, shm);
-            const double b = block_max(gab, shm);
-            const KSum kk = block_ksum(ksum, shk);
-            if (threadIdx.x == 0 && threadIdx.y == 0) {
-                in.gpart[4 * lt] = a;
-                in.gpart[4 * lt + 1] = b;
-                in.gpart[4 * lt + 2] = kk.s;
-                in.gpart[4 * lt + 3] = kk.c;
-            }
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Control: one block per instance.  Reduces the stage-1 partials (energy and
 // baryon number of the field entering this step) and the previous step's
