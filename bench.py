@@ -648,7 +648,7 @@ def run_serve(args):
                           args.max_steps)
     # 1. continuous batching on the resident engine
     with Engine(0) as eng:
-        srv = Server(eng, chunk=64, fp32_mode=args.schedule)
+        srv = Server(eng, chunk=64, fp32_mode=args.schedule, defect_period=args.defect_period)
         for r, _, _ in reqs:
             srv.submit(r)
         torch.cuda.synchronize()
@@ -692,7 +692,7 @@ def run_serve(args):
             "config": {"workload": "poisson_stream", "requests": args.requests, "rate_per_s": args.rate,
                        "mix": mix, "B": f"1..{args.bmax}", "max_side": args.max_side,
                        "h": "0.2 (rho 0.05)", "dt": "0.2 h (rho 0.05 h)",
-                       "tol_max_abs_gradient": GRAD_TOL,
+                       "tol_max_abs_gradient": GRAD_TOL, "defect_period": args.defect_period or 16,
                        "schedule": {"fp64": "fp64 throughout",
                                     "fp32d": "fp32d until max|g| <= tol or a stall, then fp64"}.get(
                            args.schedule, f"{args.schedule} until twice the FP32 gradient floor, then fp64")},
@@ -871,6 +871,8 @@ def main():
     ap.add_argument("--schedule", choices=("fp32d", "fp32c", "fp32", "fp64"), default="fp64",
                     help="serving precision schedule: FP32 phase then FP64, or FP64 throughout")
     ap.add_argument("--max-side", type=int, default=64)
+    ap.add_argument("--defect-period", type=int, default=None,
+                    help="serving: steps between refreshes of the fp32d correction (default 16)")
     ap.add_argument("--batch", action="store_true", help="48 mixed pion / rho instances in one engine")
     ap.add_argument("--instances", type=int, default=48)
     ap.add_argument("--dynamics", action="store_true", help="RK4 dynamics of two boosted tori with energy audit")

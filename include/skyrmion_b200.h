@@ -209,6 +209,10 @@ int sky_engine_set_precision(void* engine, int id, int precision);
  * (0 = automatic choice from the grid and the SM count).  The state and the
  * pending arrest decision carry over. */
 int sky_engine_retile(void* engine, int id, int xc);
+/* Steps between refreshes of a defect-corrected instance's FP64 correction
+ * (precision 3; default 16, period >= 1).  A shorter period follows a field
+ * that moves (a drifting soliton) at the cost of more FP64 gradient passes. */
+int sky_engine_set_defect_period(void* engine, int id, int period);
 /* Current x-chunk of an instance (-1 if unknown). */
 int sky_engine_get_xc(void* engine, int id);
 

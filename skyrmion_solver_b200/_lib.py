@@ -81,6 +81,7 @@ SIGNATURES = {
     "sky_engine_set_active": ([_P, _I, _I], _I),
     "sky_engine_retile": ([_P, _I, _I], _I),
     "sky_engine_get_xc": ([_P, _I], _I),
+    "sky_engine_set_defect_period": ([_P, _I, _I], _I),
     "sky_engine_audit": ([_P, _I, _F64P], _I),
     "sky_engine_step": ([_P, _I], _I),
     "sky_engine_synchronize": ([_P], _I),

@@ -23,6 +23,7 @@ struct HostInst {
     int prec = 0;  // storage: 0 = FP32 storage/arithmetic, 1 = FP64
     int comp = 0;    // FP32 storage with a compensated (hi + lo) field
     int defect = 0;  // ... and a defect-corrected gradient (precision 3; marching theories only)
+    int defect_period = kDefectRefresh;  // steps between refreshes of the correction
     Params p{};
     int64_t N = 0;
     int C = 0;
@@ -378,6 +379,7 @@ static InstDesc<S> make_desc(const HostInst& h, int tile_begin) {
     d.tiles_nx = h.tnx;
     d.xc = h.xc;
     d.active = h.active ? 1 : 0;
+    d.refresh_period = h.defect_period;
     return d;
 }
 
@@ -980,6 +982,25 @@ int sky_engine_audit(void* handle, int id, double* out2) {
         case SKY_THEORY_LIGHTLY_BOUND: return audit_prec<LightlyBound>(*e, *hp, out2);
     }
     return invalid("unknown theory id");
+}
+
+int sky_engine_set_defect_period(void* handle, int id, int period) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return invalid("null engine");
+    HostInst* hp = find(e, id);
+    if (!hp) return invalid("unknown instance id");
+    if (period < 1) return invalid("defect refresh period must be >= 1");
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    hp->defect_period = period;
+    Group& g = e->groups[hp->theory][hp->prec];
+    const size_t sz = hp->prec ? sizeof(InstDesc<double>) : sizeof(InstDesc<float>);
+    const size_t off = hp->prec ? offsetof(InstDesc<double>, refresh_period) : offsetof(InstDesc<float>, refresh_period);
+    char* base = reinterpret_cast<char*>(g.d_desc) + sz * hp->group_slot;
+    int rc = check_cuda(cudaMemcpyAsync(base + off, &period, sizeof(int), cudaMemcpyHostToDevice, e->stream),
+                        "write refresh period", __LINE__);
+    if (rc) return rc;
+    return check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__);
 }
 
 int sky_engine_get_xc(void* handle, int id) {

@@ -63,6 +63,7 @@ struct InstDesc {
     int active;        // 0 = skip (retired / paused)
     int cur;           // which half of the F / V ping-pong pairs is current
     int refresh;       // this step's stage 1 refreshes the defect correction
+    int refresh_period;  // steps between refreshes of the defect correction
 };
 
 // RK4 update of one site (core/integrator.py:163-175): V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,
@@ -240,7 +241,8 @@ __global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict_
     }
 }
 
-// Steps between refreshes of the defect correction of an FP32 instance.
+// Default number of steps between refreshes of the defect correction of an FP32
+// instance (sky_engine_set_defect_period changes it per instance).
 constexpr int kDefectRefresh = 16;
 
 // Flip the ping-pong halves and advance the step counter (after stage 4); flag the
@@ -251,7 +253,8 @@ __global__ void k_engine_advance(InstDesc<S>* __restrict__ insts, int ninst) {
     if (i < ninst && insts[i].active) {
         insts[i].step += 1;
         insts[i].cur ^= 1;
-        insts[i].refresh = (insts[i].Dlt != nullptr && insts[i].step % kDefectRefresh == 0) ? 1 : 0;
+        const int period = insts[i].refresh_period > 0 ? insts[i].refresh_period : kDefectRefresh;
+        insts[i].refresh = (insts[i].Dlt != nullptr && insts[i].step % period == 0) ? 1 : 0;
     }
 }
 

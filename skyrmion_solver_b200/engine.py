@@ -149,6 +149,10 @@ class Engine:
         """x-chunk of the marching kernels for this instance (0 = automatic)."""
         self._call("sky_engine_retile", int(iid), int(xc))
 
+    def set_defect_period(self, iid: int, period: int):
+        """Steps between refreshes of an fp32d instance's FP64 correction (default 16)."""
+        self._call("sky_engine_set_defect_period", int(iid), int(period))
+
     def xc(self, iid: int) -> int:
         return int(self._lib.sky_engine_get_xc(self._h, int(iid)))
 

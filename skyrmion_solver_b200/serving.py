@@ -123,7 +123,7 @@ class Server:
                  switch_tol: float | None = None, plateau_chunks: int = 256, plateau_gain: float = 0.99,
                  polish: bool = True,
                  keep_fields: bool = True, free_bytes=None, clock=time.perf_counter, sleep=time.sleep,
-                 fp32_mode: str = "fp32d", tune_cache=None):
+                 fp32_mode: str = "fp32d", tune_cache=None, defect_period: int | None = None):
         self.engine = engine
         self.mem_cap = float(mem_cap_bytes)
         self.reserve = float(reserve_bytes)
@@ -136,6 +136,7 @@ class Server:
         self.fp32_mode = fp32_mode
         self.tune_cache = tune_cache  # autotune.TuneCache: re-tile admitted instances with cached choices
         self.keep_fields = keep_fields
+        self.defect_period = defect_period  # refresh period of fp32d corrections (None: the engine's 16)
         self.clock = clock
         self.sleep = sleep
         if free_bytes is None:
@@ -173,6 +174,8 @@ class Server:
                 self.results.append(Result(req.rid, "failed", math.nan, math.nan, math.nan, 0, 0, req.arrival, t,
                                            t))
                 continue
+            if self.defect_period is not None and self.fp32_mode == "fp32d":
+                self.engine.set_defect_period(iid, self.defect_period)
             if self.tune_cache is not None:
                 from .autotune import apply
                 apply(self.engine, iid, req.theory, self.fp32_mode, req.p_i, self.tune_cache, self.engine.device)

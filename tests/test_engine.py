@@ -382,3 +382,23 @@ def test_renderer_view_of_a_compensated_instance(density):
     fn = O.baryon_density if density == "baryon" else O.energy_density
     ref = fn(O.THEORIES["omega"], f, p_i, p_f)
     assert G.rel_err(en.cpu().numpy().reshape(ref.shape), ref) <= 1e-12
+
+
+def test_defect_refresh_period():
+    """A shorter refresh period keeps an fp32d trajectory closer to the FP64 one; the period
+    must be at least one step."""
+    from skyrmion_solver_b200._lib import SkyInvalidArgument
+    from skyrmion_solver_b200.engine import Engine
+    d, F, V, p_i, p_f = _inputs("omega")
+    with Engine(0) as eng:
+        a = eng.add("omega", (p_i, p_f), F, V, precision="fp64")
+        b = eng.add("omega", (p_i, p_f), F, V, precision="fp32d")
+        c = eng.add("omega", (p_i, p_f), F, V, precision="fp32d")
+        eng.set_defect_period(c, 1)
+        with pytest.raises(SkyInvalidArgument):
+            eng.set_defect_period(c, 0)
+        eng.step(24)
+        fa, _ = eng.read(a)
+        fb, _ = eng.read(b)
+        fc, _ = eng.read(c)
+    assert G.rel_err(fc, fa) < G.rel_err(fb, fa)
