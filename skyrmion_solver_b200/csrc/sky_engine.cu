@@ -37,7 +37,7 @@ struct HostInst {
     double* gpart = nullptr;
     StepStats* stats = nullptr;
     int ntiles = 0, tnz = 0, tny = 0, tnx = 0;
-    int xc = 0;          // x-chunk of the marching kernels (0: tile kernels)
+    int xc = 0;          // x-chunk of the marching kernels
     int xc_request = 0;  // x-chunk asked for by the caller (0: automatic)
     int group_slot = -1;
     int64_t steps = 0;  // host mirror of the device step counter

@@ -55,7 +55,7 @@ struct InstDesc {
     int tile_begin;    // first global tile index of this instance
     int ntiles;
     int tiles_nz, tiles_ny, tiles_nx;
-    int xc;            // x-chunk of the marching kernels (0: tile kernels)
+    int xc;            // x-chunk of the marching kernels
     // control state (device-updated)
     double e_prev;     // energy entering the previous step
     int step;          // steps taken
@@ -164,7 +164,7 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
     }
 }
 
-// finalize_vals with the inputs read from global memory (3-D tile kernels).
+// finalize_vals with the inputs read from global memory (the stage-4 epilogue).
 template <typename T, typename S, int C>
 __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __restrict__ F,
                                               const S* __restrict__ Flo_in, const S* __restrict__ V,
