@@ -15,27 +15,27 @@ namespace sky {
 
 __host__ __device__ constexpr int sidx(int i, int j) { return i == j ? i : 2 + i + j; }
 
+// c_mu = det[e_mu, a, u, v] for mu = 0..3: the 4-D cross product of a, u, v,
+// from the six 2x2 minors of (u, v) (24 multiply-adds instead of four 3x3
+// cofactor expansions).
 template <typename T>
-__device__ __forceinline__ T det3(T a00, T a01, T a02, T a10, T a11, T a12, T a20, T a21, T a22) {
-    return a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20) +
-           a02 * (a10 * a21 - a11 * a20);
+__device__ __forceinline__ void cross4(const T* a, const T* u, const T* v, T (&c)[4]) {
+    const T p01 = u[0] * v[1] - u[1] * v[0], p02 = u[0] * v[2] - u[2] * v[0], p03 = u[0] * v[3] - u[3] * v[0];
+    const T p12 = u[1] * v[2] - u[2] * v[1], p13 = u[1] * v[3] - u[3] * v[1], p23 = u[2] * v[3] - u[3] * v[2];
+    c[0] = a[1] * p23 - a[2] * p13 + a[3] * p12;
+    c[1] = -(a[0] * p23 - a[2] * p03 + a[3] * p02);
+    c[2] = a[0] * p13 - a[1] * p03 + a[3] * p01;
+    c[3] = -(a[0] * p12 - a[1] * p02 + a[2] * p01);
 }
 
-// Determinant of the 4x4 matrix with columns c0..c3, expanded along row 0
-// (th/nuclear_skyrme/kernels.py:155-194).
-template <typename T>
-__device__ __forceinline__ T det4_cols(const T* c0, const T* c1, const T* c2, const T* c3) {
-    T d0 = det3(c1[1], c2[1], c3[1], c1[2], c2[2], c3[2], c1[3], c2[3], c3[3]);
-    T d1 = det3(c0[1], c2[1], c3[1], c0[2], c2[2], c3[2], c0[3], c2[3], c3[3]);
-    T d2 = det3(c0[1], c1[1], c3[1], c0[2], c1[2], c3[2], c0[3], c1[3], c3[3]);
-    T d3 = det3(c0[1], c1[1], c2[1], c0[2], c1[2], c2[2], c0[3], c1[3], c2[3]);
-    return c0[0] * d0 - c1[0] * d1 + c2[0] * d2 - c3[0] * d3;
-}
-
-// -det[phi, d_x phi, d_y phi, d_z phi]; baryon density = this * h^3 / (2 pi^2).
+// -det[phi, d_x phi, d_y phi, d_z phi] = sum_mu det[e_mu, phi, d_y phi, d_z phi] d_x phi_mu
+// (expansion along the d_x phi column, th/nuclear_skyrme/kernels.py:155-194);
+// baryon density = this * h^3 / (2 pi^2).
 template <typename T, int C>
 __device__ __forceinline__ T neg_det_b(const T* phi, const T (&D)[3][C]) {
-    return -det4_cols<T>(phi, D[0], D[1], D[2]);
+    T c[4];
+    cross4<T>(phi, D[1], D[2], c);
+    return c[0] * D[0][0] + c[1] * D[0][1] + c[2] * D[0][2] + c[3] * D[0][3];
 }
 
 // Projection of the first nsky components of g orthogonal to phi
@@ -89,13 +89,12 @@ __device__ __forceinline__ void skyrme_quartic(T* g, const T (&D)[3][C], const T
     for (int a = 0; a < 4; ++a) g[a] -= coef * acc[a];
 }
 
-// sum_{ijk} eps_ijk d_i(aux) det[e_mu, phi, d_j phi, d_k phi] for mu = 0..3.
-// det[e_mu, phi, u, v] = (-1)^mu * minor of row mu; computed once per (j,k)
-// pair as the 4 cofactors of the 3-vector cross structure.  Used by the omega
-// (th/omega_skyrme/kernels.py:633-690) and Coulomb
-// (th/coulomb_skyrme/kernels.py:697-749) couplings.
+// sum_{ijk} eps_ijk d_i(aux) det[e_mu, phi, d_j phi, d_k phi] for mu = 0..3, and
+// (into *negdet) -det[phi, d_x phi, d_y phi, d_z phi], which shares the (y, z)
+// cross product.  Used by the omega (th/omega_skyrme/kernels.py:633-690) and
+// Coulomb (th/coulomb_skyrme/kernels.py:697-749) couplings.
 template <typename T, int C>
-__device__ __forceinline__ void cs_coupling(T* out, const T* phi, const T (&D)[3][C], const T* daux) {
+__device__ __forceinline__ void cs_coupling(T* out, const T* phi, const T (&D)[3][C], const T* daux, T* negdet) {
 #pragma unroll
     for (int mu = 0; mu < 4; ++mu) out[mu] = T(0);
     // ordered triples (i,j,k) with sign; det[e_mu,phi,Dj,Dk] is antisymmetric in (j,k),
@@ -104,18 +103,12 @@ __device__ __forceinline__ void cs_coupling(T* out, const T* phi, const T (&D)[3
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
         const int i = tri[t][0], j = tri[t][1], k = tri[t][2];
-        const T* u = D[j];
-        const T* v = D[k];
-        // cofactor expansion of det[e_mu, phi, u, v] along column 0
-        T m0 = det3(phi[1], u[1], v[1], phi[2], u[2], v[2], phi[3], u[3], v[3]);
-        T m1 = det3(phi[0], u[0], v[0], phi[2], u[2], v[2], phi[3], u[3], v[3]);
-        T m2 = det3(phi[0], u[0], v[0], phi[1], u[1], v[1], phi[3], u[3], v[3]);
-        T m3 = det3(phi[0], u[0], v[0], phi[1], u[1], v[1], phi[2], u[2], v[2]);
+        T c[4];
+        cross4<T>(phi, D[j], D[k], c);
         const T w = T(2) * daux[i];
-        out[0] += w * m0;
-        out[1] -= w * m1;
-        out[2] += w * m2;
-        out[3] -= w * m3;
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) out[mu] += w * c[mu];
+        if (t == 0) *negdet = c[0] * D[0][0] + c[1] * D[0][1] + c[2] * D[0][2] + c[3] * D[0][3];
     }
 }
 
@@ -167,14 +160,14 @@ struct Omega {
         const T mass2 = T(p.c0 * p.c0);
         const T cw = T(p.c1);
         const T daux[3] = {D[0][4], D[1][4], D[2][4]};
-        T cs[4];
-        cs_coupling<T, C>(cs, phi, D, daux);
+        T cs[4], nd;
+        cs_coupling<T, C>(cs, phi, D, daux, &nd);
         const T k = cw / T(4.0 * M_PI * M_PI);
 #pragma unroll
         for (int mu = 0; mu < 4; ++mu) g[mu] = -T(0.25) * (S[0][mu] + S[1][mu] + S[2][mu]) + k * cs[mu];
         g[0] -= T(0.25) * mass2;
         project<T, C>(g, phi, p.nsky);
-        const T b0 = neg_det_b<T, C>(phi, D) / T(2.0 * M_PI * M_PI);
+        const T b0 = nd / T(2.0 * M_PI * M_PI);
         g[4] = phi[4] - (S[0][4] + S[1][4] + S[2][4]) + cw * b0;
     }
     // th/omega_skyrme/kernels.py:231-302 (no -c_omega*omega*B0 term, :301)
@@ -211,13 +204,13 @@ struct Coulomb {
         skyrme_quartic<T, C>(g, D, S, T(1));
         g[0] -= mass2;
         const T daux[3] = {D[0][4], D[1][4], D[2][4]};
-        T cs[4];
-        cs_coupling<T, C>(cs, phi, D, daux);
+        T cs[4], nd;
+        cs_coupling<T, C>(cs, phi, D, daux, &nd);
         const T k = kap / T(4.0 * M_PI * M_PI);
 #pragma unroll
         for (int mu = 0; mu < 4; ++mu) g[mu] -= k * cs[mu];
         project<T, C>(g, phi, p.nsky);
-        const T b0 = neg_det_b<T, C>(phi, D) / T(2.0 * M_PI * M_PI);
+        const T b0 = nd / T(2.0 * M_PI * M_PI);
         g[4] = -(kap * (S[0][4] + S[1][4] + S[2][4]) + kap * b0);
     }
     // th/coulomb_skyrme/kernels.py:231-306 (no A0*B0 term, :305)
