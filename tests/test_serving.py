@@ -230,27 +230,29 @@ def test_autotune_picks_a_measured_chunk(tmp_path):
 @pytest.mark.parametrize("name", ["nuclear", "omega"])
 def test_request_built_on_the_device(name):
     """A request that carries an initial configuration instead of a field is built on the
-    device at admission (omega seeded there too) and relaxes to the same solution as the
-    same configuration built on the host (the two fields differ in the last bits only)."""
+    device at admission (omega seeded there too): the solve is bitwise the one of a request
+    that carries that same field from the host.  (The device builder itself is checked
+    against the host builder in tests/test_init.py; tiny input differences are not compared
+    through a solve, since the arrest decisions of the omega flow amplify them.)"""
     import torch
     from skyrmion_solver_b200.engine import Engine
-    from skyrmion_solver_b200.theories._init_common import build_host_field, seed_omega
+    from skyrmion_solver_b200.theories._init_common import build_device_field, seed_omega
     from tests.test_march import params_for
     th, p_i, p_f = params_for(name, (24, 22, 26))
     cfg = {"mode": "hedgehog", "scale": 1.0, "center": (0.1, -0.1, 0.05), "vacuum_shell": 2}
-    host = build_host_field(name, p_i, p_f, cfg)
+    t = build_device_field(name, p_i, p_f, cfg)
     if name == "omega":
-        t = torch.from_numpy(host.ravel().copy()).cuda()
         seed_omega(t, p_i, p_f)
-        host = t.cpu().numpy().reshape(host.shape)
+    torch.cuda.synchronize()
+    host = t.cpu().numpy().reshape((int(p_i[5]),) + tuple(int(v) for v in p_i[:3]))
     out = {}
-    for key, req in (("host", Request(0, name, p_i, p_f, host, 0.0, 2e-4, 4000)),
-                     ("device", Request(0, name, p_i, p_f, None, 0.0, 2e-4, 4000, init=cfg))):
+    for key, req in (("host", Request(0, name, p_i, p_f, host, 0.0, 2e-4, 2000)),
+                     ("device", Request(0, name, p_i, p_f, None, 0.0, 2e-4, 2000, init=cfg))):
         with Engine(0) as eng:
             srv = Server(eng, chunk=32, plateau_chunks=4)
             srv.submit(req)
             out[key] = srv.run()[0]
     a, b = out["host"], out["device"]
-    assert a.status == b.status and a.steps == b.steps
-    assert abs(a.energy - b.energy) <= 1e-8 * abs(a.energy)
-    assert np.max(np.abs(a.field - b.field)) <= 1e-6
+    assert (a.status, a.steps, a.fp32_steps) == (b.status, b.steps, b.fp32_steps)
+    assert a.energy == b.energy and a.gabs == b.gabs
+    assert np.array_equal(a.field, b.field)
