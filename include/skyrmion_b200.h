@@ -30,8 +30,9 @@ typedef enum {
     SKY_OK = 0,
     SKY_ERR_INVALID = 1,   /* bad argument: sizes, parameter arrays, theory id */
     SKY_ERR_CUDA = 2,      /* a CUDA runtime call failed */
-    SKY_ERR_NONFINITE = 3, /* a reduction met NaN/Inf */
-    SKY_ERR_TIMEOUT = 4,   /* a bounded device-side wait gave up */
+    SKY_ERR_NONFINITE = 3, /* reserved: non-finite energies are returned as values, as the
+                              reference returns them (its step reports NaN, it does not raise) */
+    SKY_ERR_TIMEOUT = 4,   /* reserved: no kernel of the library waits on a flag or a peer */
     SKY_ERR_NOMEM = 5      /* caller-provided scratch too small / allocation failed */
 } sky_status;
 
