@@ -97,7 +97,7 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
             for (int c = 0; c < C; ++c)
                 if (c < nsky) ss += fv[c] * fv[c];
             if (ss != T(0)) {
-                const T r = rsqrt(ss);
+                const T r = ss == T(1) ? T(1) : rsqrt(ss);  // unit fields (the vacuum shell) stay exact
 #pragma unroll
                 for (int c = 0; c < C; ++c)
                     if (c < nsky) fv[c] *= r;
@@ -132,7 +132,7 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
             for (int c = 0; c < C; ++c)
                 if (c < nsky) ss = fma(fd[c], fd[c], ss);
             if (ss != 0.0) {
-                const double r = rsqrt(ss);
+                const double r = ss == 1.0 ? 1.0 : rsqrt(ss);  // unit fields (the vacuum shell) stay exact
 #pragma unroll
                 for (int c = 0; c < C; ++c)
                     if (c < nsky) fd[c] *= r;

@@ -402,3 +402,24 @@ def test_defect_refresh_period():
         fb, _ = eng.read(b)
         fc, _ = eng.read(c)
     assert G.rel_err(fc, fa) < G.rel_err(fb, fa)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32d"])
+def test_vacuum_shell_stays_exact(precision):
+    """The two-site boundary shell, where every derivative is masked, stays exactly at the
+    vacuum under engine steps in every precision (the reference's normalisation of a unit
+    vector is exact)."""
+    from skyrmion_solver_b200.engine import Engine
+    from skyrmion_solver_b200.initial import exp_profile, hedgehog, vacuum_shell, with_extra_components
+    from tests.test_march import params_for
+    dims = (24, 20, 28)
+    th, p_i, p_f = params_for("omega", dims)
+    F = with_extra_components(hedgehog(dims, (0.2, 0.18, 0.22), exp_profile(1.0)), 5)
+    vacuum_shell(F, 2)
+    with Engine(0) as eng:
+        i = eng.add("omega", (p_i, p_f), F, None, precision=precision)
+        eng.step(20)
+        f, v = eng.read(i)
+    shell = np.ones(dims, bool)
+    shell[2:-2, 2:-2, 2:-2] = False
+    assert np.all(f[0][shell] == 1.0) and np.all(f[1:4][:, shell] == 0.0)
