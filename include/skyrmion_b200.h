@@ -110,6 +110,17 @@ int sky_set_field_zero(const int32_t* p_i, int32_t n_pi, double* field, void* st
 int sky_create_grid(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf, double* grid,
                     void* stream);
 
+/* Baryon moments for the reference's compute_center_of_mass / compute_rms_radius
+ * (th/nuclear_skyrme/observables.py:182-270 with compute_center_of_mass_kernel
+ * and compute_rms_radius_kernel, th/nuclear_skyrme/kernels.py:678-758), in one
+ * fused pass: with b the per-site baryon density (h^3 included) and r the grid
+ * point (h_x i, h_y j, h_z k), out9_host = [sum b, sum b r (3), sum |b|,
+ * sum |b| r (3), sum |b| |r|^2] (compensated FP64, deterministic).  Then
+ * COM = sum b r / sum b and RMS^2 = sum |b| |r - COM|^2 / sum b.  scratch: a
+ * device buffer of sky_reduce_scratch_size() doubles.  Synchronous. */
+int sky_baryon_moments(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                       const double* field, double* scratch, int64_t n_scratch, double* out9_host, void* stream);
+
 /* Initial field on the device (replaces the reference's initial-configuration
  * kernels, th/nuclear_skyrme/initial_config.py:583-627, 664-698, 941-953,
  * 1082-1126): the normalised quaternion product, in order, of nsol <= 48

@@ -639,6 +639,36 @@ def total_baryon(theory, field, p_i, p_f):
     return block_tree_sum(baryon_density(theory, field, p_i, p_f))
 
 
+def _grid_points(p_i, p_f):
+    """create_grid_kernel (th/nuclear_skyrme/kernels.py:27-56): r = (h_x i, h_y j, h_z k)."""
+    X, Y, Z = (int(v) for v in p_i[:3])
+    return np.meshgrid(p_f[3] * np.arange(X), p_f[4] * np.arange(Y), p_f[5] * np.arange(Z), indexing="ij")
+
+
+def center_of_mass(theory, field, p_i, p_f):
+    """compute_center_of_mass (th/nuclear_skyrme/observables.py:182-221 with
+    compute_center_of_mass_kernel, kernels.py:678-718): sum b r / sum b; zeros when |B| < 1e-30."""
+    b = baryon_density(theory, field, p_i, p_f)
+    x, y, z = _grid_points(p_i, p_f)
+    B = block_tree_sum(b)
+    if abs(B) < 1.0e-30:
+        return np.zeros(3)
+    return np.array([block_tree_sum(b * x), block_tree_sum(b * y), block_tree_sum(b * z)]) / B
+
+
+def rms_radius(theory, field, p_i, p_f):
+    """compute_rms_radius (th/nuclear_skyrme/observables.py:224-270 with compute_rms_radius_kernel,
+    kernels.py:720-758): sqrt(max(sum |r - COM|^2 |b| / sum b, 0)); 0 when |B| < 1e-30."""
+    b = baryon_density(theory, field, p_i, p_f)
+    B = block_tree_sum(b)
+    if abs(B) < 1.0e-30:
+        return 0.0
+    com = center_of_mass(theory, field, p_i, p_f)
+    x, y, z = _grid_points(p_i, p_f)
+    num = block_tree_sum(((x - com[0]) ** 2 + (y - com[1]) ** 2 + (z - com[2]) ** 2) * np.abs(b))
+    return float(np.sqrt(max(num / B, 0.0)))
+
+
 def rk4_stage(V, l_in, F, k_prev, factor, dt):
     """do_rk4_step_kernel (core/integrator.py:50-92): k = dt(V + c l); Temp = F + c k_prev."""
     return dt * (V + factor * l_in), F + factor * k_prev

@@ -57,3 +57,59 @@ class BaryonObservable:
         p_i = p_i_h if p_i_h is not None else p_i_d
         p_f = p_f_h if p_f_h is not None else p_f_d
         return _total("sky_total_baryon", self.theory_id, Field, en, entmp, gridsum_partial, p_i, p_f)
+
+
+def _moments(theory_id, Field, gridsum_partial, p_i, p_f):
+    import numpy as np
+    hi, hf = host_params(p_i, p_f)
+    scratch = pick_scratch(gridsum_partial)
+    out = np.zeros(9)
+    _lib.call("sky_baryon_moments", theory_id, i32p(hi), len(hi), f64p(hf), len(hf), dptr(Field), dptr(scratch),
+              _numel(scratch), f64p(out), stream_ptr())
+    return out
+
+
+class CenterOfMassObservable:
+    """compute_center_of_mass(Field, grid, d1fd1x, obs4, tensor_scratch, entmp, gridsum_partial, p_i_d, p_f_d,
+    p_i_h) -> ndarray (3,): sum b r / sum b over the baryon density b (grid r = h * index), zeros when
+    |sum b| < 1e-30 (th/nuclear_skyrme/observables.py:182-221).  One fused device pass
+    (sky_baryon_moments); obs4 and tensor_scratch are not needed and left untouched."""
+
+    def __init__(self, theory_id):
+        self.theory_id = theory_id
+
+    def __call__(self, Field, grid, d1fd1x, obs4, tensor_scratch, entmp, gridsum_partial, p_i_d, p_f_d, p_i_h=None):
+        import numpy as np
+        m = _moments(self.theory_id, Field, gridsum_partial, p_i_h if p_i_h is not None else p_i_d, p_f_d)
+        if abs(m[0]) < 1.0e-30:
+            return np.zeros(3, dtype=np.float64)
+        return m[1:4] / m[0]
+
+
+class RmsRadiusObservable:
+    """compute_rms_radius(Field, grid, d1fd1x, en, entmp, gridsum_partial, obs4, tensor_scratch, com_d, p_i_d,
+    p_f_d, p_i_h) -> float: sqrt(max(sum |b| |r - COM|^2 / sum b, 0)), with the centre of mass also
+    written to com_d (th/nuclear_skyrme/observables.py:224-270).  One fused device pass; en and entmp
+    are left zeroed, as the reference's energy / baryon sums leave them."""
+
+    def __init__(self, theory_id):
+        self.theory_id = theory_id
+
+    def __call__(self, Field, grid, d1fd1x, en, entmp, gridsum_partial, obs4, tensor_scratch, com_d, p_i_d, p_f_d,
+                 p_i_h=None):
+        import math
+        import numpy as np
+        m = _moments(self.theory_id, Field, gridsum_partial, p_i_h if p_i_h is not None else p_i_d, p_f_d)
+        B = m[0]
+        com = np.zeros(3) if abs(B) < 1.0e-30 else m[1:4] / B
+        if com_d is not None:
+            import torch
+            if isinstance(com_d, torch.Tensor):
+                com_d.copy_(torch.from_numpy(com))
+            else:
+                com_d.copy_to_device(com)
+        _zero(en, entmp)
+        if abs(B) < 1.0e-30:
+            return 0.0
+        num = m[8] - 2.0 * float(np.dot(com, m[5:8])) + float(np.dot(com, com)) * m[4]
+        return math.sqrt(max(num / B, 0.0))

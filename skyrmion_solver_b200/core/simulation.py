@@ -133,6 +133,18 @@ class Simulation:
         g, b = self._launch()
         self.kernels.compute_rho_meson_kernel[g, b](self.en, self.Field, self.p_i_d)
 
+    def compute_center_of_mass(self) -> np.ndarray:
+        """Baryon-density centre of mass (core/simulation.py:390-403)."""
+        return self.observables_mod.compute_center_of_mass(self.Field, self.grid, None, None, None, self.entmp,
+                                                           self.gridsum_partial, self.p_i_d, self.p_f_d,
+                                                           self.p_i_h)
+
+    def compute_rms_radius(self) -> float:
+        """Centre-of-mass RMS radius (core/simulation.py:405-418); the centre of mass lands in com_d."""
+        return self.observables_mod.compute_rms_radius(self.Field, self.grid, None, self.en, self.entmp,
+                                                       self.gridsum_partial, None, None, self.com_d, self.p_i_d,
+                                                       self.p_f_d, self.p_i_h)
+
     def step(self, prev_energy: float):
         """One arrested-Newton / RK4 step; returns (new_energy, err) (core/simulation.py:287-308)."""
         compute_norm = getattr(self.observables_mod, "compute_norm", None)

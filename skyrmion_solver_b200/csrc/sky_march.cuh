@@ -562,6 +562,68 @@ __global__ void __launch_bounds__(M::NTHREADS) k_march_density(Params p, MarchGr
     if (scratch) finish_ksum(es, scratch, out_dev, shk);
 }
 
+// ---------------------------------------------------------------------------
+// Baryon moments of a reference-layout FP64 field, for the centre of mass and
+// the RMS radius (compute_center_of_mass_kernel / compute_rms_radius_kernel,
+// th/nuclear_skyrme/kernels.py:678-758, and their host sums,
+// th/nuclear_skyrme/observables.py:182-270): with b the baryon density of a
+// site (h^3 included) and r = (h_x i, h_y j, h_z k) its grid point
+// (create_grid_kernel), the nine sums of b, b r, |b|, |b| r and |b| |r|^2.
+// Each block writes its compensated partials to parts[18 * block + 2 q].
+// ---------------------------------------------------------------------------
+constexpr int kMoments = 9;
+
+struct MomentEpi {
+    Params p;
+    KSum m[kMoments];
+    __device__ __forceinline__ void density(int64_t s, double b) {
+        const int64_t YZ = (int64_t)p.Y * p.Z;
+        const int ix = (int)(s / YZ);
+        const int64_t r = s - (int64_t)ix * YZ;
+        const int iy = (int)(r / p.Z);
+        const int iz = (int)(r - (int64_t)iy * p.Z);
+        const double x = p.hx * ix, y = p.hy * iy, z = p.hz * iz;
+        const double a = fabs(b);
+        ksum_add(m[0], b);
+        ksum_add(m[1], b * x);
+        ksum_add(m[2], b * y);
+        ksum_add(m[3], b * z);
+        ksum_add(m[4], a);
+        ksum_add(m[5], a * x);
+        ksum_add(m[6], a * y);
+        ksum_add(m[7], a * z);
+        ksum_add(m[8], a * (x * x + y * y + z * z));
+    }
+};
+
+template <template <typename> class Th, class M>
+__global__ void __launch_bounds__(M::NTHREADS) k_march_moments(Params p, MarchGrid mg, const double* __restrict__ field,
+                                                               double* __restrict__ parts) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double* sm = reinterpret_cast<double*>(smraw);
+    __shared__ KSum shk[M::NTHREADS / 32];
+    MomentEpi epi;
+    epi.p = p;
+#pragma unroll
+    for (int q = 0; q < kMoments; ++q) epi.m[q] = KSum{0.0, 0.0};
+    const double* const src[3] = {field, nullptr, nullptr};
+    KSum es{0.0, 0.0}, unused{0.0, 0.0};
+    for (int t = blockIdx.x; t < mg.count(); t += gridDim.x) {
+        int xa, xe, y0, z0;
+        march_origin(mg, t, M::BY, xa, xe, y0, z0, p.X);
+        march_tile<Th, M, double, 1, 2, MomentEpi, false, double, false>(sm, p, src, 0.0, 0.0, xa, xe, y0, z0, epi,
+                                                                         es, unused);
+    }
+#pragma unroll
+    for (int q = 0; q < kMoments; ++q) {
+        const KSum b = block_ksum(epi.m[q], shk);
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            parts[2 * kMoments * blockIdx.x + 2 * q] = b.s;
+            parts[2 * kMoments * blockIdx.x + 2 * q + 1] = b.c;
+        }
+    }
+}
+
 template <template <typename> class Th, class M, typename T>
 __global__ void __launch_bounds__(M::NTHREADS) k_march_plain(Params p, MarchGrid mg, const T* __restrict__ field,
                                                              T* __restrict__ eg, T* __restrict__ l) {

@@ -448,6 +448,47 @@ int dens64(const Params& p, int mode, const double* f, double* dens, double* scr
                      : launch_density<Th, 1, double>(p, f, dens, scratch, out_dev, st);
 }
 
+// Baryon moments (k_march_moments): at most kScratchDoubles / 18 blocks, so the
+// per-block partials fit the standard reduction scratch.
+template <template <typename> class Th>
+int moments64(const Params& p, const double* f, double* scratch, double* out9, cudaStream_t st) {
+    using M = MarchShape<4, 8, false>;
+    auto kern = k_march_moments<Th, M>;
+    const size_t smem = M::template smem_bytes<double>(1);
+    static bool configured = false;
+    if (!configured) {
+        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(moments)", __LINE__);
+        if (rc) return rc;
+        configured = true;
+    }
+    const int cap = kScratchDoubles / (2 * kMoments);
+    const MarchGrid g0 = march_grid<M>(p, p.X);
+    const MarchGrid mg = march_grid<M>(p, choose_xc(p.X, g0.nz * g0.ny, num_sms()));
+    const int blocks = mg.count() < cap ? mg.count() : cap;
+    kern<<<blocks, dim3(M::BZ, M::BY), smem, st>>>(p, mg, f, scratch);
+    int rc = check_cuda(cudaGetLastError(), "launch moments", __LINE__);
+    if (rc) return rc;
+    double parts[2 * kMoments * (kScratchDoubles / (2 * kMoments))];
+    rc = check_cuda(cudaMemcpyAsync(parts, scratch, sizeof(double) * 2 * kMoments * blocks, cudaMemcpyDeviceToHost, st),
+                    "read moments", __LINE__);
+    if (!rc) rc = check_cuda(cudaStreamSynchronize(st), "sync", __LINE__);
+    if (rc) return rc;
+    for (int q = 0; q < kMoments; ++q) {   // fixed-order compensated sum over the blocks
+        double sum = 0.0, comp = 0.0;
+        for (int b = 0; b < blocks; ++b) {
+            for (int k = 0; k < 2; ++k) {
+                const double v = parts[2 * kMoments * b + 2 * q + k];
+                const double t = sum + v;
+                comp += (fabs(sum) >= fabs(v)) ? ((sum - t) + v) : ((v - t) + sum);
+                sum = t;
+            }
+        }
+        out9[q] = sum + comp;
+    }
+    return SKY_OK;
+}
+
 int gradient_fp64(int theory, const Params& p, const double* f, double* eg, double* l, cudaStream_t st) {
     SKY_DISPATCH(theory, grad64, p, f, eg, l, st)
 }
@@ -677,6 +718,17 @@ int sky_total_energy(int theory, const int32_t* p_i, int32_t n_pi, const double*
 int sky_total_baryon(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
                      const double* field, double* scratch, int64_t n_scratch, double* out_host, void* stream) {
     return total_entry(1, theory, p_i, n_pi, p_f, n_pf, field, scratch, n_scratch, out_host, stream);
+}
+
+int sky_baryon_moments(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                       const double* field, double* scratch, int64_t n_scratch, double* out9_host, void* stream) {
+    Params p;
+    int rc = pack_params(theory, p_i, n_pi, p_f, n_pf, &p);
+    if (rc) return rc;
+    if (!field || !out9_host) return invalid("null buffer");
+    if (!scratch || n_scratch < kScratchDoubles) return SKY_ERR_NOMEM;
+    if ((int64_t)4 * n_sites(p) >= ((int64_t)1 << 31)) return invalid("lattice too large for the moments kernel");
+    SKY_DISPATCH(theory, moments64, p, field, scratch, out9_host, SKY_STREAM(stream))
 }
 
 int sky_arrested_newton_step(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,

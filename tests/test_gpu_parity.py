@@ -83,6 +83,23 @@ def test_observables(gold):
     assert not sim.en.any() and not sim.entmp.any()
 
 
+def test_center_of_mass_and_rms_radius(gold):
+    """Simulation.compute_center_of_mass / compute_rms_radius (one fused moments pass) against the
+    oracle's restatement of the reference's two kernels and host sums."""
+    from oracle import skyrme_oracle as O
+    name, d = gold
+    th, sim = golden_simulation(name, d)
+    thd = O.THEORIES[name]
+    com = sim.compute_center_of_mass()
+    ref = O.center_of_mass(thd, d["field0"], d["p_i"], d["p_f"])
+    assert np.max(np.abs(com - ref)) <= 1e-12 * max(1.0, float(np.max(np.abs(ref))))
+    r = sim.compute_rms_radius()
+    rref = O.rms_radius(thd, d["field0"], d["p_i"], d["p_f"])
+    assert abs(r - rref) <= 1e-10 * max(1.0, abs(rref))
+    assert np.allclose(host(sim.com_d), ref, rtol=0, atol=1e-12 * max(1.0, float(np.max(np.abs(ref)))))
+    assert not sim.en.any() and not sim.entmp.any()
+
+
 def test_arrested_newton_steps(gold):
     name, d = gold
     th, sim = golden_simulation(name, d)

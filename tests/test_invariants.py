@@ -67,3 +67,20 @@ def test_boundary_shell_stays_at_the_vacuum(name):
     shell[2:-2, 2:-2, 2:-2] = False
     assert np.all(F[0][shell] == 1.0)
     assert np.all(F[1:][:, shell] == 0.0)
+
+
+def test_centre_of_mass_and_radius_of_a_displaced_hedgehog():
+    """The oracle's centre of mass (reference grid r = h * index) sits at the hedgehog's centre;
+    a symmetric hedgehog's RMS radius does not depend on where it sits."""
+    from skyrmion_solver_b200.initial import exp_profile, hedgehog
+    L, h = 40, 0.2
+    p_i, p_f = _params("nuclear", L, h)
+    thd = O.THEORIES["nuclear"]
+    mid = (L - 1) / 2.0 * h
+    r0 = []
+    for c in ((0.0, 0.0, 0.0), (0.4, -0.2, 0.2)):
+        F = hedgehog((L, L, L), (h, h, h), exp_profile(0.7), center=c)
+        com = O.center_of_mass(thd, F, p_i, p_f)
+        assert np.max(np.abs(com - (mid + np.asarray(c)))) <= 2e-3, com
+        r0.append(O.rms_radius(thd, F, p_i, p_f))
+    assert abs(r0[0] - r0[1]) <= 1e-2 * r0[0]
