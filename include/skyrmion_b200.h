@@ -121,6 +121,19 @@ int sky_create_grid(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t
 int sky_baryon_moments(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
                        const double* field, double* scratch, int64_t n_scratch, double* out9_host, void* stream);
 
+/* The nuclear model's inertia and shape diagnostics (compute_U_tensor,
+ * compute_V_tensor, compute_W_tensor, compute_quadrupole_tensor and the
+ * D-term integral of compute_D_term; th/nuclear_skyrme/observables.py:273-487
+ * with kernels.py:484-1033) in one fused FP64 pass, about the centre of mass
+ * com_host (host, 3 doubles; e.g. from sky_baryon_moments).  out28_host =
+ * [U00 U01 U02 U11 U12 U22, V (the same six), W00..W22 (nine, row-major),
+ * Q (six, as U), D integral], compensated and deterministic; the D-term is
+ * -(2/5) E times the last entry.  scratch: sky_reduce_scratch_size() doubles.
+ * Synchronous. */
+int sky_nuclear_diagnostics(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                            const double* field, const double* com_host, double* scratch, int64_t n_scratch,
+                            double* out28_host, void* stream);
+
 /* Initial field on the device (replaces the reference's initial-configuration
  * kernels, th/nuclear_skyrme/initial_config.py:583-627, 664-698, 941-953,
  * 1082-1126): the normalised quaternion product, in order, of nsol <= 48

@@ -669,6 +669,126 @@ def rms_radius(theory, field, p_i, p_f):
     return float(np.sqrt(max(num / B, 0.0)))
 
 
+# ---------------------------------------------------------------------------
+# nuclear-model diagnostics (th/nuclear_skyrme/kernels.py:484-1033,
+# observables.py:273-487)
+# ---------------------------------------------------------------------------
+_EPS3 = np.zeros((3, 3, 3))
+for _i, _j, _k in ((0, 1, 2), (1, 2, 0), (2, 0, 1)):
+    _EPS3[_i, _j, _k] = 1.0
+    _EPS3[_i, _k, _j] = -1.0
+
+
+def _currents(field, D):
+    """_build_left_and_iso_currents (kernels.py:484-547): left currents lcur[k, a] and
+    isorotation currents tcur[i, a], arrays of shape (3, 3, X, Y, Z)."""
+    s = field[0]
+    pi = field[1:4]
+    lcur = np.empty((3, 3) + s.shape)
+    for k in range(3):
+        ds = D[k, 0]
+        dp = D[k, 1:4]
+        cross = np.stack([pi[1] * dp[2] - pi[2] * dp[1], pi[2] * dp[0] - pi[0] * dp[2],
+                          pi[0] * dp[1] - pi[1] * dp[0]])
+        for a in range(3):
+            lcur[k, a] = s * dp[a] - pi[a] * ds + cross[a]
+    pi2 = (pi ** 2).sum(axis=0)
+    tcur = np.empty((3, 3) + s.shape)
+    for i in range(3):
+        for a in range(3):
+            v = pi[i] * pi[a] - (pi2 if i == a else 0.0)
+            tcur[i, a] = v + s * sum(_EPS3[i, a, b] * pi[b] for b in range(3))
+    return lcur, tcur
+
+
+def _gram(a, b):
+    return np.einsum("iaxyz,jaxyz->ijxyz", a, b)
+
+
+def _site_tensors(field, p_i, p_f):
+    g = Grid.from_params(p_i, p_f)
+    D, _ = derivatives(field, g, comps=range(4), second=False)
+    lcur, tcur = _currents(field, D)
+    LL, TT, LT = _gram(lcur, lcur), _gram(tcur, tcur), _gram(tcur, lcur)
+    return D, lcur, tcur, LL, TT, LT
+
+
+def _r_minus_com(theory, field, p_i, p_f):
+    com = center_of_mass(theory, field, p_i, p_f)
+    x, y, z = _grid_points(p_i, p_f)
+    return np.stack([x - com[0], y - com[1], z - com[2]])
+
+
+def _sum9(t):
+    return np.array([[block_tree_sum(t[i, j]) for j in range(3)] for i in range(3)])
+
+
+def u_tensor(theory, field, p_i, p_f):
+    """compute_U_tensor: sum of 2 U0 h^3, U0 = TT + kappa^2 sum_k (TT_ij LL_kk - LT_ik LT_jk)
+    (_compute_U0_and_A, kernels.py:548-612; compute_U_tensor_kernel, :813-851)."""
+    k2 = p_f[9] * p_f[9]
+    _, _, _, LL, TT, LT = _site_tensors(field, p_i, p_f)
+    trLL = LL[0, 0] + LL[1, 1] + LL[2, 2]
+    U0 = TT + k2 * (TT * trLL - np.einsum("ikxyz,jkxyz->ijxyz", LT, LT))
+    return _sum9(2.0 * U0 * p_f[6])
+
+
+def v_tensor(theory, field, p_i, p_f):
+    """compute_V_tensor: sum of 2 h^3 eps_ilm eps_jnp r_l r_n A_mp, A = LL + kappa^2 sum_k
+    (LL_ij LL_kk - LL_ik LL_jk), r from the centre of mass (kernels.py:852-905)."""
+    k2 = p_f[9] * p_f[9]
+    _, _, _, LL, _, _ = _site_tensors(field, p_i, p_f)
+    trLL = LL[0, 0] + LL[1, 1] + LL[2, 2]
+    A = LL + k2 * (LL * trLL - np.einsum("ikxyz,jkxyz->ijxyz", LL, LL))
+    r = _r_minus_com(theory, field, p_i, p_f)
+    V = np.einsum("ilm,jnp,lxyz,nxyz,mpxyz->ijxyz", _EPS3, _EPS3, r, r, A)
+    return _sum9(2.0 * V * p_f[6])
+
+
+def w_tensor(theory, field, p_i, p_f):
+    """compute_W_tensor: sum of 2 h^3 eps_jlm r_l B_im, B = LT + kappa^2 sum_k (LT_im LL_kk -
+    LT_ik LL_mk) (kernels.py:906-975)."""
+    k2 = p_f[9] * p_f[9]
+    _, _, _, LL, _, LT = _site_tensors(field, p_i, p_f)
+    trLL = LL[0, 0] + LL[1, 1] + LL[2, 2]
+    Bm = LT + k2 * (LT * trLL - np.einsum("ikxyz,mkxyz->imxyz", LT, LL))
+    r = _r_minus_com(theory, field, p_i, p_f)
+    W = np.einsum("jlm,lxyz,imxyz->ijxyz", _EPS3, r, Bm)
+    return _sum9(2.0 * W * p_f[6])
+
+
+def quadrupole_tensor(theory, field, p_i, p_f):
+    """compute_quadrupole_tensor: sum of (3 r_i r_j - delta_ij r^2) b / 2 (kernels.py:760-812)."""
+    b = baryon_density(theory, field, p_i, p_f)
+    r = _r_minus_com(theory, field, p_i, p_f)
+    r2 = (r ** 2).sum(axis=0)
+    Q = 3.0 * np.einsum("ixyz,jxyz->ijxyz", r, r)
+    for i in range(3):
+        Q[i, i] -= r2
+    return _sum9(Q * (0.5 * b))
+
+
+def d_term(theory, field, p_i, p_f):
+    """compute_D_term: -(2/5) E sum h^3 (r_i r_j T_ij - r^2 tr T / 3), T the stress tensor
+    (_compute_stress_tensor, kernels.py:614-676; compute_D_integrand_kernel, :976-1033;
+    observables.py:440-487)."""
+    m2 = p_f[8] * p_f[8]
+    k2 = p_f[9] * p_f[9]
+    _, _, _, LL, _, _ = _site_tensors(field, p_i, p_f)
+    trD = LL[0, 0] + LL[1, 1] + LL[2, 2]
+    quartic = sum(LL[i, i] * LL[j, j] - LL[i, j] * LL[i, j] for i in range(3) for j in range(i + 1, 3))
+    e = 0.5 * trD + 0.5 * k2 * quartic + m2 * (1.0 - field[0])
+    T = LL + k2 * (trD * LL - np.einsum("ikxyz,kjxyz->ijxyz", LL, LL))
+    for i in range(3):
+        T[i, i] -= e
+    r = _r_minus_com(theory, field, p_i, p_f)
+    r2 = (r ** 2).sum(axis=0)
+    trT = T[0, 0] + T[1, 1] + T[2, 2]
+    scalar = np.einsum("ixyz,jxyz,ijxyz->xyz", r, r, T) - r2 * trT / 3.0
+    E = total_energy(theory, field, p_i, p_f)
+    return -(2.0 / 5.0) * E * block_tree_sum(scalar * p_f[6])
+
+
 def rk4_stage(V, l_in, F, k_prev, factor, dt):
     """do_rk4_step_kernel (core/integrator.py:50-92): k = dt(V + c l); Temp = F + c k_prev."""
     return dt * (V + factor * l_in), F + factor * k_prev

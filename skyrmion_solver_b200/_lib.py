@@ -73,6 +73,7 @@ SIGNATURES = {
                                  _I),
     "sky_arrested_newton_step_noalloc": ([_I, _I32P, _I32, _F64P, _I32, _P, _P, _P, _D, _F64P, _F64P, _P], _I),
     "sky_baryon_moments": ([_I, _I32P, _I32, _F64P, _I32, _P, _P, _I64, _F64P, _P], _I),
+    "sky_nuclear_diagnostics": ([_I32P, _I32, _F64P, _I32, _P, _F64P, _P, _I64, _F64P, _P], _I),
     "sky_init_field": ([_I32P, _I32, _F64P, _I32, _I32, _I32P, _F64P, _F64P, _D, _I32, _P, _P], _I),
     "sky_engine_create": ([_I, ctypes.POINTER(ctypes.c_void_p)], _I),
     "sky_engine_destroy": ([_P], _I),

@@ -113,3 +113,104 @@ class RmsRadiusObservable:
             return 0.0
         num = m[8] - 2.0 * float(np.dot(com, m[5:8])) + float(np.dot(com, com)) * m[4]
         return math.sqrt(max(num / B, 0.0))
+
+
+# ---------------------------------------------------------------------------
+# nuclear-model inertia and shape diagnostics (th/nuclear_skyrme/observables.py:273-487)
+# ---------------------------------------------------------------------------
+def _sym(v6):
+    import numpy as np
+    a, b, c, d, e, f = v6
+    return np.array([[a, b, c], [b, d, e], [c, e, f]], dtype=np.float64)
+
+
+def _nuclear_diag(theory_id, Field, gridsum_partial, p_i, p_f):
+    """(centre of mass, the 28 fused sums of sky_nuclear_diagnostics)."""
+    import numpy as np
+    m = _moments(theory_id, Field, gridsum_partial, p_i, p_f)
+    com = np.zeros(3) if abs(m[0]) < 1.0e-30 else m[1:4] / m[0]
+    hi, hf = host_params(p_i, p_f)
+    scratch = pick_scratch(gridsum_partial)
+    out = np.zeros(28)
+    _lib.call("sky_nuclear_diagnostics", i32p(hi), len(hi), f64p(hf), len(hf), dptr(Field), f64p(np.ascontiguousarray(com)),
+              dptr(scratch), _numel(scratch), f64p(out), stream_ptr())
+    return com, out
+
+
+def _store_com(com_d, com):
+    if com_d is None:
+        return
+    import torch
+    if isinstance(com_d, torch.Tensor):
+        com_d.copy_(torch.from_numpy(com))
+    else:
+        com_d.copy_to_device(com)
+
+
+class UTensorObservable:
+    """compute_U_tensor(Field, d1fd1x, obs9, tensor_scratch, entmp, gridsum_partial, p_i_d, p_f_d, p_i_h)
+    -> (3, 3): the isospin inertia tensor (observables.py:273-305)."""
+
+    def __init__(self, theory_id):
+        self.theory_id = theory_id
+
+    def __call__(self, Field, d1fd1x, obs9, tensor_scratch, entmp, gridsum_partial, p_i_d, p_f_d, p_i_h=None):
+        _, out = _nuclear_diag(self.theory_id, Field, gridsum_partial, p_i_h if p_i_h is not None else p_i_d, p_f_d)
+        return _sym(out[0:6])
+
+
+class _ComTensorObservable:
+    """(Field, grid, d1fd1x, obs9, tensor_scratch, entmp, gridsum_partial, obs4, com_d, p_i_d, p_f_d, p_i_h)
+    -> (3, 3), about the centre of mass, which is also written to com_d."""
+
+    def __init__(self, theory_id):
+        self.theory_id = theory_id
+
+    def __call__(self, Field, grid, d1fd1x, obs9, tensor_scratch, entmp, gridsum_partial, obs4, com_d, p_i_d, p_f_d,
+                 p_i_h=None):
+        com, out = _nuclear_diag(self.theory_id, Field, gridsum_partial, p_i_h if p_i_h is not None else p_i_d,
+                                 p_f_d)
+        _store_com(com_d, com)
+        return self.pick(out)
+
+
+class VTensorObservable(_ComTensorObservable):
+    """compute_V_tensor: the spin inertia tensor (observables.py:308-349)."""
+
+    @staticmethod
+    def pick(out):
+        return _sym(out[6:12])
+
+
+class WTensorObservable(_ComTensorObservable):
+    """compute_W_tensor: the mixed inertia tensor (observables.py:352-393)."""
+
+    @staticmethod
+    def pick(out):
+        return out[12:21].reshape(3, 3).copy()
+
+
+class QuadrupoleTensorObservable(_ComTensorObservable):
+    """compute_quadrupole_tensor: the baryon quadrupole tensor (observables.py:396-437)."""
+
+    @staticmethod
+    def pick(out):
+        return _sym(out[21:27])
+
+
+class DTermObservable:
+    """compute_D_term(Field, grid, d1fd1x, en, entmp, gridsum_partial, obs4, tensor_scratch, com_d, p_i_d, p_f_d,
+    p_i_h, p_f_h) -> float: -(2/5) E times the stress integral about the centre of mass
+    (observables.py:440-487); en and entmp are left zeroed."""
+
+    def __init__(self, theory_id):
+        self.theory_id = theory_id
+
+    def __call__(self, Field, grid, d1fd1x, en, entmp, gridsum_partial, obs4, tensor_scratch, com_d, p_i_d, p_f_d,
+                 p_i_h=None, p_f_h=None):
+        p_i = p_i_h if p_i_h is not None else p_i_d
+        p_f = p_f_h if p_f_h is not None else p_f_d
+        com, out = _nuclear_diag(self.theory_id, Field, gridsum_partial, p_i, p_f)
+        _store_com(com_d, com)
+        E = _total("sky_total_energy", self.theory_id, Field, en, entmp, gridsum_partial, p_i, p_f)
+        return -(2.0 / 5.0) * E * float(out[27])

@@ -139,6 +139,33 @@ class Simulation:
                                                            self.gridsum_partial, self.p_i_d, self.p_f_d,
                                                            self.p_i_h)
 
+    def compute_U_tensor(self) -> np.ndarray:
+        """Isospin inertia tensor (core/simulation.py:420-433)."""
+        return self.observables_mod.compute_U_tensor(self.Field, None, None, None, self.entmp, self.gridsum_partial,
+                                                     self.p_i_d, self.p_f_d, self.p_i_h)
+
+    def _com_tensor(self, fn):
+        return fn(self.Field, self.grid, None, None, None, self.entmp, self.gridsum_partial, None, self.com_d,
+                  self.p_i_d, self.p_f_d, self.p_i_h)
+
+    def compute_V_tensor(self) -> np.ndarray:
+        """Spin inertia tensor (core/simulation.py:435-448)."""
+        return self._com_tensor(self.observables_mod.compute_V_tensor)
+
+    def compute_W_tensor(self) -> np.ndarray:
+        """Mixed inertia tensor (core/simulation.py:450-463)."""
+        return self._com_tensor(self.observables_mod.compute_W_tensor)
+
+    def compute_quadrupole_tensor(self) -> np.ndarray:
+        """Baryon quadrupole tensor (core/simulation.py:465-478)."""
+        return self._com_tensor(self.observables_mod.compute_quadrupole_tensor)
+
+    def compute_D_term(self) -> float:
+        """Monopole D-term (core/simulation.py:480-500)."""
+        return self.observables_mod.compute_D_term(self.Field, self.grid, None, self.en, self.entmp,
+                                                   self.gridsum_partial, None, None, self.com_d, self.p_i_d,
+                                                   self.p_f_d, self.p_i_h, self.p_f_h)
+
     def compute_rms_radius(self) -> float:
         """Centre-of-mass RMS radius (core/simulation.py:405-418); the centre of mass lands in com_d."""
         return self.observables_mod.compute_rms_radius(self.Field, self.grid, None, self.en, self.entmp,

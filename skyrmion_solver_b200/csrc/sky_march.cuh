@@ -287,7 +287,8 @@ __device__ __forceinline__ T diff5(const T* f, int st) {
 // epilogue); the ring may then hold just the first M::C <= Th::C components
 // (the baryon density needs phi_0..3 only) and each site's FP64 density (the
 // potential of the RK4 dynamics when DENS & 4, else energy when DENS & 1, else
-// baryon) is passed to epi.density(s, value).
+// baryon) is passed to epi.density(s, value); with DENS & 16 the site's FP64
+// field values and first derivatives go to epi.site(s, phi, D) instead.
 template <template <typename> class Th, class M, typename T, int NSRC, int DENS, class Epi, bool LO = false,
           typename S = T, bool GRAD = true>
 __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, const S* const (&src)[3], T a, T b,
@@ -466,6 +467,8 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                 if constexpr (GRAD) {
                     ksum_add(esum, Th<double>::energy(phd, Dd, p));
                     ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
+                } else if constexpr ((DENS & 16) != 0) {
+                    epi.site(s, phd, Dd);  // the epilogue reads the FP64 field and first derivatives
                 } else {
                     double v;
                     if constexpr ((DENS & 4) != 0)
@@ -620,6 +623,178 @@ __global__ void __launch_bounds__(M::NTHREADS) k_march_moments(Params p, MarchGr
         if (threadIdx.x == 0 && threadIdx.y == 0) {
             parts[2 * kMoments * blockIdx.x + 2 * q] = b.s;
             parts[2 * kMoments * blockIdx.x + 2 * q + 1] = b.c;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Nuclear-model diagnostics in one FP64 pass (th/nuclear_skyrme/kernels.py:
+// 484-1033 and observables.py:273-487): per site the left currents L_k and
+// isorotation currents T_i, their Gram matrices LL, TT, LT, and with
+// r = grid point - centre of mass (grid point = (h_x i, h_y j, h_z k)):
+//   U  += 2 h^3 U0,  U0 = TT + kappa^2 (TT tr LL - LT LT^T)          (symmetric)
+//   V  += 2 h^3 r x (r x A),  A = LL + kappa^2 (LL tr LL - LL LL)   (symmetric)
+//   W  += 2 h^3 r x B_i,      B = LT + kappa^2 (LT tr LL - LT LL)
+//   Q  += (3 r r^T - r^2) b / 2                                      (symmetric)
+//   D  += h^3 (r^T S r - r^2 tr S / 3),  S the stress tensor
+// (V_ij = eps_ilm eps_jnp r_l r_n A_mp and W_ij = eps_jlm r_l B_im, written as
+// cross products).  28 sums, accumulated per thread and reduced per block with
+// compensation; parts[56 * block + 2 q].
+// ---------------------------------------------------------------------------
+constexpr int kDiag = 28;  // U(6) V(6) W(9) Q(6) D(1)
+
+struct DiagEpi {
+    Params p;
+    double com[3];
+    double acc[kDiag];
+    __device__ __forceinline__ static void cross3(const double* a, const double* b, double* o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    }
+    __device__ __forceinline__ void site(int64_t s, const double* phi, const double (&D)[3][4]) {
+        const double k2 = p.c1 * p.c1, m2 = p.c0 * p.c0, vol = p.vol;
+        const double sg = phi[0];
+        const double pi[3] = {phi[1], phi[2], phi[3]};
+        double L[3][3], T[3][3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double ds = D[k][0];
+            const double dp[3] = {D[k][1], D[k][2], D[k][3]};
+            double cr[3];
+            cross3(pi, dp, cr);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) L[k][a] = sg * dp[a] - pi[a] * ds + cr[a];
+        }
+        const double pi2 = pi[0] * pi[0] + pi[1] * pi[1] + pi[2] * pi[2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                double e = 0.0;
+#pragma unroll
+                for (int b = 0; b < 3; ++b) e += double(eps3(i, a, b)) * pi[b];
+                T[i][a] = pi[i] * pi[a] - (i == a ? pi2 : 0.0) + sg * e;
+            }
+        double LL[3][3], TT[3][3], LT[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                LL[i][j] = L[i][0] * L[j][0] + L[i][1] * L[j][1] + L[i][2] * L[j][2];
+                TT[i][j] = T[i][0] * T[j][0] + T[i][1] * T[j][1] + T[i][2] * T[j][2];
+                LT[i][j] = T[i][0] * L[j][0] + T[i][1] * L[j][1] + T[i][2] * L[j][2];
+            }
+        const double tr = LL[0][0] + LL[1][1] + LL[2][2];
+        // grid point relative to the centre of mass
+        const int64_t YZ = (int64_t)p.Y * p.Z;
+        const int ix = (int)(s / YZ);
+        const int64_t rem = s - (int64_t)ix * YZ;
+        const int iy = (int)(rem / p.Z);
+        const int iz = (int)(rem - (int64_t)iy * p.Z);
+        const double r[3] = {p.hx * ix - com[0], p.hy * iy - com[1], p.hz * iz - com[2]};
+        const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+        const int si[6] = {0, 0, 0, 1, 1, 2}, sj[6] = {0, 1, 2, 1, 2, 2};
+        // U
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const int i = si[q], j = sj[q];
+            const double u = TT[i][j] + k2 * (TT[i][j] * tr - (LT[i][0] * LT[j][0] + LT[i][1] * LT[j][1] +
+                                                                 LT[i][2] * LT[j][2]));
+            acc[q] += 2.0 * vol * u;
+        }
+        // V = r x (r x A): X[:, p] = r x A[:, p], then V[i, :] = r x X[i, :]
+        double A[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                A[i][j] = LL[i][j] + k2 * (LL[i][j] * tr - (LL[i][0] * LL[j][0] + LL[i][1] * LL[j][1] +
+                                                             LL[i][2] * LL[j][2]));
+        double X[3][3];
+#pragma unroll
+        for (int pp = 0; pp < 3; ++pp) {
+            const double col[3] = {A[0][pp], A[1][pp], A[2][pp]};
+            double o[3];
+            cross3(r, col, o);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) X[i][pp] = o[i];
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const int i = si[q], j = sj[q];
+            double o[3];
+            cross3(r, X[i], o);
+            acc[6 + q] += 2.0 * vol * o[j];
+        }
+        // W[i, :] = r x B[i, :]
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            double Bi[3];
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+                Bi[m] = LT[i][m] + k2 * (LT[i][m] * tr - (LT[i][0] * LL[m][0] + LT[i][1] * LL[m][1] +
+                                                           LT[i][2] * LL[m][2]));
+            double o[3];
+            cross3(r, Bi, o);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc[12 + 3 * i + j] += 2.0 * vol * o[j];
+        }
+        // Q
+        const double rho = 0.5 * Nuclear<double>::baryon(phi, D, p);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const int i = si[q], j = sj[q];
+            acc[21 + q] += (3.0 * r[i] * r[j] - (i == j ? r2 : 0.0)) * rho;
+        }
+        // D-term integrand: S = LL + kappa^2 (tr LL - LL LL) - e 1
+        double quartic = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = i + 1; j < 3; ++j) quartic += LL[i][i] * LL[j][j] - LL[i][j] * LL[i][j];
+        const double e = 0.5 * tr + 0.5 * k2 * quartic + m2 * (1.0 - sg);
+        double rSr = 0.0, trS = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double d2 = LL[i][0] * LL[0][j] + LL[i][1] * LL[1][j] + LL[i][2] * LL[2][j];
+                const double Sij = LL[i][j] + k2 * (tr * LL[i][j] - d2) - (i == j ? e : 0.0);
+                rSr += r[i] * r[j] * Sij;
+                if (i == j) trS += Sij;
+            }
+        acc[27] += (rSr - r2 * trS / 3.0) * vol;
+    }
+};
+
+template <class M>
+__global__ void __launch_bounds__(M::NTHREADS) k_march_diag(Params p, MarchGrid mg, const double* __restrict__ field,
+                                                            double cx, double cy, double cz,
+                                                            double* __restrict__ parts) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double* sm = reinterpret_cast<double*>(smraw);
+    __shared__ KSum shk[M::NTHREADS / 32];
+    DiagEpi epi;
+    epi.p = p;
+    epi.com[0] = cx;
+    epi.com[1] = cy;
+    epi.com[2] = cz;
+#pragma unroll
+    for (int q = 0; q < kDiag; ++q) epi.acc[q] = 0.0;
+    const double* const src[3] = {field, nullptr, nullptr};
+    KSum es{0.0, 0.0}, unused{0.0, 0.0};
+    for (int t = blockIdx.x; t < mg.count(); t += gridDim.x) {
+        int xa, xe, y0, z0;
+        march_origin(mg, t, M::BY, xa, xe, y0, z0, p.X);
+        march_tile<Nuclear, M, double, 1, 16, DiagEpi, false, double, false>(sm, p, src, 0.0, 0.0, xa, xe, y0, z0,
+                                                                             epi, es, unused);
+    }
+    for (int q = 0; q < kDiag; ++q) {
+        const KSum b = block_ksum(KSum{epi.acc[q], 0.0}, shk);
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            parts[2 * kDiag * blockIdx.x + 2 * q] = b.s;
+            parts[2 * kDiag * blockIdx.x + 2 * q + 1] = b.c;
         }
     }
 }

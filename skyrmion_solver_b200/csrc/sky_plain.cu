@@ -489,6 +489,45 @@ int moments64(const Params& p, const double* f, double* scratch, double* out9, c
     return SKY_OK;
 }
 
+// Nuclear diagnostics (k_march_diag): at most kScratchDoubles / 56 blocks.
+int diag64(const Params& p, const double* f, const double* com, double* scratch, double* out28, cudaStream_t st) {
+    using M = MarchShape<4, 8, false>;
+    auto kern = k_march_diag<M>;
+    const size_t smem = M::template smem_bytes<double>(1);
+    static bool configured = false;
+    if (!configured) {
+        int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "cudaFuncSetAttribute(diagnostics)", __LINE__);
+        if (rc) return rc;
+        configured = true;
+    }
+    const int cap = kScratchDoubles / (2 * kDiag);
+    const MarchGrid g0 = march_grid<M>(p, p.X);
+    const MarchGrid mg = march_grid<M>(p, choose_xc(p.X, g0.nz * g0.ny, num_sms()));
+    const int blocks = mg.count() < cap ? mg.count() : cap;
+    kern<<<blocks, dim3(M::BZ, M::BY), smem, st>>>(p, mg, f, com[0], com[1], com[2], scratch);
+    int rc = check_cuda(cudaGetLastError(), "launch diagnostics", __LINE__);
+    if (rc) return rc;
+    double parts[2 * kDiag * (kScratchDoubles / (2 * kDiag))];
+    rc = check_cuda(cudaMemcpyAsync(parts, scratch, sizeof(double) * 2 * kDiag * blocks, cudaMemcpyDeviceToHost, st),
+                    "read diagnostics", __LINE__);
+    if (!rc) rc = check_cuda(cudaStreamSynchronize(st), "sync", __LINE__);
+    if (rc) return rc;
+    for (int q = 0; q < kDiag; ++q) {   // fixed-order compensated sum over the blocks
+        double sum = 0.0, comp = 0.0;
+        for (int b = 0; b < blocks; ++b) {
+            for (int k = 0; k < 2; ++k) {
+                const double v = parts[2 * kDiag * b + 2 * q + k];
+                const double t = sum + v;
+                comp += (fabs(sum) >= fabs(v)) ? ((sum - t) + v) : ((v - t) + sum);
+                sum = t;
+            }
+        }
+        out28[q] = sum + comp;
+    }
+    return SKY_OK;
+}
+
 int gradient_fp64(int theory, const Params& p, const double* f, double* eg, double* l, cudaStream_t st) {
     SKY_DISPATCH(theory, grad64, p, f, eg, l, st)
 }
@@ -729,6 +768,18 @@ int sky_baryon_moments(int theory, const int32_t* p_i, int32_t n_pi, const doubl
     if (!scratch || n_scratch < kScratchDoubles) return SKY_ERR_NOMEM;
     if ((int64_t)4 * n_sites(p) >= ((int64_t)1 << 31)) return invalid("lattice too large for the moments kernel");
     SKY_DISPATCH(theory, moments64, p, field, scratch, out9_host, SKY_STREAM(stream))
+}
+
+int sky_nuclear_diagnostics(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
+                            const double* field, const double* com_host, double* scratch, int64_t n_scratch,
+                            double* out28_host, void* stream) {
+    Params p;
+    int rc = pack_params(SKY_THEORY_NUCLEAR, p_i, n_pi, p_f, n_pf, &p);
+    if (rc) return rc;
+    if (!field || !com_host || !out28_host) return invalid("null buffer");
+    if (!scratch || n_scratch < kScratchDoubles) return SKY_ERR_NOMEM;
+    if ((int64_t)4 * n_sites(p) >= ((int64_t)1 << 31)) return invalid("lattice too large for the diagnostics kernel");
+    return diag64(p, field, com_host, scratch, out28_host, SKY_STREAM(stream));
 }
 
 int sky_arrested_newton_step(int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,
