@@ -133,6 +133,33 @@ class Simulation:
         g, b = self._launch()
         self.kernels.compute_rho_meson_kernel[g, b](self.en, self.Field, self.p_i_d)
 
+    def save_output(self, output_dir: str | None = None, precision: int = 32):
+        """Write the theory's output bundle in the reference's ``.dat`` format
+        (core/simulation.py:310-371): lattice metadata, the whole field, grid coordinates,
+        field components and the energy and baryon densities (computed on the device)."""
+        import inspect
+        import os
+        torch = _torch()
+        if output_dir is None:
+            output_dir = os.path.join(os.path.dirname(os.path.abspath(self.theory.io.__file__)), "results")
+        os.makedirs(output_dir, exist_ok=True)
+        self.compute_energy_density()
+        h_energy = self.en.detach().cpu().numpy().copy()
+        g, b = self._launch()
+        self.kernels.compute_skyrmion_number_kernel[g, b](self.entmp, self.Field, None, self.p_i_d, self.p_f_d)
+        torch.cuda.synchronize()
+        h_baryon = self.entmp.detach().cpu().numpy().copy()
+        if hasattr(self.kernels, "compute_potential_kernel"):
+            self.compute_potential_density()
+            torch.cuda.synchronize()
+        kwargs = dict(output_dir=output_dir, h_Field=self.Field.detach().cpu().numpy(), h_EnergyDensity=h_energy,
+                      h_BaryonDensity=h_baryon, h_OmegaDensity=self.en.detach().cpu().numpy(),
+                      h_grid=self.grid.detach().cpu().numpy(), xlen=int(self.p_i_h[0]), ylen=int(self.p_i_h[1]),
+                      zlen=int(self.p_i_h[2]), number_coordinates=int(self.p_i_h[4]),
+                      number_total_fields=int(self.p_i_h[5]), precision=precision)
+        accepted = set(inspect.signature(self.theory.io.output_data_bundle).parameters)
+        self.theory.io.output_data_bundle(**{k: v for k, v in kwargs.items() if k in accepted})
+
     def compute_center_of_mass(self) -> np.ndarray:
         """Baryon-density centre of mass (core/simulation.py:390-403)."""
         return self.observables_mod.compute_center_of_mass(self.Field, self.grid, None, None, None, self.entmp,
