@@ -147,6 +147,30 @@ int sky_init_field(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t 
                    const int32_t* baryon, const double* centers, const double* quats, double scale,
                    int32_t vacuum_shell, double* field, void* stream);
 
+/* Replace the viewer's volume builder (build_rgba_volume_kernel with the
+ * extrema of _reduce_density_extrema, th/nuclear_skyrme/render_gl.py:157-222,
+ * 447-500): volume[((z * Y + y) * X + x) * 4 + c] (FP32) holds the density
+ * normalised to its [min, max] (c = 0) and the unit pion vector (c = 1..3;
+ * (0, 0, 1) where |pi|^2 <= 1e-20).  `density` holds N FP64 values, `field`
+ * the reference-layout field (C >= 4).  `scratch` holds at least
+ * sky_volume_scratch_size() doubles.  If minmax_host is not NULL, the density
+ * minimum and maximum are written there and the stream is synchronised. */
+int64_t sky_volume_scratch_size(void);
+int sky_build_rgba_volume(const int32_t* p_i, int32_t n_pi, const double* density, const double* field,
+                          double* scratch, int64_t n_scratch, float* volume, double* minmax_host, void* stream);
+
+/* Replaces the viewer's ray-march fragment shader
+ * (visualization/gl_backend.py:519-710) without a graphics API: image[(row *
+ * width + col) * 4 + c] (FP32 RGBA, row 0 at the top) from the volume above
+ * (xlen * ylen * zlen texels, trilinear, clamp to edge).  params (host, 23
+ * floats): the three inverse-view rows (12), box scale (3), zoom, brightness,
+ * levelset, density min, density max, transfer scale, opacity scale, tstep.
+ * color_mode 0 uses the viewer's nine-entry transfer table; any other value
+ * the pion vector's HSL colour.  Rays that miss the box give (1, 1, 1, 1). */
+int sky_render_volume(const float* volume, int32_t xlen, int32_t ylen, int32_t zlen, const float* params,
+                      int32_t max_steps, int32_t color_mode, int32_t width, int32_t height, float* image,
+                      void* stream);
+
 /* Replace compute_sum / compute_max (core/utils.py:201-279, 321-373):
  * deterministic FP64 reductions (compensated sum; signed max).  `scratch` is a
  * device buffer of sky_reduce_scratch_size(n) doubles; the result is written to

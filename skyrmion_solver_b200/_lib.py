@@ -43,6 +43,7 @@ class SkyInvalidArgument(SkyError, ValueError):
 _P = ctypes.c_void_p
 _I32P = ctypes.POINTER(ctypes.c_int32)
 _F64P = ctypes.POINTER(ctypes.c_double)
+_F32P = ctypes.POINTER(ctypes.c_float)
 _I = ctypes.c_int
 _I32 = ctypes.c_int32
 _I64 = ctypes.c_int64
@@ -75,6 +76,9 @@ SIGNATURES = {
     "sky_baryon_moments": ([_I, _I32P, _I32, _F64P, _I32, _P, _P, _I64, _F64P, _P], _I),
     "sky_nuclear_diagnostics": ([_I32P, _I32, _F64P, _I32, _P, _F64P, _P, _I64, _F64P, _P], _I),
     "sky_init_field": ([_I32P, _I32, _F64P, _I32, _I32, _I32P, _F64P, _F64P, _D, _I32, _P, _P], _I),
+    "sky_volume_scratch_size": ([], _I64),
+    "sky_build_rgba_volume": ([_I32P, _I32, _P, _P, _P, _I64, _P, _F64P, _P], _I),
+    "sky_render_volume": ([_P, _I32, _I32, _I32, _F32P, _I32, _I32, _I32, _I32, _P, _P], _I),
     "sky_engine_create": ([_I, ctypes.POINTER(ctypes.c_void_p)], _I),
     "sky_engine_destroy": ([_P], _I),
     "sky_engine_add": ([_P, _I, _I32P, _I32, _F64P, _I32, _I, _P, _P, _I, ctypes.POINTER(_I)], _I),
@@ -202,6 +206,10 @@ def i32p(a):
 
 def f64p(a):
     return a.ctypes.data_as(_F64P)
+
+
+def f32p(a):
+    return a.ctypes.data_as(_F32P)
 
 
 def stream_ptr(stream=None):

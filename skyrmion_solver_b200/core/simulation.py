@@ -210,8 +210,9 @@ class Simulation:
             self.observables_mod.compute_energy, self.gradient_step_kernel, self.rk4_kernel,
             compute_norm=compute_norm, do_norm_kernel=do_norm_kernel)
 
-    def save_output(self, output_dir: str | None = None, precision: int = 32):
-        """Snapshot of the state (field, velocity, densities, parameters) as ``state.npz``."""
+    def save_state(self, output_dir: str | None = None):
+        """Snapshot of the state (field, velocity, densities, parameters) as ``state.npz``; the
+        reference-format text bundle is ``save_output``."""
         out = Path(output_dir or "results")
         out.mkdir(parents=True, exist_ok=True)
         C = int(self.p_i_h[5])

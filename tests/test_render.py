@@ -1,0 +1,264 @@
+"""Headless viewer: the RGBA volume builder and the ray-march.
+
+* The volume oracle against the reference's own kernels (tests/golden/volume.npz,
+  made by make_golden_volume.py under Numba's CUDA simulator), and the device
+  builder against both.
+* The ray-march oracle against cases derived by hand from the shader, and the
+  device ray-march against the oracle on the same volume.  The shader runs only
+  through OpenGL, so the image itself is not pinned to the reference.
+
+Image tolerance: the device and the oracle both compute in FP32 but round
+differently (the device contracts multiply-adds), and the shader has hard
+thresholds (box-edge test, alpha > 0.95, t > tfar), so a pixel whose ray
+passes a threshold within rounding may take the other branch.  At most 1% of
+the pixels may differ by more than 1e-3 in any channel, and the median pixel
+difference must stay below 1e-5.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle import render_oracle as R
+from skyrmion_solver_b200 import _lib
+from skyrmion_solver_b200.visualization import HeadlessRenderer, inv_view_rows
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+VOLUME = os.path.join(HERE, "golden", "volume.npz")
+
+
+def _gold():
+    if not os.path.exists(VOLUME):
+        pytest.skip("volume.npz not generated")
+    return dict(np.load(VOLUME))
+
+
+def _uniform(value, n=(1.0, 0.0, 0.0), dims=(6, 5, 4)):
+    X, Y, Z = dims
+    vol = np.empty((Z, Y, X, 4), np.float32)
+    vol[..., 0] = value
+    vol[..., 1:] = np.asarray(n, np.float32)
+    return vol
+
+
+# ---------------------------------------------------------------------------
+# CPU: the oracle and the host logic
+# ---------------------------------------------------------------------------
+def test_volume_oracle_matches_the_reference_kernels():
+    d = _gold()
+    X, Y, Z = (int(v) for v in d["p_i"][:3])
+    vol, vmin, vmax = R.rgba_volume(d["density"], np.load(os.path.join(HERE, "golden", "nuclear.npz"))["field0"],
+                                    (X, Y, Z))
+    assert vmin == d["dmin"] and vmax == d["dmax"]
+    assert vol.dtype == np.float32 and vol.shape == d["volume"].shape == (Z, Y, X, 4)
+    assert np.array_equal(vol, d["volume"])
+
+
+def test_view_rows_match_the_oracle():
+    for rot, tr in [((0, 0, 0), (0, 0, -4)), ((30, -45, 10), (0.3, -0.2, -3.5)), ((-90, 180, 0), (1, 2, 3))]:
+        assert np.array_equal(inv_view_rows(rot, tr), R.inv_view_rows(rot, tr))
+    rows = inv_view_rows()
+    assert np.array_equal(rows[:, 3], [0.0, 0.0, 4.0])   # default eye at z = 4 looking down -z
+
+
+def test_shader_params_layout_and_defaults():
+    r = HeadlessRenderer(40, 30, 8)
+
+    class _Sim:
+        p_i_h = np.array([8, 6, 4], np.int32)
+        p_f_h = np.array([2.0, 1.0, 0.5], np.float64)
+    r._sim = _Sim()
+    r._sync_box_scale()
+    prm = r.shader_params()
+    assert prm.dtype == np.float32 and prm.shape == (23,)
+    assert np.array_equal(prm[:12], inv_view_rows().ravel())
+    assert np.array_equal(prm[12:15], np.array([1.0, 0.5, 0.25], np.float32))
+    assert np.allclose(prm[15:], [5.5, 6.0, 0.2, 0.0, 1.0, 4.0, 1.0, 0.002])
+    assert r.color_mode == 0 and r.max_steps == 2500
+    r.set_display_mode(2)
+    assert r.color_mode == 1
+    r.set_display_mode(99)                               # unknown modes are ignored
+    assert r.color_mode == 1
+
+
+def test_oracle_hand_cases():
+    W, H = 33, 25                      # odd sizes: the centre pixel's ray is the view axis
+    c = (H // 2, W // 2)
+    rows = inv_view_rows()
+    # norm 0.5 lands on transfer texel 4 exactly: opaque green, alpha 1 on the first sample
+    img = R.render(_uniform(0.5), rows, width=W, height=H, color_mode=0)
+    assert np.array_equal(img[c], [0.0, 1.0, 0.0, 1.0])
+    # pion vector (1, 0, 0) has hue 0: red; input (0.45 - 0.2) * 4 = 1
+    img = R.render(_uniform(0.45), rows, width=W, height=H, color_mode=1)
+    assert np.allclose(img[c], [1.0, 0.0, 0.0, 1.0], atol=1e-6)
+    # a camera well to the side misses the box: every pixel keeps the white clear colour
+    img = R.render(_uniform(0.5), inv_view_rows((0, 0, 0), (5, 0, -4)), width=W, height=H)
+    assert np.array_equal(img, np.ones_like(img))
+    # constant per-sample opacity a and white colour (n = (0, 0, 1)): after n samples
+    # alpha = 1 - (1 - a)^n and rgb = a * alpha; the axis ray crosses the box (t = 3..5) in ~1001 samples
+    a = 1e-4
+    img = R.render(_uniform(0.5, (0.0, 0.0, 1.0)), rows, width=W, height=H, color_mode=1, brightness=1.0,
+                   levelset=0.0, transfer_scale=2 * a)
+    alpha = img[c][3]
+    n = np.log(1.0 - alpha) / np.log(1.0 - a)
+    assert abs(n - 1001) < 1.5
+    assert np.allclose(img[c][:3], a * alpha, rtol=1e-3)
+
+
+def test_volume_and_render_reject_bad_arguments():
+    lib = _lib.load()
+    pi = np.array([8, 8, 8, 2, 3, 4, 512, 2048, 1, 1, 1], dtype=np.int32)
+    dummy = ctypes.c_void_p(256)
+    mm = np.zeros(2)
+    n = lib.sky_volume_scratch_size()
+    assert n > 0
+    assert lib.sky_build_rgba_volume(_lib.i32p(pi), 11, None, dummy, dummy, n, dummy, _lib.f64p(mm), None) == 1
+    assert lib.sky_build_rgba_volume(_lib.i32p(pi), 11, dummy, dummy, dummy, n, ctypes.c_void_p(260),
+                                     _lib.f64p(mm), None) == 1            # volume not 16-byte aligned
+    assert lib.sky_build_rgba_volume(_lib.i32p(pi), 11, dummy, dummy, dummy, n - 1, dummy, _lib.f64p(mm), None) == 5
+    prm = np.zeros(23, np.float32)
+    prm[12:15] = 1.0
+    prm[22] = 0.002
+    args = (dummy, 8, 8, 8, _lib.f32p(prm))
+    assert lib.sky_render_volume(*args, 100, 0, 0, 10, dummy, None) == 1    # empty image
+    assert lib.sky_render_volume(*args, -1, 0, 10, 10, dummy, None) == 1    # negative step count
+    assert lib.sky_render_volume(*args, 100, 0, 10, 10, None, None) == 1    # null image
+    bad = prm.copy()
+    bad[22] = 0.0
+    assert lib.sky_render_volume(dummy, 8, 8, 8, _lib.f32p(bad), 100, 0, 10, 10, dummy, None) == 1
+    bad = prm.copy()
+    bad[13] = 0.0
+    assert lib.sky_render_volume(dummy, 8, 8, 8, _lib.f32p(bad), 100, 0, 10, 10, dummy, None) == 1
+
+
+# ---------------------------------------------------------------------------
+# GPU: the device path through the C ABI
+# ---------------------------------------------------------------------------
+def _image_close(got, want):
+    diff = np.abs(got - want).max(axis=-1)
+    return float((diff > 1e-3).mean()) <= 0.01 and float(np.median(diff)) <= 1e-5
+
+
+def _draw(vol, rows, box=(1.0, 1.0, 1.0), zoom=5.5, brightness=6.0, levelset=0.2, dmin=0.0, dmax=1.0,
+          transfer_scale=4.0, opacity_scale=1.0, tstep=0.002, max_steps=2500, color_mode=0, width=64, height=48):
+    import torch
+    Z, Y, X = vol.shape[:3]
+    v = torch.from_numpy(np.ascontiguousarray(vol)).cuda()
+    img = torch.empty((height, width, 4), dtype=torch.float32, device="cuda")
+    prm = np.concatenate([np.asarray(rows, np.float32).ravel(), np.asarray(box, np.float32),
+                          np.asarray([zoom, brightness, levelset, dmin, dmax, transfer_scale, opacity_scale, tstep],
+                                     np.float32)]).astype(np.float32)
+    _lib.call("sky_render_volume", _lib.dptr(v, "float32"), X, Y, Z, _lib.f32p(prm), max_steps, color_mode, width,
+              height, _lib.dptr(img, "float32"), _lib.stream_ptr())
+    torch.cuda.synchronize()
+    return img.cpu().numpy()
+
+
+@pytest.mark.gpu
+def test_device_volume_matches_the_reference_kernels():
+    import torch
+    from tests._gpu import dev
+    d = _gold()
+    X, Y, Z = (int(v) for v in d["p_i"][:3])
+    field = np.load(os.path.join(HERE, "golden", "nuclear.npz"))["field0"]
+    vol = torch.empty((Z, Y, X, 4), dtype=torch.float32, device="cuda")
+    scratch = torch.empty(int(_lib.load().sky_volume_scratch_size()), dtype=torch.float64, device="cuda")
+    mm = np.zeros(2)
+    p_i = np.ascontiguousarray(d["p_i"], np.int32)
+    dens_d, field_d = dev(d["density"]), dev(field)       # held: the call reads them on the device
+    _lib.call("sky_build_rgba_volume", _lib.i32p(p_i), len(p_i), _lib.dptr(dens_d), _lib.dptr(field_d),
+              _lib.dptr(scratch), scratch.numel(), _lib.dptr(vol, "float32"), _lib.f64p(mm), _lib.stream_ptr())
+    assert mm[0] == d["dmin"] and mm[1] == d["dmax"]
+    assert np.array_equal(vol.cpu().numpy(), d["volume"])
+
+
+@pytest.mark.gpu
+def test_device_volume_at_a_larger_lattice_matches_the_oracle():
+    """Ragged tile edges (X, Z not multiples of 32) and more than one extrema block."""
+    import torch
+    from tests._gpu import dev
+    X, Y, Z = 45, 38, 70
+    rng = np.random.default_rng(5)
+    dens = rng.standard_normal(X * Y * Z) * 3.0
+    field = rng.standard_normal((4, X * Y * Z))
+    field[1:, :50] = 0.0                                  # pion vector below the threshold: (0, 0, 1)
+    pi = np.array([X, Y, Z, 2, 3, 4, X * Y * Z, 4 * X * Y * Z, 1, 1, 1], np.int32)
+    vol = torch.empty((Z, Y, X, 4), dtype=torch.float32, device="cuda")
+    scratch = torch.empty(int(_lib.load().sky_volume_scratch_size()), dtype=torch.float64, device="cuda")
+    mm = np.zeros(2)
+    dens_d, field_d = dev(dens), dev(field)
+    _lib.call("sky_build_rgba_volume", _lib.i32p(pi), len(pi), _lib.dptr(dens_d), _lib.dptr(field_d),
+              _lib.dptr(scratch), scratch.numel(), _lib.dptr(vol, "float32"), _lib.f64p(mm), _lib.stream_ptr())
+    want, vmin, vmax = R.rgba_volume(dens, field, (X, Y, Z))
+    assert mm[0] == vmin and mm[1] == vmax
+    assert np.array_equal(vol.cpu().numpy(), want)
+
+
+@pytest.mark.gpu
+def test_device_render_hand_cases():
+    W, H = 33, 25
+    c = (H // 2, W // 2)
+    rows = inv_view_rows()
+    assert np.array_equal(_draw(_uniform(0.5), rows, width=W, height=H)[c], [0.0, 1.0, 0.0, 1.0])
+    img = _draw(_uniform(0.5), inv_view_rows((0, 0, 0), (5, 0, -4)), width=W, height=H)
+    assert np.array_equal(img, np.ones_like(img))
+    a = 1e-4
+    img = _draw(_uniform(0.5, (0.0, 0.0, 1.0)), rows, width=W, height=H, color_mode=1, brightness=1.0,
+                levelset=0.0, transfer_scale=2 * a)
+    n = np.log(1.0 - img[c][3]) / np.log(1.0 - a)
+    assert abs(n - 1001) < 1.5
+    assert np.allclose(img[c][:3], a * img[c][3], rtol=1e-3)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("color_mode", [0, 1])
+@pytest.mark.parametrize("pose", [((0, 0, 0), (0, 0, -4), 5.5), ((25, -40, 0), (0.2, -0.1, -3.6), 4.0)])
+def test_device_render_matches_the_oracle(color_mode, pose):
+    from skyrmion_solver_b200 import initial as ini
+    rot, tr, zoom = pose
+    # a B = 2 rational map on an anisotropic box, with a smooth density concentrated on it
+    dims = (40, 34, 28)
+    h = (0.12, 0.14, 0.16)
+    F = ini.normalise(ini.rational_map(dims, h, 2, ini.exp_profile(1.2), (0.0, 0.0, 0.0)))
+    r2 = sum(((np.arange(n) - (n - 1) / 2.0) * s)[tuple(slice(None) if k == j else None for k in range(3))] ** 2
+             for j, (n, s) in enumerate(zip(dims, h)))
+    dens = np.exp(-r2 / 0.6) * (1.0 - F[0])
+    vol, _, _ = R.rgba_volume(dens.ravel(), F.reshape(4, -1), dims)
+    size = np.array([(n - 1) * s for n, s in zip(dims, h)])
+    box = (size / size.max()).astype(np.float32)
+    rows = inv_view_rows(rot, tr)
+    kw = dict(box=box, zoom=zoom, color_mode=color_mode, width=64, height=48)
+    got = _draw(vol, rows, **kw)
+    want = R.render(vol, rows, **kw)
+    assert (want != 1.0).any() and (want == 1.0).all(axis=-1).mean() < 0.9   # the soliton is in view
+    assert _image_close(got, want)
+
+
+@pytest.mark.gpu
+def test_headless_renderer_frame_and_screenshot(tmp_path):
+    import torch
+    from skyrmion_solver_b200 import theories as T
+    from skyrmion_solver_b200.core.simulation import Simulation
+    th = T.load_theory("Nuclear Skyrme model")
+    params = th.params.default_params(xlen=32, ylen=32, zlen=32, lsx=0.2, lsy=0.2, lsz=0.2, time_step=0.04)
+    sim = Simulation(params, th)
+    sim.initialize({"mode": "rational_map", "baryon_number": 2})
+    sim.compute_baryon_density()
+    r = HeadlessRenderer(48, 36, 32)
+    r.bind_sim(sim)
+    img = r.render(density_flat=sim.en, field_flat=sim.Field)
+    torch.cuda.synchronize()
+    vol, vmin, vmax = R.rgba_volume(sim.en.cpu().numpy(), sim.Field.cpu().numpy(), (32, 32, 32))
+    assert r.extrema == (vmin, vmax)
+    assert np.array_equal(r.volume.cpu().numpy(), vol)
+    want = R.render(vol, inv_view_rows(), box=r.box_scale, width=48, height=36)
+    assert _image_close(img.cpu().numpy(), want)
+    r.set_display_mode(2)
+    img2 = r.draw().cpu().numpy()
+    assert _image_close(img2, R.render(vol, inv_view_rows(), box=r.box_scale, color_mode=1, width=48, height=36))
+    path = r.save_screenshot(str(tmp_path))
+    from PIL import Image
+    px = np.asarray(Image.open(path))
+    assert px.shape == (36, 48, 3) and px.dtype == np.uint8
+    assert np.array_equal(px, r.read_pixels())
