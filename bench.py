@@ -627,7 +627,7 @@ def serve_requests(n, rate, seed, mix, bmax, max_side, tol, max_steps):
         p_i, p_f = th.params.pack_device_params(prm.resolved())
         p_i = np.asarray(p_i, np.int32)
         p_f = np.asarray(p_f, np.float64)
-        cfg = {"mode": "smorgasbord", "count": B, "seed": seed * 1000 + k, "scale": 1.5, "vacuum_shell": 2}
+        cfg = {"mode": "cloud", "count": B, "seed": seed * 1000 + k, "scale": 1.5, "vacuum_shell": 2}
         # the field is built on the device when the request is admitted (sky_init_field)
         reqs.append((Request(k, name, p_i, p_f, None, float(arrivals[k]), tol, max_steps, init=cfg), prm, th))
     return reqs
@@ -742,7 +742,7 @@ def run_batch(args):
                                        **SERVE_THEORIES[name])
         p_i, p_f = th.params.pack_device_params(prm.resolved())
         p_i, p_f = np.asarray(p_i, np.int32), np.asarray(p_f, np.float64)
-        f = build_host_field(name, p_i, p_f, {"mode": "smorgasbord", "count": B, "seed": 100 + k, "scale": 1.5,
+        f = build_host_field(name, p_i, p_f, {"mode": "cloud", "count": B, "seed": 100 + k, "scale": 1.5,
                                                 "vacuum_shell": 2})
         eng.add(name, (p_i, p_f), f, None, precision=FAST)
         sites[name] += side ** 3

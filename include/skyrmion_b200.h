@@ -147,6 +147,26 @@ int sky_init_field(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t 
                    const int32_t* baryon, const double* centers, const double* quats, double scale,
                    int32_t vacuum_shell, double* field, void* stream);
 
+/* Replaces the reference's initial configurations (th/<theory>/initial_config.py:
+ * create_ground_state_kernel, create_initial_configuration_kernel, and the
+ * smorgasbord's create_rational_map_skyrmion_kernel + product_ansatz_kernel).
+ * Field components 0..3 become the product, in list order, of n_lumps lumps,
+ * each normalised and each product normalised; components 4.. become 0.  With
+ * from_vacuum != 0 the product starts from (1, 0, 0, 0) and composes every lump
+ * (the smorgasbord); otherwise it starts from the first lump itself (the single
+ * ansatz).  n_lumps = 0 gives the vacuum.  Each lump is 16 doubles:
+ *   [0] kind: 0 Gaussian hedgehog pi exp(-(r / r0)^2) (hedgehog_field),
+ *             1 rational map with the fitted profile (profilefun, rational_map_value)
+ *   [1] baryon number (the map's R_B and profile, rounded, >= 1)
+ *   [2..4] centre in grid coordinates (x_i = h i)
+ *   [5..7] Euler angles z, y, z applied to the position (maps only)
+ *   [8..10] Euler angles applied to the target direction (hedgehog: [10] about z)
+ *   [11] profile length r0 > 0 (maps: the profile is evaluated at r / r0)
+ *   [12] profile mass mixing m0 (maps; below 1 blends the massless fit)
+ *   [13..15] unused (0). */
+int sky_init_lumps(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf, int32_t n_lumps,
+                   const double* lumps, int32_t from_vacuum, double* field, void* stream);
+
 /* Replace the viewer's volume builder (build_rgba_volume_kernel with the
  * extrema of _reduce_density_extrema, th/nuclear_skyrme/render_gl.py:157-222,
  * 447-500): volume[((z * Y + y) * X + x) * 4 + c] (FP32) holds the density

@@ -76,6 +76,7 @@ SIGNATURES = {
     "sky_baryon_moments": ([_I, _I32P, _I32, _F64P, _I32, _P, _P, _I64, _F64P, _P], _I),
     "sky_nuclear_diagnostics": ([_I32P, _I32, _F64P, _I32, _P, _F64P, _P, _I64, _F64P, _P], _I),
     "sky_init_field": ([_I32P, _I32, _F64P, _I32, _I32, _I32P, _F64P, _F64P, _D, _I32, _P, _P], _I),
+    "sky_init_lumps": ([_I32P, _I32, _F64P, _I32, _I32, _F64P, _I32, _P, _P], _I),
     "sky_volume_scratch_size": ([], _I64),
     "sky_build_rgba_volume": ([_I32P, _I32, _P, _P, _P, _I64, _P, _F64P, _P], _I),
     "sky_render_volume": ([_P, _I32, _I32, _I32, _F32P, _I32, _I32, _I32, _I32, _P, _P], _I),

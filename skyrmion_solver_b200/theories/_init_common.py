@@ -1,20 +1,35 @@
 """Shared ``initialize`` implementation for the theory packages.
 
-Builds the initial Skyrme field in FP64: on the device by ``sky_init_field``
-(``build_device_field``), or on the host (``skyrmion_solver_b200.initial``,
-``build_host_field``) for configurations with noise or an explicit field, and
-writes it into the simulation's ``Field`` buffer.  Supported ``config`` keys:
+Two families of initial fields are built, both in FP64 in the reference layout.
 
-* ``mode``: ``"ground"`` (vacuum), ``"hedgehog"``, ``"rational_map"``,
-  ``"product"`` (explicit ``positions`` / ``orientations``), ``"smorgasbord"``
-  (``count`` seeded hedgehogs at random positions with Haar orientations) or
-  ``"field"`` (an explicit ``field`` array, optional ``velocity``);
-* ``scale`` (profile f(r) = pi exp(-r/scale), default 1.5), ``baryon_number``,
-  ``center``, ``seed``, ``min_separation``;
-* ``noise`` (uniform amplitude added before renormalising, seeded),
-  ``vacuum_shell`` (width of the boundary shell set to the vacuum);
-* omega theory: ``omega_seed`` (default True) sets omega = -c_omega B0, as the
-  reference's create_omega_field_kernel (th/omega_skyrme/initial_config.py:1496-1533).
+The reference's own configurations (th/<theory>/initial_config.py ``initialize``),
+built on the device by ``sky_init_lumps``; this is what a configuration without
+the keys below selects, exactly as the reference reads it:
+
+* ``mode``: ``"ground"`` / ``"uniform"`` / ``"vacuum"`` / ``"gs"`` (vacuum),
+  ``"smorgasbord"`` / ``"smorgaasbord"`` / ``"smorg"`` (seeded rational-map lumps
+  composed by quaternion products; keys ``seed``, ``count``, ``lump_baryon``,
+  ``profile_m0``, ``profile_m1``, ``position_scale``), ``"rational_map"``, or
+  anything else (default ``"initial"``): the ansatz of the ``ansatz`` key or of
+  the parameters' flags, a Gaussian hedgehog, a fitted-profile rational map or the
+  vacuum;
+* ``baryon_number``, ``isospin_rotation`` (default: the packed parameters);
+* omega: the omega field is seeded as -c_omega B0 (create_omega_field_kernel,
+  th/omega_skyrme/initial_config.py:1496-1533) except in the vacuum.
+
+Synthetic workload fields (``build_device_field`` through ``sky_init_field``, or
+``build_host_field`` in NumPy where noise or an explicit field is asked for):
+selected by ``mode`` ``"product"``, ``"field"`` or ``"cloud"``, or by any of the
+keys ``scale`` (profile f(r) = pi exp(-r/scale), default 1.5), ``center``,
+``noise`` (seeded uniform amplitude added before renormalising),
+``vacuum_shell`` (width of the boundary shell set to the vacuum), ``positions``,
+``orientations``, ``min_separation``.  Modes there: ``"ground"``,
+``"hedgehog"``, ``"rational_map"`` (B = 1, 2, 4), ``"product"`` (explicit
+positions / orientations), ``"cloud"`` (``count`` seeded hedgehogs at random
+positions with Haar orientations; ``"smorgasbord"`` with one of the keys above
+means the same), ``"field"`` (explicit ``field``, optional ``velocity``).
+Omega's field is seeded likewise unless ``omega_seed`` is False or the field is
+explicit.
 """
 from __future__ import annotations
 
@@ -43,7 +58,7 @@ def build_host_field(short, p_i, p_f, config):
     elif mode == "product":
         phi = ini.product_ansatz(dims, h, config["positions"], config.get("orientations",
                                  [None] * len(config["positions"])), prof)
-    elif mode == "smorgasbord":
+    elif mode in ("cloud", "smorgasbord"):
         B = int(config.get("count", config.get("baryon_number", 1)))
         box = (X * h[0], Y * h[1], Z * h[2])
         pos = ini.seeded_positions(rng, B, box, float(config.get("min_separation", 2.0)))
@@ -83,7 +98,7 @@ def _soliton_list(X, Y, Z, h, config, rng):
         pos = list(config["positions"])
         qs = list(config.get("orientations", [None] * len(pos)))
         return [1] * len(pos), pos, qs
-    if mode == "smorgasbord":
+    if mode in ("cloud", "smorgasbord"):
         B = int(config.get("count", config.get("baryon_number", 1)))
         box = (X * h[0], Y * h[1], Z * h[2])
         pos = ini.seeded_positions(rng, B, box, float(config.get("min_separation", 2.0)))
@@ -119,6 +134,115 @@ def build_device_field(short, p_i, p_f, config, device=0, stream=None):
     return out
 
 
+GROUND_MODES = ("ground", "uniform", "vacuum", "gs")
+SMORGASBORD_MODES = ("smorgasbord", "smorgaasbord", "smorg")
+RATIONAL_MODES = ("rational_map", "rational map", "rational-map")
+SYNTHETIC_MODES = ("product", "field", "cloud")
+SYNTHETIC_KEYS = ("scale", "center", "noise", "vacuum_shell", "positions", "orientations", "min_separation")
+LUMP_STRIDE = 16
+
+
+def is_reference_config(config) -> bool:
+    """True when the configuration asks for one of the reference's own initial fields."""
+    cfg = config or {}
+    mode = str(cfg.get("mode", "initial")).lower().strip()
+    return mode not in SYNTHETIC_MODES and not any(k in cfg for k in SYNTHETIC_KEYS)
+
+
+def _ansatz_slots(short):
+    """(p_i index of the hedgehog flag, p_f index of the baryon number) of a theory's packing."""
+    if short in ("omega", "coulomb"):
+        return 12, 10
+    if short == "rho":
+        return 11, 11
+    return 11, 10
+
+
+def _profile_lengths(short, B, p_f):
+    """(hedgehog r0, map radius divisor) of th/<theory>/initial_config.py: omega uses
+    0.15 min(size) for both, Coulomb 0.4 min(size) / max(|B|, 1) for both; the others
+    max(size) / (8 max(|B|, 1)) in the hedgehog and the unscaled radius in the map."""
+    size = [float(p_f[0]), float(p_f[1]), float(p_f[2])]
+    if short == "omega":
+        s = max(0.15 * min(size) / 1.0, 1.0e-6)
+        return s, s
+    if short == "coulomb":
+        s = max(0.4 * min(size) / max(abs(B), 1.0), 1.0e-6)
+        return s, s
+    return max(max(size) / (8.0 * max(abs(B), 1.0)), 1.0e-6), 1.0
+
+
+def reference_lumps(short, p_i, p_f, config=None):
+    """The lump list (n, 16) and the from-vacuum flag of the reference's initialize for this
+    configuration (th/nuclear_skyrme/initial_config.py:1267-1560 and the theory's variant)."""
+    cfg = dict(config or {})
+    p_i = np.asarray(p_i)
+    p_f = np.asarray(p_f, np.float64)
+    X, Y, Z = (int(v) for v in p_i[:3])
+    h = (float(p_f[3]), float(p_f[4]), float(p_f[5]))
+    centre = [0.5 * (0.0 + h[d] * float(n - 1)) for d, n in enumerate((X, Y, Z))]   # _physical_box_center
+    mode = str(cfg.get("mode", "initial")).lower().strip()
+    if mode in GROUND_MODES:
+        return np.zeros((0, LUMP_STRIDE)), True
+    iflag, ib = _ansatz_slots(short)
+    if mode in SMORGASBORD_MODES:
+        rng = np.random.default_rng(int(cfg.get("seed", 0)))
+        size = [float(p_f[0]), float(p_f[1]), float(p_f[2])]
+        count = int(cfg.get("count", max(1, int(round(abs(float(cfg.get("baryon_number", p_f[10]))))))))
+        lump_b = int(cfg.get("lump_baryon", 1))
+        m0 = float(cfg.get("profile_m0", 1.0))
+        scale = float(cfg.get("position_scale", 0.18))
+        half = [scale * v for v in size]
+        pos = rng.uniform(low=[-half[0], -half[1], -half[2]], high=half, size=(count, 3))
+        pos -= pos.mean(axis=0, keepdims=True)
+        alpha = rng.uniform(0.0, 2.0 * np.pi, size=(count, 3))
+        beta = rng.uniform(0.0, 2.0 * np.pi, size=(count, 3))
+        _, r_map = _profile_lengths(short, float(lump_b), p_f)
+        lumps = np.zeros((count, LUMP_STRIDE))
+        for n in range(count):
+            lumps[n, 0] = 1.0
+            lumps[n, 1] = float(lump_b)
+            lumps[n, 2:5] = [float(centre[d] + pos[n, d]) for d in range(3)]
+            lumps[n, 5:8] = alpha[n]
+            lumps[n, 8:11] = beta[n]
+            lumps[n, 11] = r_map
+            lumps[n, 12] = m0
+        return lumps, True
+    ans = "hedgehog"
+    if int(p_i[iflag + 1]) != 0:
+        ans = "rational_map"
+    elif int(p_i[iflag + 2]) != 0:
+        ans = "uniform"
+    ans = "rational_map" if mode in RATIONAL_MODES else str(cfg.get("ansatz", ans)).lower().strip()
+    B = float(cfg.get("baryon_number", p_f[ib]))
+    iso = float(cfg.get("isospin_rotation", p_f[ib + 1]))
+    r_hh, r_map = _profile_lengths(short, B, p_f)
+    lump = np.zeros((1, LUMP_STRIDE))
+    lump[0, 1] = B
+    lump[0, 2:5] = centre
+    lump[0, 10] = iso
+    if ans in RATIONAL_MODES:
+        lump[0, 0], lump[0, 11], lump[0, 12] = 1.0, r_map, 1.0
+    elif ans == "hedgehog":
+        lump[0, 0], lump[0, 11] = 0.0, r_hh
+    else:
+        return np.zeros((0, LUMP_STRIDE)), True
+    return lump, False
+
+
+def build_reference_field(short, p_i, p_f, config, out, stream=None):
+    """Write the reference's initial field for `config` into `out` (FP64 CUDA tensor of C*N
+    values) with sky_init_lumps; omega's field component is left at 0."""
+    from .. import _lib
+    p_i = np.ascontiguousarray(p_i, np.int32)
+    p_f = np.ascontiguousarray(p_f, np.float64)
+    lumps, from_vacuum = reference_lumps(short, p_i, p_f, config)
+    lumps = np.ascontiguousarray(lumps, np.float64)
+    _lib.call("sky_init_lumps", _lib.i32p(p_i), len(p_i), _lib.f64p(p_f), len(p_f), len(lumps), _lib.f64p(lumps),
+              1 if from_vacuum else 0, _lib.dptr(out), _lib.stream_ptr(stream))
+    return out
+
+
 def make_initialize(short):
     def initialize(*, Velocity, Field, grid=None, p_i_d=None, p_f_d=None, p_i_h=None, p_f_h=None, config=None,
                    **_unused):
@@ -126,16 +250,29 @@ def make_initialize(short):
         cfg = config or {}
         p_i = np.asarray(p_i_h if p_i_h is not None else p_i_d.host)
         p_f = np.asarray(p_f_h if p_f_h is not None else p_f_d.host)
-        if Field.is_cuda and not float(cfg.get("noise", 0.0)) and str(cfg.get("mode", "ground")).lower() != "field":
-            # built in place on the device (sky_init_field); noise and explicit fields come from the host
-            Field.copy_(build_device_field(short, p_i, p_f, cfg, Field.device.index or 0))
+        mode = str(cfg.get("mode", "initial")).lower().strip()
+        if is_reference_config(cfg):
+            if not Field.is_cuda:
+                raise RuntimeError("the reference's initial configurations are built on a CUDA device")
+            build_reference_field(short, p_i, p_f, cfg, Field)
+            Velocity.zero_()
+            for name in ("k1", "k2", "k3", "k4", "l1", "l2", "l3", "l4", "Temp"):   # zeroed as the reference's kernels do
+                buf = _unused.get(name)
+                if buf is not None and hasattr(buf, "zero_"):
+                    buf.zero_()
+            seed = short == "omega" and mode not in GROUND_MODES
         else:
-            f = build_host_field(short, p_i, p_f, cfg)
-            Field.copy_(torch.from_numpy(f.ravel()).to(Field.device))
+            if Field.is_cuda and not float(cfg.get("noise", 0.0)) and mode != "field":
+                # built in place on the device (sky_init_field); noise and explicit fields come from the host
+                Field.copy_(build_device_field(short, p_i, p_f, cfg, Field.device.index or 0))
+            else:
+                f = build_host_field(short, p_i, p_f, cfg)
+                Field.copy_(torch.from_numpy(f.ravel()).to(Field.device))
+            seed = short == "omega" and cfg.get("omega_seed", True) and mode != "field"
         if "velocity" in cfg:
             v = np.asarray(cfg["velocity"], dtype=np.float64).ravel()
             Velocity.copy_(torch.from_numpy(v).to(Velocity.device))
-        if short == "omega" and cfg.get("omega_seed", True) and cfg.get("mode", "ground") != "field":
+        if seed:
             seed_omega(Field, p_i, p_f)
     return initialize
 

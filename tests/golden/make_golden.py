@@ -124,7 +124,7 @@ DIMS = (12, 11, 10)
 SPACING = (0.2, 0.18, 0.22)
 
 
-def theory_params(short, mod):
+def theory_params(short, mod, **overrides):
     common = dict(xlen=DIMS[0], ylen=DIMS[1], zlen=DIMS[2],
                   lsx=SPACING[0], lsy=SPACING[1], lsz=SPACING[2],
                   xsize=SPACING[0] * (DIMS[0] - 1), ysize=SPACING[1] * (DIMS[1] - 1),
@@ -139,6 +139,7 @@ def theory_params(short, mod):
         "lightly_bound": dict(mpi=0.7, alpha=0.3),
     }[short]
     common.update(extra)
+    common.update(overrides)
     return mod.params.default_params(**common)
 
 

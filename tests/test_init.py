@@ -17,7 +17,7 @@ CONFIGS = [
     {"mode": "rational_map", "baryon_number": 4, "scale": 2.0, "vacuum_shell": 2},
     {"mode": "product", "positions": [(-1.0, 0.0, 0.2), (1.1, 0.3, -0.4)],
      "orientations": [None, (0.5, 0.5, 0.5, 0.5)]},
-    {"mode": "smorgasbord", "count": 3, "seed": 7, "vacuum_shell": 2},
+    {"mode": "cloud", "count": 3, "seed": 7, "vacuum_shell": 2},
 ]
 
 
@@ -47,7 +47,8 @@ def test_initialize_builds_on_the_device_and_keeps_the_host_path_for_noise():
     from skyrmion_solver_b200.theories._init_common import build_host_field
     th = T.by_short_name("nuclear")
     p = th.params.default_params(xlen=20, ylen=20, zlen=20, lsx=0.2, lsy=0.2, lsz=0.2)
-    for cfg in ({"mode": "rational_map", "baryon_number": 2}, {"mode": "hedgehog", "noise": 1e-3, "seed": 3}):
+    for cfg in ({"mode": "rational_map", "baryon_number": 2, "scale": 1.5},
+                {"mode": "hedgehog", "noise": 1e-3, "seed": 3}):
         sim = Simulation(p, th)
         sim.initialize(cfg)
         torch.cuda.synchronize()
