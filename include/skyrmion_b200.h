@@ -201,6 +201,19 @@ int sky_sum(const double* values, int64_t n, double* scratch, int64_t n_scratch,
 int sky_max(const double* values, int64_t n, double* scratch, int64_t n_scratch, double* out_host,
             double* out_dev, void* stream);
 
+/* Replaces compute_min (core/utils.py:282-319, 375-400): the minimum of n values,
+ * exact (the negated maximum of the negated values).  Same buffers as sky_max. */
+int sky_min(const double* values, int64_t n, double* scratch, int64_t n_scratch, double* out_host,
+            double* out_dev, void* stream);
+
+/* Replaces arresting_criteria and arresting_criteria_kernel
+ * (core/integrator.py:178-282): per site the power sum_a V_a EG_a (written to en
+ * if it is not NULL) and its compensated sum over the lattice, into *out_host
+ * (synchronous) when out_host is not NULL.  scratch: sky_reduce_scratch_size()
+ * doubles. */
+int sky_arresting_criteria(const int32_t* p_i, int32_t n_pi, const double* velocity, const double* energy_gradient,
+                           double* en, double* scratch, int64_t n_scratch, double* out_host, void* stream);
+
 /* Replace the host compute_energy / compute_skyrmion_number
  * (th/nuclear_skyrme/observables.py:408-474): the per-site density and its
  * compensated FP64 sum fused into one launch (no per-site buffer round trip). */

@@ -626,6 +626,19 @@ def block_tree_sum(values):
     return float(buf[:, 0].sum())
 
 
+def arresting_power(velocity, eg):
+    """Lattice sum of sum_a V_a EG_a (arresting_criteria, core/integrator.py:178-282), exact
+    (math.fsum) on the per-site powers summed in component order."""
+    import math as _m
+    C = velocity.shape[0]
+    v = velocity.reshape(C, -1)
+    g = eg.reshape(C, -1)
+    site = np.zeros(v.shape[1])
+    for a in range(C):
+        site = site + v[a] * g[a]
+    return site, _m.fsum(site.tolist())
+
+
 def signed_max(values):
     """compute_max_field (core/utils.py:241-279, 402-424): signed maximum over all entries."""
     return float(np.max(values))

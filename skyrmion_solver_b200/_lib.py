@@ -68,6 +68,8 @@ SIGNATURES = {
     "sky_create_grid": ([_I32P, _I32, _F64P, _I32, _P, _P], _I),
     "sky_sum": ([_P, _I64, _P, _I64, _F64P, _P, _P], _I),
     "sky_max": ([_P, _I64, _P, _I64, _F64P, _P, _P], _I),
+    "sky_min": ([_P, _I64, _P, _I64, _F64P, _P, _P], _I),
+    "sky_arresting_criteria": ([_I32P, _I32, _P, _P, _P, _P, _I64, _F64P, _P], _I),
     "sky_total_energy": ([_I, _I32P, _I32, _F64P, _I32, _P, _P, _I64, _F64P, _P], _I),
     "sky_total_baryon": ([_I, _I32P, _I32, _F64P, _I32, _P, _P, _I64, _F64P, _P], _I),
     "sky_arrested_newton_step": ([_I, _I32P, _I32, _F64P, _I32] + [_P] * 12 + [_P, _I64, _D, _F64P, _F64P, _P],

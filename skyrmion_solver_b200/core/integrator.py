@@ -12,11 +12,26 @@ import ctypes
 
 from .. import _lib
 from .._lib import dptr, f64p, host_params, i32p, stream_ptr
-from .launch import RK4FinalizeKernel, RK4StageKernel
+from .launch import ArrestingCriteriaKernel, RK4FinalizeKernel, RK4StageKernel
 from .utils import compute_max_field, launch_3d, pick_scratch, set_field_zero_kernel, _numel
 
 do_rk4_step_kernel = RK4StageKernel()
 do_rk4_kernel_no_constraint = RK4FinalizeKernel(-1, "do_rk4_kernel_no_constraint")
+arresting_criteria_kernel = ArrestingCriteriaKernel()
+
+
+def arresting_criteria(Velocity, EnergyGradient, en, entmp, gridsum_partial, p_i_d, p_i_h) -> float:
+    """Lattice sum of the power V . EG (core/integrator.py:243-282), one fused launch with a
+    compensated sum; leaves en and entmp zeroed, as the reference does."""
+    hi, _ = host_params(p_i_h)
+    scratch = pick_scratch(gridsum_partial)
+    out = ctypes.c_double(0.0)
+    _lib.call("sky_arresting_criteria", i32p(hi), len(hi), dptr(Velocity), dptr(EnergyGradient), None,
+              dptr(scratch), _numel(scratch), ctypes.byref(out), stream_ptr())
+    for buf in (en, entmp):
+        if buf is not None and hasattr(buf, "zero_"):
+            buf.zero_()
+    return float(out.value)
 
 
 def make_do_gradient_step_kernel(do_gradient_step_point):

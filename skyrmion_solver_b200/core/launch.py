@@ -135,6 +135,20 @@ class RhoMesonKernel(Launchable):
         _lib.call("sky_rho_meson_density", i32p(hi), len(hi), dptr(en), dptr(Field), stream_ptr())
 
 
+class ArrestingCriteriaKernel(Launchable):
+    """arresting_criteria_kernel(Velocity, EnergyGradient, en, p_i) (core/integrator.py:213-241):
+    en = per-site power V . EG."""
+
+    name = "arresting_criteria_kernel"
+
+    def __call__(self, Velocity, EnergyGradient, en, p_i):
+        from .utils import reduction_scratch
+        hi, _ = self._params(p_i)
+        scratch = reduction_scratch()
+        _lib.call("sky_arresting_criteria", i32p(hi), len(hi), dptr(Velocity), dptr(EnergyGradient), dptr(en),
+                  dptr(scratch), scratch.numel(), None, stream_ptr())
+
+
 class SetFieldZeroKernel(Launchable):
     """set_field_zero_kernel(Field, p_i) (core/utils.py:148-174)."""
 

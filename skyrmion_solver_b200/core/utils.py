@@ -1,7 +1,7 @@
 """Launch helpers and reductions with the reference's interface
 (skyrmion_solver ``core/utils.py:176-424``).
 
-The reductions are deterministic FP64 (compensated sum, signed max) and run
+The reductions are deterministic FP64 (compensated sum, signed max, min) and run
 as a single sm_100a launch each; the reference's block-partial buffers are
 accepted and used as scratch when large enough.
 """
@@ -81,6 +81,11 @@ def compute_sum(var_d, partial_d, size: int) -> float:
 def compute_max(var_d, partial_d, size: int) -> float:
     """Signed maximum of the first ``size`` entries (core/utils.py:348-373)."""
     return _reduce("sky_max", var_d, partial_d, size)
+
+
+def compute_min(var_d, partial_d, size: int) -> float:
+    """Minimum of the first ``size`` entries (core/utils.py:375-400)."""
+    return _reduce("sky_min", var_d, partial_d, size)
 
 
 def compute_max_field(EnergyGradient, max_partial, p_i_h) -> float:

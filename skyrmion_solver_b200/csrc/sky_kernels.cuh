@@ -142,8 +142,11 @@ __device__ __forceinline__ void finish_ksum(KSum v, double* __restrict__ scratch
     }
 }
 
+// Block maxima, then the last block to finish reduces them; the result, times `sign`,
+// goes to scratch[2 kMaxRedBlocks] and *out_dev (sign -1 turns a maximum of negated
+// values into a minimum).
 __device__ __forceinline__ void finish_max(double v, double* __restrict__ scratch, double* __restrict__ out_dev,
-                                           double* shm) {
+                                           double* shm, double sign = 1.0) {
     __shared__ bool am_last;
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
     double b = block_max(v, shm);
@@ -160,7 +163,7 @@ __device__ __forceinline__ void finish_max(double v, double* __restrict__ scratc
     const int nthreads = blockDim.x * blockDim.y;
     double acc = -1.0e300;
     for (int i = tid; i < (int)gridDim.x; i += nthreads) acc = fmax(acc, __ldcg(scratch + 2 * i));
-    double r = block_max(acc, shm);
+    const double r = sign * block_max(acc, shm);
     if (tid == 0) {
         scratch[2 * kMaxRedBlocks] = r;
         if (out_dev) *out_dev = r;

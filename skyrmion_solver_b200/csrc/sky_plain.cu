@@ -135,6 +135,34 @@ __global__ void __launch_bounds__(256) k_max(const double* __restrict__ v, int64
     finish_max(acc, scratch, out_dev, shm);
 }
 
+// compute_min (core/utils.py:282-319, 375-400) as the negated maximum of the negated
+// values: exact, and +1e300 padding becomes the maximum's -1e300.
+__global__ void __launch_bounds__(256) k_min(const double* __restrict__ v, int64_t n, double* __restrict__ scratch,
+                                             double* __restrict__ out_dev) {
+    __shared__ double shm[32];
+    double acc = -1.0e300;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc = fmax(acc, -v[i]);
+    finish_max(acc, scratch, out_dev, shm, -1.0);
+}
+
+// arresting_criteria_kernel + arresting_criteria (core/integrator.py:178-282): per site
+// the power V . EG over the C components (summed in component order), optionally stored
+// in en, and its compensated sum over the lattice.
+__global__ void __launch_bounds__(256) k_power(const double* __restrict__ vel, const double* __restrict__ eg,
+                                               int64_t N, int C, double* __restrict__ en,
+                                               double* __restrict__ scratch, double* __restrict__ out_dev) {
+    __shared__ KSum shk[32];
+    KSum acc{0.0, 0.0};
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < N; s += (int64_t)gridDim.x * blockDim.x) {
+        double f = 0.0;
+        for (int a = 0; a < C; ++a) f += vel[a * N + s] * eg[a * N + s];
+        if (en) en[s] = f;
+        ksum_add(acc, f);
+    }
+    finish_ksum(acc, scratch, out_dev, shk);
+}
+
 // ---------------------------------------------------------------------------
 // host helpers
 // ---------------------------------------------------------------------------
@@ -585,8 +613,10 @@ int reduce(int kind, const double* v, int64_t n, double* scratch, double* out_de
     if (rc) return rc;
     if (kind == 0)
         k_sum<<<(int)b, 256, 0, st>>>(v, n, scratch, out_dev);
-    else
+    else if (kind == 1)
         k_max<<<(int)b, 256, 0, st>>>(v, n, scratch, out_dev);
+    else
+        k_min<<<(int)b, 256, 0, st>>>(v, n, scratch, out_dev);
     return check_cuda(cudaGetLastError(), "launch reduce", __LINE__);
 }
 
@@ -733,6 +763,30 @@ int sky_sum(const double* values, int64_t n, double* scratch, int64_t n_scratch,
 int sky_max(const double* values, int64_t n, double* scratch, int64_t n_scratch, double* out_host, double* out_dev,
             void* stream) {
     return reduce_entry(1, values, n, scratch, n_scratch, out_host, out_dev, stream);
+}
+
+int sky_min(const double* values, int64_t n, double* scratch, int64_t n_scratch, double* out_host, double* out_dev,
+            void* stream) {
+    return reduce_entry(2, values, n, scratch, n_scratch, out_host, out_dev, stream);
+}
+
+int sky_arresting_criteria(const int32_t* p_i, int32_t n_pi, const double* velocity, const double* energy_gradient,
+                           double* en, double* scratch, int64_t n_scratch, double* out_host, void* stream) {
+    Params p;
+    int rc = pack_core(p_i, n_pi, nullptr, 0, &p, false);
+    if (rc) return rc;
+    if (!velocity || !energy_gradient) return invalid("null buffer");
+    if (!scratch || n_scratch < kScratchDoubles) return SKY_ERR_NOMEM;
+    cudaStream_t st = SKY_STREAM(stream);
+    const int64_t N = n_sites(p);
+    int64_t b = (N + 1023) / 1024;
+    if (b > kMaxRedBlocks) b = kMaxRedBlocks;
+    rc = check_cuda(cudaMemsetAsync(scratch + 2 * kMaxRedBlocks + 1, 0, sizeof(double), st), "memset", __LINE__);
+    if (rc) return rc;
+    k_power<<<(int)b, 256, 0, st>>>(velocity, energy_gradient, N, p.C, en, scratch, nullptr);
+    rc = check_cuda(cudaGetLastError(), "launch arresting criteria", __LINE__);
+    if (rc || !out_host) return rc;
+    return read_result(scratch, out_host, st);
 }
 
 static int total_entry(int mode, int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,

@@ -155,7 +155,7 @@ def test_unfused_schedule_matches_fused(gold):
 def test_reductions_exact_and_deterministic():
     import math
     import torch
-    from skyrmion_solver_b200.core.utils import compute_max, compute_sum
+    from skyrmion_solver_b200.core.utils import compute_max, compute_min, compute_sum
     rng = np.random.default_rng(7)
     for n in (1, 1023, 1024, 1025, 262144, 3_000_001):
         x = rng.standard_normal(n) * 10.0 ** rng.uniform(-8, 8, size=n)
@@ -165,7 +165,29 @@ def test_reductions_exact_and_deterministic():
         assert s1 == s2
         assert abs(s1 - math.fsum(x)) <= 1e-15 * np.abs(x).sum() + 1e-300
         assert compute_max(t, None, n) == float(np.max(x))
+        assert compute_min(t, None, n) == float(np.min(x))
+    assert compute_min(dev(np.arange(3.0, 5000.0)), None, 4997) == 3.0    # all positive: not the padding
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("name", ["nuclear", "rho"])
+def test_arresting_criteria_matches_the_oracle(name):
+    """Power V . EG (arresting_criteria, core/integrator.py:178-282) on the golden velocity and
+    gradient: the lattice sum to the exact sum's rounding, the per-site values to FMA rounding."""
+    import torch
+    from oracle import skyrme_oracle as O
+    from skyrmion_solver_b200.core.integrator import arresting_criteria, arresting_criteria_kernel
+    d = G.load(name)
+    V, EG = d["velocity0"], d["grad_eg"]
+    site, total = O.arresting_power(V, EG)
+    en = torch.full((site.size,), 5.0, dtype=torch.float64, device="cuda")
+    entmp = torch.full_like(en, 5.0)
+    got = arresting_criteria(dev(V), dev(EG), en, entmp, None, None, d["p_i"])
+    assert abs(got - total) <= 1e-15 * np.abs(site).sum()
+    assert float(en.abs().max()) == 0.0 and float(entmp.abs().max()) == 0.0
+    arresting_criteria_kernel[(1, 1, 1), (8, 8, 4)](dev(V), dev(EG), en, d["p_i"])
+    torch.cuda.synchronize()
+    assert np.max(np.abs(en.cpu().numpy() - site)) <= 1e-14 * np.abs(site).max()
 
 
 def test_signed_max_padding_semantics():

@@ -67,3 +67,14 @@ def test_init_field_rejects_bad_soliton_lists():
     assert lib.sky_init_field(*args, 1, _lib.i32p(b3), _lib.f64p(c), _lib.f64p(q), 1.5, 0, dummy, None) == 1
     assert lib.sky_init_field(*args, 1, _lib.i32p(b), _lib.f64p(c), _lib.f64p(q), 0.0, 0, dummy, None) == 1
     assert lib.sky_init_field(*args, 1, _lib.i32p(b), _lib.f64p(c), _lib.f64p(q), 1.5, 0, None, None) == 1
+
+
+def test_min_and_arresting_criteria_reject_bad_arguments():
+    lib = _lib.load()
+    dummy = ctypes.c_void_p(16)
+    out = ctypes.c_double()
+    assert lib.sky_min(None, 10, dummy, 1 << 20, ctypes.byref(out), None, None) == 1
+    assert lib.sky_min(dummy, 10, dummy, 4, ctypes.byref(out), None, None) == 5
+    n = lib.sky_reduce_scratch_size(0)
+    assert lib.sky_arresting_criteria(_lib.i32p(_pi()), 11, None, dummy, None, dummy, n, ctypes.byref(out), None) == 1
+    assert lib.sky_arresting_criteria(_lib.i32p(_pi()), 11, dummy, dummy, None, dummy, 4, ctypes.byref(out), None) == 5
