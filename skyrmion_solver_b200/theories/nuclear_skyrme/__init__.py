@@ -1,9 +1,9 @@
 """Nuclear Skyrme model: theory package with the reference's submodules (params, kernels,
-initial_config, observables, io) backed by the sm_100a engine."""
+initial_config, observables, io, render_headless) backed by the sm_100a engine."""
 from __future__ import annotations
 
 from ..registry import TheorySpec
-from . import initial_config, io, kernels, observables, params
+from . import initial_config, io, kernels, observables, params, render_headless
 
 THEORY_SPEC = TheorySpec(
     name="Nuclear Skyrme model",

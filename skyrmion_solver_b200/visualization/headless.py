@@ -28,6 +28,58 @@ DISPLAY_BARYON = 2
 DISPLAY_TITLES = {DISPLAY_ENERGY_SINGLE: "Energy density", DISPLAY_BARYON: "Baryon density"}
 
 
+def advance_solver(sim, steps_per_frame: int, state: dict) -> None:
+    """The viewer's solver advance (th/nuclear_skyrme/render_gl.py:944-973): the first call
+    takes the energy from ``observables()``; with Newton flow on, ``steps_per_frame`` calls of
+    ``sim.step`` update ``state["energy"]``, ``state["error"]`` and ``state["epochs"]``."""
+    if state.get("energy") is None:
+        state["energy"] = float(sim.observables()["energy"])
+    if sim.rp.newtonflow:
+        for _ in range(int(steps_per_frame)):
+            state["energy"], state["error"] = sim.step(state["energy"])
+            state["epochs"] += 1
+
+
+def hud_text(sim, state: dict, running: bool = True):
+    """The viewer's two HUD lines (render_gl.py:1055-1069): time and epochs with the error,
+    then energy, baryon number and the run state."""
+    epochs = int(state.get("epochs", 0))
+    top = f"t={epochs * float(sim.p_f_h[7]):.3f} ({epochs} epochs)"
+    if state.get("error") is not None:
+        top += f", err={float(state['error']):.3e}"
+    parts = []
+    if state.get("energy") is not None:
+        parts.append(f"E={float(state['energy']):.6f}")
+    if state.get("baryon") is not None:
+        parts.append(f"B={float(state['baryon']):.6f}")
+    parts.append("running" if running else "paused")
+    return top, ", ".join(parts)
+
+
+def viewer_loop(sim, renderer, density_for_mode, *, steps_per_frame: int = 5, frames: int = 1,
+                output_dir: str | None = "screenshots", display_mode: int = DISPLAY_ENERGY_SINGLE):
+    """The reference's run_viewer loop (render_gl.py:1001-1075) without a window: per frame,
+    advance the solver, read the observables, fill the density of the display mode, draw, and
+    (when output_dir is given) save a screenshot.  Returns (state, screenshot paths)."""
+    renderer.bind_sim(sim)
+    renderer.set_display_mode(display_mode)
+    state = {"energy": None, "error": None, "epochs": 0, "baryon": None}
+    paths = []
+    for _ in range(int(frames)):
+        advance_solver(sim, steps_per_frame, state)
+        obs = sim.observables()
+        state["energy"] = float(obs["energy"])
+        if "skyrmion_number" in obs:
+            state["baryon"] = float(obs["skyrmion_number"])
+        density_for_mode(sim, renderer.display_mode)
+        top, bottom = hud_text(sim, state)
+        renderer.set_hud_text(top=top, bottom=bottom)
+        renderer.render(density_flat=sim.en, field_flat=sim.Field)
+        if output_dir is not None:
+            paths.append(renderer.save_screenshot(output_dir))
+    return state, paths
+
+
 def inv_view_rows(view_rotation=(0.0, 0.0, 0.0), view_translation=(0.0, 0.0, -4.0)) -> np.ndarray:
     """Rows 0..2 (float32, shape (3, 4)) of R @ T(-t) with R = R_x(-rx) R_y(-ry), the shader's
     inverse view (gl_backend.py:1166-1228): columns 0..2 rotate the eye ray, column 3 is its origin."""
@@ -48,9 +100,12 @@ class HeadlessRenderer:
     ``bind_sim(sim)`` sizes the volume from the simulation's lattice and sets the box
     aspect from its extents; ``render(density_flat=sim.en, field_flat=sim.Field)`` draws
     one frame into ``self.image`` (CUDA tensor (height, width, 4), FP32).  The display
-    mode picks the colouring: DISPLAY_ENERGY_SINGLE uses the transfer table, any other
-    mode the pion vector's colour (the reference's color_mode 0 / 1).
+    mode picks the colouring: DISPLAY_BARYON uses the pion vector's colour, the other
+    modes the transfer table (the reference's color_mode 1 / 0).  ``titles`` lists the
+    display modes; the theories' render_headless modules add their third mode.
     """
+
+    titles = DISPLAY_TITLES
 
     def __init__(self, width: int, height: int, depth: int = 1, title: str = "skyrmion_solver (headless)",
                  device=None) -> None:
@@ -80,6 +135,8 @@ class HeadlessRenderer:
         self.volume = None
         self.image = None
         self._scratch = None
+        self.hud_top_text = ""
+        self.hud_bottom_text = ""
 
     # -- binding and controls -------------------------------------------------
     def bind_sim(self, sim) -> None:
@@ -110,8 +167,12 @@ class HeadlessRenderer:
         self.set_render_params(box_scale=(size / scale).astype(np.float32))
 
     def set_display_mode(self, mode: int) -> None:
-        if mode in DISPLAY_TITLES:
+        if mode in self.titles:
             self.display_mode = mode
+
+    def set_hud_text(self, *, top: str = "", bottom: str = "") -> None:
+        self.hud_top_text = top
+        self.hud_bottom_text = bottom
 
     def set_render_params(self, *, brightness=None, levelset=None, transfer_scale=None, opacity_scale=None,
                           max_steps=None, tstep=None, density_min=None, density_max=None, box_scale=None,
@@ -153,7 +214,9 @@ class HeadlessRenderer:
 
     @property
     def color_mode(self) -> int:
-        return 0 if self.display_mode == DISPLAY_ENERGY_SINGLE else 1
+        """Pion-vector colouring for the baryon display, the transfer table otherwise (the
+        viewers' _sync_render_params)."""
+        return 1 if self.display_mode == DISPLAY_BARYON else 0
 
     def shader_params(self) -> np.ndarray:
         """The 23 floats of sky_render_volume: view rows, box, zoom, brightness, levelset,

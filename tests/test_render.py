@@ -262,3 +262,112 @@ def test_headless_renderer_frame_and_screenshot(tmp_path):
     px = np.asarray(Image.open(path))
     assert px.shape == (36, 48, 3) and px.dtype == np.uint8
     assert np.array_equal(px, r.read_pixels())
+
+
+# ---------------------------------------------------------------------------
+# the viewer loop (render_gl.py advance_solver / run_viewer without a window)
+# ---------------------------------------------------------------------------
+class _FakeSim:
+    """Records the calls the viewer loop makes; energy falls by 1 per step."""
+
+    def __init__(self, newtonflow=True):
+        self.rp = type("RP", (), {"newtonflow": newtonflow})()
+        self.p_f_h = np.array([1.0, 1.0, 1.0, 0.1, 0.1, 0.1, 1e-3, 0.25])
+        self.calls = []
+
+    def observables(self):
+        self.calls.append("observables")
+        return {"energy": 10.0}
+
+    def step(self, e):
+        self.calls.append("step")
+        return e - 1.0, 0.5
+
+
+def test_advance_solver_follows_the_reference():
+    from skyrmion_solver_b200.visualization import advance_solver, hud_text
+    sim = _FakeSim()
+    state = {"energy": None, "error": None, "epochs": 0, "baryon": None}
+    advance_solver(sim, 3, state)
+    assert sim.calls == ["observables", "step", "step", "step"]
+    assert state == {"energy": 7.0, "error": 0.5, "epochs": 3, "baryon": None}
+    advance_solver(sim, 2, state)
+    assert state["epochs"] == 5 and state["energy"] == 5.0 and sim.calls.count("observables") == 1
+    state["baryon"] = 1.0
+    assert hud_text(sim, state) == ("t=1.250 (5 epochs), err=5.000e-01", "E=5.000000, B=1.000000, running")
+    off = _FakeSim(newtonflow=False)                      # without Newton flow the viewer does not step
+    st = {"energy": None, "error": None, "epochs": 0}
+    advance_solver(off, 4, st)
+    assert off.calls == ["observables"] and st["epochs"] == 0
+
+
+def test_viewer_loop_host_logic():
+    """Frame order of the loop with a recording renderer: advance, observables, density, HUD,
+    draw, screenshot."""
+    from skyrmion_solver_b200.visualization import viewer_loop
+    from skyrmion_solver_b200.visualization.headless import HeadlessRenderer
+
+    class _Rec(HeadlessRenderer):
+        def bind_sim(self, sim):
+            self._sim = sim
+            sim.calls.append("bind")
+
+        def render(self, *, density_flat, field_flat, stream=None):
+            self._sim.calls.append(("render", self.hud_top_text, self.hud_bottom_text))
+
+        def save_screenshot(self, directory="screenshots"):
+            self._sim.calls.append("shot")
+            return directory + "/frame.png"
+
+    sim = _FakeSim()
+    sim.en, sim.Field = "en", "field"
+    state, paths = viewer_loop(sim, _Rec(8, 6), lambda s, m: s.calls.append(("density", m)), steps_per_frame=1,
+                               frames=2, output_dir="out", display_mode=2)
+    assert paths == ["out/frame.png"] * 2 and state["epochs"] == 2
+    assert sim.calls == ["bind", "observables", "step", "observables", ("density", 2),
+                         ("render", "t=0.250 (1 epochs), err=5.000e-01", "E=10.000000, running"), "shot",
+                         "step", "observables", ("density", 2),
+                         ("render", "t=0.500 (2 epochs), err=5.000e-01", "E=10.000000, running"), "shot"]
+
+
+def test_theory_display_modes():
+    from skyrmion_solver_b200 import theories as T
+    for short, third in [("nuclear", None), ("berger", None), ("lightly_bound", None),
+                         ("omega", "DISPLAY_OMEGA"), ("coulomb", "DISPLAY_COULOMB"), ("rho", "DISPLAY_RHO_MESON")]:
+        m = T.by_short_name(short).render_headless
+        r = m.Renderer(16, 12)
+        assert r.color_mode == 0                          # energy display: transfer table
+        r.set_display_mode(2)
+        assert r.color_mode == 1                          # baryon display: pion colouring
+        if third:
+            r.set_display_mode(getattr(m, third))
+            assert r.display_mode == 3 and r.color_mode == 0
+        else:
+            r.set_display_mode(3)
+            assert r.display_mode == 2                    # not a mode of this theory
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("short,mode", [("nuclear", 2), ("omega", 3), ("rho", 3)])
+def test_headless_run_viewer(tmp_path, short, mode):
+    import torch
+    from skyrmion_solver_b200 import theories as T
+    from skyrmion_solver_b200.core.simulation import Simulation
+    th = T.by_short_name(short)
+    params = th.params.default_params(xlen=24, ylen=24, zlen=24, lsx=0.25, lsy=0.25, lsz=0.25)
+    sim = Simulation(params, th)
+    sim.initialize({"mode": "rational_map", "baryon_number": 2})
+    e0 = float(sim.observables()["energy"])
+    state, paths = th.render_headless.run_viewer(sim, params, steps_per_frame=2, frames=3, output_dir=str(tmp_path),
+                                                 display_mode=mode, width=40, height=30)
+    torch.cuda.synchronize()
+    assert state["epochs"] == 6 and len(paths) == 3 and all(os.path.exists(p) for p in paths)
+    assert state["energy"] < e0
+    # the last frame shows the display mode's density, as left in sim.en
+    want = {2: "compute_baryon_density", 3: ("compute_potential_density" if short == "omega"
+                                             else "compute_rho_meson_density")}[mode]
+    en = sim.en.clone()
+    sim.en.zero_()                                        # the rho-meson kernel accumulates, as the reference's does
+    getattr(sim, want)()
+    torch.cuda.synchronize()
+    assert torch.equal(en, sim.en)
