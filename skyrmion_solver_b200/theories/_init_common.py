@@ -243,13 +243,34 @@ def build_reference_field(short, p_i, p_f, config, out, stream=None):
     return out
 
 
+def _host_params(p_i_d, p_f_d):
+    """Host copies of device parameter arrays (DeviceParams, Numba device arrays or tensors)."""
+    from .. import _lib
+    return _lib.host_params(p_i_d, p_f_d)
+
+
+def _as_tensor(buf):
+    """A torch view of a device buffer: torch tensors as they are, other objects with a
+    __cuda_array_interface__ (Numba device arrays from the reference's Simulation) zero-copy."""
+    import torch
+    if buf is None or isinstance(buf, torch.Tensor):
+        return buf
+    if hasattr(buf, "__cuda_array_interface__"):
+        return torch.as_tensor(buf, device="cuda")
+    return buf
+
+
 def make_initialize(short):
     def initialize(*, Velocity, Field, grid=None, p_i_d=None, p_f_d=None, p_i_h=None, p_f_h=None, config=None,
                    **_unused):
         import torch
+        Field, Velocity = _as_tensor(Field), _as_tensor(Velocity)
+        _unused = {k: _as_tensor(v) if k in ("k1", "k2", "k3", "k4", "l1", "l2", "l3", "l4", "Temp") else v
+                   for k, v in _unused.items()}
         cfg = config or {}
-        p_i = np.asarray(p_i_h if p_i_h is not None else p_i_d.host)
-        p_f = np.asarray(p_f_h if p_f_h is not None else p_f_d.host)
+        hi, hf = _host_params(p_i_d if p_i_h is None else None, p_f_d if p_f_h is None else None)
+        p_i = np.asarray(p_i_h if p_i_h is not None else hi)
+        p_f = np.asarray(p_f_h if p_f_h is not None else hf)
         mode = str(cfg.get("mode", "initial")).lower().strip()
         if is_reference_config(cfg):
             if not Field.is_cuda:

@@ -188,3 +188,31 @@ def test_device_lumps_match_the_oracle_on_larger_lattices(short, cfg):
     torch.cuda.synchronize()
     want = I.initial_field(short, p_i, p_f, cfg)
     _check(short, p_i, p_f, out.cpu().numpy(), want)
+
+
+class _CAI:
+    """A device buffer known only by its __cuda_array_interface__, as a Numba device array is."""
+
+    def __init__(self, t):
+        self._t = t
+        self.__cuda_array_interface__ = t.__cuda_array_interface__
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("key", ["omega/map_b3", "nuclear/smorgasbord", "rho/default"])
+def test_initialize_accepts_foreign_device_arrays(key):
+    """The theory's initialize as the reference's own Simulation calls it, with buffers that are
+    not torch tensors: the field is written through them."""
+    import torch
+    from skyrmion_solver_b200 import theories as T
+    short, p_i, p_f, cfg, want, _ = _case(key)
+    th = T.by_short_name(short)
+    C, N = int(p_i[5]), int(p_i[6])
+    field = torch.zeros(C * N, dtype=torch.float64, device="cuda")
+    vel = torch.full((C * N,), 2.0, dtype=torch.float64, device="cuda")
+    temp = torch.full((C * N,), 2.0, dtype=torch.float64, device="cuda")
+    th.initial_config.initialize(Velocity=_CAI(vel), Field=_CAI(field), Temp=_CAI(temp), p_i_h=p_i, p_f_h=p_f,
+                                 p_i_d=None, p_f_d=None, grid3d=None, block3d=None, config=dict(cfg))
+    torch.cuda.synchronize()
+    _check(short, p_i, p_f, field.cpu().numpy(), want)
+    assert float(vel.abs().max()) == 0.0 and float(temp.abs().max()) == 0.0
