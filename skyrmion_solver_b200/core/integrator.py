@@ -28,9 +28,8 @@ def arresting_criteria(Velocity, EnergyGradient, en, entmp, gridsum_partial, p_i
     out = ctypes.c_double(0.0)
     _lib.call("sky_arresting_criteria", i32p(hi), len(hi), dptr(Velocity), dptr(EnergyGradient), None,
               dptr(scratch), _numel(scratch), ctypes.byref(out), stream_ptr())
-    for buf in (en, entmp):
-        if buf is not None and hasattr(buf, "zero_"):
-            buf.zero_()
+    from .observables import _zero
+    _zero(en, entmp)
     return float(out.value)
 
 

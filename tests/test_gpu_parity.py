@@ -212,3 +212,47 @@ def test_simulation_initialize_modes():
     g = sim.grid.view(3, -1)
     assert float(g[0, -1]) == pytest.approx(0.2 * 23)
     torch.cuda.synchronize()
+
+
+class _Foreign:
+    """A device array as Numba hands it over: __cuda_array_interface__ plus copy_to_host, and
+    slice assignment of a scalar; no torch methods."""
+
+    def __init__(self, t):
+        self._t = t
+        self.__cuda_array_interface__ = t.__cuda_array_interface__
+
+    def copy_to_host(self):
+        return self._t.cpu().numpy()
+
+    def __setitem__(self, key, value):
+        self._t[key] = value
+
+
+@pytest.mark.parametrize("opaque", [False, True])
+def test_reference_driver_with_foreign_buffers(gold, opaque):
+    """The reference's Simulation.step / observables call pattern with Numba-like buffers: the
+    fused call and the per-launch schedule give the same bits as the torch-buffer driver."""
+    from skyrmion_solver_b200.core.integrator import do_arrested_newton_flow
+    name, d = gold
+    th, sim_a = golden_simulation(name, d)
+    _, sim_b = golden_simulation(name, d)
+    F = {k: _Foreign(getattr(sim_b, k)) for k in ("Velocity", "Field", "EnergyGradient", "k1", "k2", "k3", "k4", "l1",
+                                                   "l2", "l3", "l4", "Temp", "en", "entmp", "gridsum_partial",
+                                                   "max_partial")}
+    p_i_d, p_f_d = _Foreign(sim_b.p_i_d.device), _Foreign(sim_b.p_f_d.device)
+    wrap = _Opaque if opaque else (lambda k: k)
+    for s in range(2):
+        prev = float(d[f"prev{s}"])
+        ea, erra = sim_a.step(prev)
+        eb, errb = do_arrested_newton_flow(
+            F["Velocity"], F["Field"], None, None, F["EnergyGradient"], F["k1"], F["k2"], F["k3"], F["k4"], F["l1"],
+            F["l2"], F["l3"], F["l4"], F["Temp"], F["en"], F["entmp"], F["gridsum_partial"], F["max_partial"],
+            p_i_d, p_f_d, sim_b.p_i_h, sim_b.p_f_h, prev, wrap(th.observables.compute_energy),
+            wrap(th.kernels.do_gradient_step_kernel), wrap(th.kernels.do_rk4_kernel))
+        assert ea == eb and erra == errb
+        assert bool((sim_a.Field == sim_b.Field).all()) and bool((sim_a.Velocity == sim_b.Velocity).all())
+    e = th.observables.compute_energy(F["Field"], None, F["en"], F["entmp"], F["gridsum_partial"], p_i_d, p_f_d,
+                                      sim_b.p_i_h, sim_b.p_f_h)
+    assert e == sim_a.observables()["energy"]
+    assert not sim_b.en.any() and not sim_b.entmp.any()
