@@ -173,8 +173,10 @@ int sky_init_lumps(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t 
  * normalised to its [min, max] (c = 0) and the unit pion vector (c = 1..3;
  * (0, 0, 1) where |pi|^2 <= 1e-20).  `density` holds N FP64 values, `field`
  * the reference-layout field (C >= 4).  `scratch` holds at least
- * sky_volume_scratch_size() doubles.  If minmax_host is not NULL, the density
- * minimum and maximum are written there and the stream is synchronised. */
+ * sky_volume_scratch_size() doubles; once the stream reaches the end of the
+ * call, scratch[0] and scratch[1] hold the density minimum and maximum.  If
+ * minmax_host is not NULL, they are also copied there and the stream is
+ * synchronised; otherwise the call is asynchronous. */
 int64_t sky_volume_scratch_size(void);
 int sky_build_rgba_volume(const int32_t* p_i, int32_t n_pi, const double* density, const double* field,
                           double* scratch, int64_t n_scratch, float* volume, double* minmax_host, void* stream);

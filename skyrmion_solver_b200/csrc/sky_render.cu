@@ -282,15 +282,15 @@ int sky_build_rgba_volume(const int32_t* p_i, int32_t n_pi, const double* densit
     const int64_t N = n_sites(p);
     int nb = ew_blocks(N);
     if (nb > kMMBlocks) nb = kMMBlocks;
-    k_minmax_partial<<<nb, 256, 0, st>>>(density, N, scratch);
-    k_minmax_final<<<1, 256, 0, st>>>(scratch, nb, scratch + 2 * kMMBlocks);
+    // partial extrema at scratch[2 ..], the global pair at scratch[0], scratch[1]
+    k_minmax_partial<<<nb, 256, 0, st>>>(density, N, scratch + 2);
+    k_minmax_final<<<1, 256, 0, st>>>(scratch + 2, nb, scratch);
     const dim3 vgrid((p.Z + 31) / 32, p.Y, (p.X + 31) / 32);
-    k_build_volume<<<vgrid, dim3(32, 8), 0, st>>>(p.X, p.Y, p.Z, density, field, scratch + 2 * kMMBlocks,
+    k_build_volume<<<vgrid, dim3(32, 8), 0, st>>>(p.X, p.Y, p.Z, density, field, scratch,
                                                   reinterpret_cast<float4*>(volume));
     rc = check_cuda(cudaGetLastError(), "launch volume", __LINE__);
     if (rc || !minmax_host) return rc;
-    rc = check_cuda(cudaMemcpyAsync(minmax_host, scratch + 2 * kMMBlocks, 2 * sizeof(double), cudaMemcpyDeviceToHost,
-                                    st),
+    rc = check_cuda(cudaMemcpyAsync(minmax_host, scratch, 2 * sizeof(double), cudaMemcpyDeviceToHost, st),
                     "read extrema", __LINE__);
     if (rc) return rc;
     return check_cuda(cudaStreamSynchronize(st), "sync", __LINE__);

@@ -129,7 +129,6 @@ class HeadlessRenderer:
         self.density_min = 0.0
         self.density_max = 1.0  # the volume's channel 0 is already normalised to [0, 1]
         self.box_scale = np.array([1.0, 1.0, 1.0], dtype=np.float32)
-        self.extrema = None
         self._sim = None
         self._dims = None
         self.volume = None
@@ -228,16 +227,23 @@ class HeadlessRenderer:
 
     # -- frame ------------------------------------------------------------------
     def build_volume(self, density_flat, field_flat, stream=None):
-        """Fill ``self.volume`` from the density (N FP64 values) and the field; returns it."""
+        """Fill ``self.volume`` from the density (N FP64 values) and the field; returns it.
+        Asynchronous: the density extrema stay on the device until ``extrema`` is read."""
         if self._sim is None:
             raise RuntimeError("bind_sim(sim) first")
         p_i, _ = _lib.host_params(self._sim.p_i_h)
-        mm = np.zeros(2, np.float64)
         _lib.call("sky_build_rgba_volume", _lib.i32p(p_i), len(p_i), _lib.dptr(density_flat), _lib.dptr(field_flat),
-                  _lib.dptr(self._scratch), self._scratch.numel(), _lib.dptr(self.volume, "float32"), _lib.f64p(mm),
+                  _lib.dptr(self._scratch), self._scratch.numel(), _lib.dptr(self.volume, "float32"), None,
                   _lib.stream_ptr(stream))
-        self.extrema = (float(mm[0]), float(mm[1]))
         return self.volume
+
+    @property
+    def extrema(self):
+        """(min, max) of the density of the last volume (the library leaves them in scratch[0:2])."""
+        if self._scratch is None:
+            return None
+        mm = self._scratch[:2].cpu().numpy()
+        return float(mm[0]), float(mm[1])
 
     def draw(self, stream=None):
         """Ray-march ``self.volume`` into ``self.image`` with the current controls; returns it."""

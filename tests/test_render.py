@@ -193,6 +193,14 @@ def test_device_volume_at_a_larger_lattice_matches_the_oracle():
     want, vmin, vmax = R.rgba_volume(dens, field, (X, Y, Z))
     assert mm[0] == vmin and mm[1] == vmax
     assert np.array_equal(vol.cpu().numpy(), want)
+    # without a host pointer the call is asynchronous and leaves the extrema in scratch[0:2]
+    vol.zero_()
+    scratch.zero_()
+    _lib.call("sky_build_rgba_volume", _lib.i32p(pi), len(pi), _lib.dptr(dens_d), _lib.dptr(field_d),
+              _lib.dptr(scratch), scratch.numel(), _lib.dptr(vol, "float32"), None, _lib.stream_ptr())
+    torch.cuda.synchronize()
+    assert scratch[0].item() == vmin and scratch[1].item() == vmax
+    assert np.array_equal(vol.cpu().numpy(), want)
 
 
 @pytest.mark.gpu
