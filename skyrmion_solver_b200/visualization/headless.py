@@ -138,6 +138,18 @@ class HeadlessRenderer:
         self.hud_bottom_text = ""
 
     # -- binding and controls -------------------------------------------------
+    def bind_params(self, p_i, p_f, device=None) -> None:
+        """Attach a lattice by its packed parameters alone (e.g. a resident engine instance,
+        whose FP64 field and density come from ``Engine.view``)."""
+        class _Lattice:
+            pass
+        lat = _Lattice()
+        lat.p_i_h = np.asarray(p_i, np.int32)
+        lat.p_f_h = np.asarray(p_f, np.float64)
+        if device is not None:
+            self._device = device
+        self.bind_sim(lat)
+
     def bind_sim(self, sim) -> None:
         """Attach a simulation: device buffers for its lattice (on the device of its field) and
         the box aspect of its domain."""

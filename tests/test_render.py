@@ -379,3 +379,32 @@ def test_headless_run_viewer(tmp_path, short, mode):
     getattr(sim, want)()
     torch.cuda.synchronize()
     assert torch.equal(en, sim.en)
+
+
+@pytest.mark.gpu
+def test_renderer_draws_a_resident_engine_instance():
+    """Engine.view's FP64 buffers of a defect-corrected FP32 instance, drawn by a renderer bound
+    to the instance's parameters: the volume equals the oracle's volume of those buffers."""
+    import torch
+    from skyrmion_solver_b200 import theories as T
+    from skyrmion_solver_b200.engine import Engine
+    from skyrmion_solver_b200.theories._init_common import build_reference_field
+    th = T.by_short_name("nuclear")
+    p = th.params.default_params(xlen=36, ylen=30, zlen=33, lsx=0.2, lsy=0.2, lsz=0.2)
+    p_i, p_f = th.params.pack_device_params(p.resolved())
+    p_i, p_f = np.asarray(p_i, np.int32), np.asarray(p_f, np.float64)
+    F = torch.empty(int(p_i[7]), dtype=torch.float64, device="cuda")
+    build_reference_field("nuclear", p_i, p_f, {"mode": "rational_map", "baryon_number": 3}, F)
+    with Engine(0) as eng:
+        i = eng.add("nuclear", (p_i, p_f), F.cpu().numpy().reshape((4,) + tuple(int(v) for v in p_i[:3])),
+                    None, precision="fp32d")
+        eng.step(4)
+        field, en = eng.view(i, "baryon")
+        r = HeadlessRenderer(40, 30)
+        r.bind_params(p_i, p_f)
+        img = r.render(density_flat=en, field_flat=field)
+        torch.cuda.synchronize()
+        want, vmin, vmax = R.rgba_volume(en.cpu().numpy(), field.cpu().numpy(), tuple(int(v) for v in p_i[:3]))
+        assert r.extrema == (vmin, vmax)
+        assert np.array_equal(r.volume.cpu().numpy(), want)
+        assert _image_close(img.cpu().numpy(), R.render(want, inv_view_rows(), box=r.box_scale, width=40, height=30))
