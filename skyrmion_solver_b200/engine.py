@@ -232,6 +232,36 @@ class Engine:
                   _lib.dptr(field), _lib.stream_ptr(torch.cuda.current_stream(dev)))
         return field, en
 
+    def diagnostics(self, iid: int) -> dict:
+        """Centre of mass and RMS radius of an instance of any precision and, for the nuclear
+        model, its U, V and W inertia tensors, quadrupole tensor and D-term: the fused FP64
+        passes behind Simulation.compute_center_of_mass ... compute_D_term
+        (th/nuclear_skyrme/observables.py:182-487), run on the instance's FP64 field."""
+        import math
+        import numpy as np
+        import torch
+        from .core import observables as ob
+        m = self.meta[iid]
+        p_i, p_f = m["p_i"], m["p_f"]
+        dev = torch.device("cuda", self.device)
+        field = torch.empty(m["C"] * int(p_i[6]), dtype=torch.float64, device=dev)
+        torch.cuda.current_stream(dev).synchronize()
+        self.read_device(iid, field)
+        mom = ob._moments(m["theory"], field, None, p_i, p_f)
+        B = mom[0]
+        com = np.zeros(3) if abs(B) < 1.0e-30 else mom[1:4] / B
+        rms = 0.0
+        if abs(B) >= 1.0e-30:
+            num = mom[8] - 2.0 * float(np.dot(com, mom[5:8])) + float(np.dot(com, com)) * mom[4]
+            rms = math.sqrt(max(num / B, 0.0))
+        out = {"center_of_mass": com, "rms_radius": rms}
+        if m["theory"] == 0:
+            _, d = ob._nuclear_diag(0, field, None, p_i, p_f)
+            E = ob._total("sky_total_energy", 0, field, None, None, None, p_i, p_f)
+            out.update(U=ob._sym(d[0:6]), V=ob._sym(d[6:12]), W=d[12:21].reshape(3, 3).copy(),
+                       quadrupole=ob._sym(d[21:27]), D_term=-(2.0 / 5.0) * E * float(d[27]))
+        return out
+
     def time_stages(self, nsteps: int) -> dict:
         """Advance nsteps un-captured steps timing each launch kind with CUDA events (ms per step)."""
         out = (ctypes.c_double * 6)()

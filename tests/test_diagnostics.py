@@ -54,3 +54,29 @@ def test_device_diagnostics_match_the_oracle():
     torch.cuda.synchronize()
     assert _close(host(sim.com_d), O.center_of_mass(thd, F, p_i, p_f))
     assert not sim.en.any() and not sim.entmp.any()
+
+
+@pytest.mark.gpu
+def test_engine_diagnostics_of_a_resident_instance():
+    """Engine.diagnostics on a resident FP64 instance of the golden field gives the reference's
+    own values; on a defect-corrected FP32 instance it matches the oracle on the instance's field."""
+    import torch
+    from skyrmion_solver_b200.engine import Engine
+    d = _gold()
+    F, p_i, p_f = d["field"], d["p_i"], d["p_f"]
+    th = O.THEORIES["nuclear"]
+    with Engine(0) as eng:
+        i = eng.add("nuclear", (p_i, p_f), F, None, precision="fp64")
+        g = eng.diagnostics(i)
+        assert _close(g["center_of_mass"], d["com"]) and _close(g["rms_radius"], d["rms"])
+        for k, ref in (("U", "U"), ("V", "V"), ("W", "W"), ("quadrupole", "Q"), ("D_term", "D")):
+            assert _close(g[k], d[ref]), k
+        j = eng.add("nuclear", (p_i, p_f), F, None, precision="fp32d")
+        eng.step(3)
+        g = eng.diagnostics(j)
+        field, _ = eng.view(j)
+        torch.cuda.synchronize()
+        Fj = field.cpu().numpy().reshape(F.shape)
+        assert _close(g["center_of_mass"], O.center_of_mass(th, Fj, p_i, p_f))
+        assert _close(g["U"], O.u_tensor(th, Fj, p_i, p_f))
+        assert _close(g["D_term"], O.d_term(th, Fj, p_i, p_f))
