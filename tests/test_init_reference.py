@@ -216,3 +216,32 @@ def test_initialize_accepts_foreign_device_arrays(key):
     torch.cuda.synchronize()
     _check(short, p_i, p_f, field.cpu().numpy(), want)
     assert float(vel.abs().max()) == 0.0 and float(temp.abs().max()) == 0.0
+
+
+def test_lump_list_edge_cases():
+    """Host rules of the reference's initialize: Python rounding of the default smorgasbord count,
+    an unknown ansatz gives the vacuum, negative baryon numbers keep their sign in the lump (the
+    kernel rounds |B|), and the mode name is read case- and space-insensitively."""
+    from skyrmion_solver_b200.theories._init_common import reference_lumps
+    p_i = np.array([10, 10, 10, 2, 3, 4, 1000, 4000, 1, 1, 1, 1, 0, 0], np.int32)
+    p_f = np.array([1.8, 1.8, 1.8, 0.2, 0.2, 0.2, 0.008, 0.04, 1.0, 1.0, 2.5, 0.0])
+    lumps, vac = reference_lumps("nuclear", p_i, p_f, {"mode": "smorgasbord"})
+    assert vac and len(lumps) == 2                       # round(2.5) == 2 (round half to even)
+    lumps, vac = reference_lumps("nuclear", p_i, p_f, {"mode": "smorgasbord", "baryon_number": 3.5})
+    assert len(lumps) == 4
+    lumps, vac = reference_lumps("nuclear", p_i, p_f, {"ansatz": "torus"})
+    assert vac and len(lumps) == 0
+    lumps, vac = reference_lumps("nuclear", p_i, p_f, {"mode": " Rational_Map ", "baryon_number": -3})
+    assert not vac and lumps[0, 0] == 1.0 and lumps[0, 1] == -3.0
+    g, _ = I._grid(p_i, p_f)
+    F = I.initial_field("nuclear", p_i, p_f, {"mode": " Rational_Map ", "baryon_number": -3})
+    v = I._normalise(I.map_lump(g, lumps[0, 2:5], lumps[0, 5:8], lumps[0, 8:11], lumps[0, 1], lumps[0, 11],
+                                lumps[0, 12]))
+    assert np.array_equal(F[:4], v)
+    # theory profile lengths: omega 0.15 min(size), Coulomb 0.4 min(size) / max(|B|, 1)
+    size = np.array([1.8, 2.4, 3.0, 0.2, 0.2, 0.2, 0.008, 0.04, 1.0, 1.0, 2.0, 0.0])
+    pi5 = np.array([10, 10, 10, 2, 3, 5, 1000, 5000, 1, 1, 1, 4, 1, 0, 0], np.int32)
+    om, _ = reference_lumps("omega", pi5, size, {})
+    co, _ = reference_lumps("coulomb", pi5, size, {})
+    assert om[0, 11] == max(0.15 * 1.8, 1e-6) and co[0, 11] == max(0.4 * 1.8 / 2.0, 1e-6)
+    assert om[0, 0] == 0.0 and co[0, 0] == 0.0           # the parameters' hedgehog flag (p_i[12])
