@@ -184,14 +184,15 @@ int sky_build_rgba_volume(const int32_t* p_i, int32_t n_pi, const double* densit
 /* Replaces the viewer's ray-march fragment shader
  * (visualization/gl_backend.py:519-710) without a graphics API: image[(row *
  * width + col) * 4 + c] (FP32 RGBA, row 0 at the top) from the volume above
- * (xlen * ylen * zlen texels, trilinear, clamp to edge).  params (host, 23
- * floats): the three inverse-view rows (12), box scale (3), zoom, brightness,
- * levelset, density min, density max, transfer scale, opacity scale, tstep.
+ * (xlen * ylen * zlen texels, trilinear, clamp to edge).  params (host,
+ * n_params >= 23 floats): the three inverse-view rows (12), box scale (3), zoom,
+ * brightness, levelset, density min, density max, transfer scale, opacity scale,
+ * tstep.
  * color_mode 0 uses the viewer's nine-entry transfer table; any other value
  * the pion vector's HSL colour.  Rays that miss the box give (1, 1, 1, 1). */
 int sky_render_volume(const float* volume, int32_t xlen, int32_t ylen, int32_t zlen, const float* params,
-                      int32_t max_steps, int32_t color_mode, int32_t width, int32_t height, float* image,
-                      void* stream);
+                      int32_t n_params, int32_t max_steps, int32_t color_mode, int32_t width, int32_t height,
+                      float* image, void* stream);
 
 /* Replace compute_sum / compute_max (core/utils.py:201-279, 321-373):
  * deterministic FP64 reductions (compensated sum; signed max).  `scratch` is a

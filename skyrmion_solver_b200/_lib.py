@@ -81,7 +81,7 @@ SIGNATURES = {
     "sky_init_lumps": ([_I32P, _I32, _F64P, _I32, _I32, _F64P, _I32, _P, _P], _I),
     "sky_volume_scratch_size": ([], _I64),
     "sky_build_rgba_volume": ([_I32P, _I32, _P, _P, _P, _I64, _P, _F64P, _P], _I),
-    "sky_render_volume": ([_P, _I32, _I32, _I32, _F32P, _I32, _I32, _I32, _I32, _P, _P], _I),
+    "sky_render_volume": ([_P, _I32, _I32, _I32, _F32P, _I32, _I32, _I32, _I32, _I32, _P, _P], _I),
     "sky_engine_create": ([_I, ctypes.POINTER(ctypes.c_void_p)], _I),
     "sky_engine_destroy": ([_P], _I),
     "sky_engine_add": ([_P, _I, _I32P, _I32, _F64P, _I32, _I, _P, _P, _I, ctypes.POINTER(_I)], _I),

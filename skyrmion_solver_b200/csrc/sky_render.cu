@@ -297,9 +297,10 @@ int sky_build_rgba_volume(const int32_t* p_i, int32_t n_pi, const double* densit
 }
 
 int sky_render_volume(const float* volume, int32_t xlen, int32_t ylen, int32_t zlen, const float* params,
-                      int32_t max_steps, int32_t color_mode, int32_t width, int32_t height, float* image,
-                      void* stream) {
+                      int32_t n_params, int32_t max_steps, int32_t color_mode, int32_t width, int32_t height,
+                      float* image, void* stream) {
     if (!volume || !params || !image) return invalid("null buffer");
+    if (n_params < 23) return invalid("the shader parameters are 23 floats");
     if (reinterpret_cast<uintptr_t>(volume) % 16 || reinterpret_cast<uintptr_t>(image) % 16)
         return invalid("the volume and the image must be 16-byte aligned");
     if (xlen < 1 || ylen < 1 || zlen < 1 || width < 1 || height < 1) return invalid("empty volume or image");

@@ -263,7 +263,7 @@ class HeadlessRenderer:
             raise RuntimeError("bind_sim(sim) first")
         X, Y, Z = self._dims
         prm = self.shader_params()
-        _lib.call("sky_render_volume", _lib.dptr(self.volume, "float32"), X, Y, Z, _lib.f32p(prm),
+        _lib.call("sky_render_volume", _lib.dptr(self.volume, "float32"), X, Y, Z, _lib.f32p(prm), len(prm),
                   int(self.max_steps), int(self.color_mode), self.width, self.height,
                   _lib.dptr(self.image, "float32"), _lib.stream_ptr(stream))
         return self.image

@@ -120,16 +120,17 @@ def test_volume_and_render_reject_bad_arguments():
     prm = np.zeros(23, np.float32)
     prm[12:15] = 1.0
     prm[22] = 0.002
-    args = (dummy, 8, 8, 8, _lib.f32p(prm))
+    args = (dummy, 8, 8, 8, _lib.f32p(prm), 23)
     assert lib.sky_render_volume(*args, 100, 0, 0, 10, dummy, None) == 1    # empty image
     assert lib.sky_render_volume(*args, -1, 0, 10, 10, dummy, None) == 1    # negative step count
     assert lib.sky_render_volume(*args, 100, 0, 10, 10, None, None) == 1    # null image
+    assert lib.sky_render_volume(dummy, 8, 8, 8, _lib.f32p(prm), 22, 100, 0, 10, 10, dummy, None) == 1
     bad = prm.copy()
     bad[22] = 0.0
-    assert lib.sky_render_volume(dummy, 8, 8, 8, _lib.f32p(bad), 100, 0, 10, 10, dummy, None) == 1
+    assert lib.sky_render_volume(dummy, 8, 8, 8, _lib.f32p(bad), 23, 100, 0, 10, 10, dummy, None) == 1
     bad = prm.copy()
     bad[13] = 0.0
-    assert lib.sky_render_volume(dummy, 8, 8, 8, _lib.f32p(bad), 100, 0, 10, 10, dummy, None) == 1
+    assert lib.sky_render_volume(dummy, 8, 8, 8, _lib.f32p(bad), 23, 100, 0, 10, 10, dummy, None) == 1
 
 
 # ---------------------------------------------------------------------------
@@ -149,8 +150,8 @@ def _draw(vol, rows, box=(1.0, 1.0, 1.0), zoom=5.5, brightness=6.0, levelset=0.2
     prm = np.concatenate([np.asarray(rows, np.float32).ravel(), np.asarray(box, np.float32),
                           np.asarray([zoom, brightness, levelset, dmin, dmax, transfer_scale, opacity_scale, tstep],
                                      np.float32)]).astype(np.float32)
-    _lib.call("sky_render_volume", _lib.dptr(v, "float32"), X, Y, Z, _lib.f32p(prm), max_steps, color_mode, width,
-              height, _lib.dptr(img, "float32"), _lib.stream_ptr())
+    _lib.call("sky_render_volume", _lib.dptr(v, "float32"), X, Y, Z, _lib.f32p(prm), len(prm), max_steps,
+              color_mode, width, height, _lib.dptr(img, "float32"), _lib.stream_ptr())
     torch.cuda.synchronize()
     return img.cpu().numpy()
 
