@@ -134,13 +134,23 @@ __device__ __forceinline__ void lin_axis(float s, int n, int& i0, int& i1, float
     i1 = min(max(i + 1, 0), n - 1);
 }
 
-__device__ __forceinline__ float4 sample3(const float4* __restrict__ v, int X, int Y, int Z, float sx, float sy,
-                                          float sz) {
+// Texel indices and weight along one axis from the texel-space coordinate u = s n - 1/2.
+__device__ __forceinline__ void lin_texel(float u, int n, int& i0, int& i1, float& w) {
+    const float f = floorf(u);
+    w = u - f;
+    const int i = (int)f;
+    i0 = min(max(i, 0), n - 1);
+    i1 = min(max(i + 1, 0), n - 1);
+}
+
+// Trilinear lookup at texel-space coordinates (ux, uy, uz).
+__device__ __forceinline__ float4 sample3(const float4* __restrict__ v, int X, int Y, int Z, float ux, float uy,
+                                          float uz) {
     int x0, x1, y0, y1, z0, z1;
     float wx, wy, wz;
-    lin_axis(sx, X, x0, x1, wx);
-    lin_axis(sy, Y, y0, y1, wy);
-    lin_axis(sz, Z, z0, z1, wz);
+    lin_texel(ux, X, x0, x1, wx);
+    lin_texel(uy, Y, y0, y1, wy);
+    lin_texel(uz, Z, z0, z1, wz);
     auto at = [&](int x, int y, int z) { return v[((int64_t)z * Y + y) * X + x]; };
     float4 c[8] = {at(x0, y0, z0), at(x1, y0, z0), at(x0, y1, z0), at(x1, y1, z0),
                    at(x0, y0, z1), at(x1, y0, z1), at(x0, y1, z1), at(x1, y1, z1)};
@@ -152,14 +162,14 @@ __device__ __forceinline__ float4 sample3(const float4* __restrict__ v, int X, i
     return lerp4(lerp4(c00, c10, wy), lerp4(c01, c11, wy), wz);
 }
 
-__device__ __forceinline__ float4 transfer(float s) {
+// The transfer table is read from a shared-memory copy: lanes index different entries,
+// which the constant cache would serialise.
+__device__ __forceinline__ float4 transfer(const float4* tf, float s) {
     int i0, i1;
     float w;
     lin_axis(s, 9, i0, i1, w);
-    const float* a = c_transfer[i0];
-    const float* b = c_transfer[i1];
-    return make_float4(a[0] + (b[0] - a[0]) * w, a[1] + (b[1] - a[1]) * w, a[2] + (b[2] - a[2]) * w,
-                       a[3] + (b[3] - a[3]) * w);
+    const float4 a = tf[i0], b = tf[i1];
+    return make_float4(a.x + (b.x - a.x) * w, a.y + (b.y - a.y) * w, a.z + (b.z - a.z) * w, a.w + (b.w - a.w) * w);
 }
 
 // pionVectorToRGB (gl_backend.py:573-592): HSL with saturation 1, lightness from n_z
@@ -185,6 +195,10 @@ __device__ __forceinline__ float3 pion_rgb(float nx, float ny, float nz) {
 
 __global__ void k_render(const float4* __restrict__ vol, int X, int Y, int Z, RenderParams rp,
                          float4* __restrict__ img) {
+    __shared__ float4 tf[9];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid < 9) tf[tid] = make_float4(c_transfer[tid][0], c_transfer[tid][1], c_transfer[tid][2], c_transfer[tid][3]);
+    __syncthreads();
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int row = blockIdx.y * blockDim.y + threadIdx.y;
     if (px >= rp.width || row >= rp.height) return;
@@ -216,7 +230,10 @@ __global__ void k_render(const float4* __restrict__ vol, int X, int Y, int Z, Re
     float t = tnear;
     float p0 = ox + dx * tnear, p1 = oy + dy * tnear, p2 = oz + dz * tnear;
     const float st0 = dx * rp.tstep, st1 = dy * rp.tstep, st2 = dz * rp.tstep;
-    const float denom = fmaxf(rp.dmax - rp.dmin, 1.0e-30f);
+    const float inv_denom = 1.0f / fmaxf(rp.dmax - rp.dmin, 1.0e-30f);
+    // texel-space coordinate per axis: ((p / b) / 2 + 1/2) n - 1/2 = p (n / 2b) + (n - 1) / 2
+    const float kx = 0.5f * (float)X / bx, ky = 0.5f * (float)Y / by, kz = 0.5f * (float)Z / bz;
+    const float cx = 0.5f * (float)(X - 1), cy = 0.5f * (float)(Y - 1), cz = 0.5f * (float)(Z - 1);
     for (int i = 0; i < rp.max_steps; ++i) {
         // box edges are drawn black
         const float e0 = fminf(fabsf(p0 + bx), fabsf(p0 - bx));
@@ -227,14 +244,13 @@ __global__ void k_render(const float4* __restrict__ vol, int X, int Y, int Z, Re
             *out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
             return;
         }
-        const float4 sv = sample3(vol, X, Y, Z, (p0 / bx) * 0.5f + 0.5f, (p1 / by) * 0.5f + 0.5f,
-                                  (p2 / bz) * 0.5f + 0.5f);
-        const float norm = (sv.x - rp.dmin) / denom;
+        const float4 sv = sample3(vol, X, Y, Z, p0 * kx + cx, p1 * ky + cy, p2 * kz + cz);
+        const float norm = (sv.x - rp.dmin) * inv_denom;
         float inp = (norm - rp.levelset) * rp.tscale;
         if (inp < 0.0f) inp = 0.0f;
         float cr, cg, cb, ca;
         if (rp.color_mode == 0) {
-            const float4 c = transfer(fminf(fmaxf(norm, 0.0f), 1.0f));
+            const float4 c = transfer(tf, fminf(fmaxf(norm, 0.0f), 1.0f));
             cr = c.x, cg = c.y, cb = c.z, ca = c.w * rp.oscale;
         } else {
             const float3 rgb = pion_rgb(sv.y, sv.z, sv.w);
