@@ -285,7 +285,9 @@ def run_reference(args):
     cb = cpu_baseline()
     N = L ** 3
     steps_per_s = cb["site_steps_per_s"] / N
-    s64 = cal["fp64_steps_to_converge"] if cal else None
+    # the plain FP64 solve to max|g| <= 1e-6 takes 119,000 steps (FP64 engine on a B200; the CPU port runs
+    # the same arithmetic, so the same step count), far more than a CPU run can time
+    s64 = cal["fp64_total_steps"] if cal else None
     value = steps_per_s / s64 if s64 else None
     emit({"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
@@ -302,7 +304,45 @@ def run_reference(args):
 # our arm
 # ---------------------------------------------------------------------------
 
+def solve_to_tolerance(eng, iid, stream, chunk, max_steps, tol=GRAD_TOL):
+    """Advance instance `iid` in chunks of `chunk` steps, reading its latest statistics (one
+    64-byte device->host read) after each chunk, until max|g| <= tol; a defect-corrected or
+    compensated FP32 instance whose gradient stops improving by 1 % over 16,384 steps switches to
+    FP64 first (the serving rule).  Returns (stats, steps, fp32 steps, device ms, wall s)."""
+    import torch
+    from skyrmion_solver_b200.serving import PlateauRule
+    rule = PlateauRule(tol)
+    prec = eng.meta[iid]["precision"]
+    fp32_steps = 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    n = 0
+    st = eng.stats(iid)
+    while n < max_steps:
+        eng.step(chunk)
+        n += chunk
+        st = eng.stats(iid)
+        if not math.isfinite(st.energy):
+            break
+        if prec == "fp64" or eng.meta[iid]["precision"] == "fp64":
+            if st.gabs <= tol:
+                break
+        elif st.gabs <= tol:
+            break
+        elif rule.update(st.gabs, chunk):
+            eng.set_precision(iid, "fp64")
+            fp32_steps = n
+    ev1.record(stream)
+    ev1.synchronize()
+    wall = time.perf_counter() - t0
+    if eng.meta[iid]["precision"] != "fp64":
+        fp32_steps = n
+    return st, n, fp32_steps, ev0.elapsed_time(ev1), wall
+
+
 def run_ours(args):
+    import ctypes
     import numpy as np
     import torch
     from skyrmion_solver_b200.core.simulation import Simulation
@@ -318,24 +358,23 @@ def run_ours(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
         pg = dist
     warmup = max(3, args.warmup)
     K = args.steps
     th, p, p_i, p_f = workload_params()
     C, N = int(p_i[5]), int(p_i[6])
     field = workload_field_device(p_i, p_f, dev)
-    cal = load_calibration()
-
-    eng = Engine(local)
-    iid = eng.add("omega", (p_i, p_f), field, None, precision=FAST)
-    stream = torch.cuda.ExternalStream(eng.stream, device=dev)
 
     def barrier():
         if pg is not None:
             pg.barrier()
         torch.cuda.synchronize()
 
+    # ---- K timed steps of the resident engine (inputs resident in HBM) ----
+    eng = Engine(local)
+    iid = eng.add("omega", (p_i, p_f), field, None, precision=FAST)
+    stream = torch.cuda.ExternalStream(eng.stream, device=dev)
     eng.step(warmup)
     clocks = ClockSampler(local)
     time.sleep(0.3)
@@ -346,26 +385,24 @@ def run_ours(args):
     eng.step(K)
     ev1.record(stream)
     ev1.synchronize()
-    clocks.mark_end()
+    clocks.mark_end()     # moved to the end of the solves below when they run
     barrier()
-    ms = ev0.elapsed_time(ev1)
-    clk = clocks.stop()
-    ms = max_over_ranks([ms], device=dev)[0]      # the job is as slow as its slowest GPU
+    ms = max_over_ranks([ev0.elapsed_time(ev1)], device=dev)[0]   # the job is as slow as its slowest GPU
     ms_step = ms / K
-    steps_per_s = 1e3 / ms_step
     launches = eng.launches_per_step * K
-    st = eng.stats(iid)
 
     # per-launch-kind timing (CUDA events on the engine stream, un-captured launches)
     stages = eng.time_stages(max(5, min(50, K)))
     dom = max(("stage1", "stage2", "stage3", "stage4"), key=lambda k: stages[k])
-    alg_bytes = stage_passes(dom, FAST) * C * 4 * N
+    alg_bytes = STAGE_PASSES[dom] * C * 4 * N                 # minimal fused schedule: 16 C s per step
+    fmt_bytes = stage_passes(dom, FAST) * C * 4 * N           # with the compensated format's extra arrays
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (stages[dom] * 1e-3) / 1e9
-    step_bytes = sum(stage_passes(k, FAST) for k in STAGE_PASSES) * C * 4 * N
+    step_bytes = sum(STAGE_PASSES.values()) * C * 4 * N
     traffic = load_traffic(dom)
+    eng.close()
 
-    # plain FP64 drop-in path (reference layout, sky_arrested_newton_step) on the same field
+    # ---- plain FP64 drop-in path (reference layout, sky_arrested_newton_step), K steps ----
     sim = Simulation(p, th)
     sim.Field.copy_(field)
     sim.Velocity.zero_()
@@ -382,111 +419,126 @@ def run_ours(args):
         e, _ = sim.step(e)
     t1.record(cur)
     t1.synchronize()
-    plain_ms = t0.elapsed_time(t1) / nplain
+    plain_ms = max_over_ranks([t0.elapsed_time(t1) / nplain], device=dev)[0]
     del sim
 
-    # engine in FP64 (for the FP64 polishing phase and the calibration)
-    e64 = Engine(local)
-    i64 = e64.add("omega", (p_i, p_f), field, None, precision="fp64")
-    e64.step(3)
-    s64t = torch.cuda.ExternalStream(e64.stream, device=dev)
-    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a0.record(s64t)
-    e64.step(max(8, min(64, K)))
-    a1.record(s64t)
-    a1.synchronize()
-    eng64_ms = a0.elapsed_time(a1) / max(8, min(64, K))
-    e64.close()
+    solve = None
+    ref = None
+    if not args.quick:
+        # ---- the headline: one complete solve through the public API, host buffers in and out ----
+        host = torch.empty(C * N, dtype=torch.float64, pin_memory=True)
+        host.copy_(field)
+        host_np = host.numpy().reshape((C, L, L, L))
+        out_pin = torch.empty(C * N, dtype=torch.float64, pin_memory=True)
+        out_np = out_pin.numpy().reshape((C, L, L, L))
+        barrier()
+        tw0 = time.perf_counter()
+        ee = Engine(local)
+        j = ee.add("omega", (p_i, p_f), host_np, None, precision=FAST)
+        t_admit = time.perf_counter() - tw0
+        es = torch.cuda.ExternalStream(ee.stream, device=dev)
+        st, nsteps, n32, dev_ms, _ = solve_to_tolerance(ee, j, es, args.chunk, args.max_steps)
+        tr = time.perf_counter()
+        ee._call("sky_engine_read", j, ctypes.c_void_p(out_np.ctypes.data), None, 0)
+        t_down = time.perf_counter() - tr
+        wall = time.perf_counter() - tw0
+        ee.close()
+        barrier()
+        solve = dict(stats=st, steps=nsteps, fp32_steps=n32, dev_s=dev_ms * 1e-3, wall_s=wall, admit_s=t_admit,
+                     download_s=t_down)
+        # ---- the plain-FP64 reference solve of the same field (resident FP64 engine) ----
+        e64 = Engine(local)
+        i64 = e64.add("omega", (p_i, p_f), field, None, precision="fp64")
+        s64t = torch.cuda.ExternalStream(e64.stream, device=dev)
+        st64, n64, _, dev64_ms, wall64 = solve_to_tolerance(e64, i64, s64t, args.chunk, args.max_steps)
+        e64.close()
+        ref = dict(stats=st64, steps=n64, dev_s=dev64_ms * 1e-3, wall_s=wall64)
+        clocks.mark_end()
 
-    # end to end through the public API, one solve's worth: admission from a pinned host FP64 field,
-    # per-step host read of (E, B, err) in both phases, the precision switch, and the final field
-    # download into pinned host memory; each piece timed, then combined over the calibrated steps
-    host = torch.empty(C * N, dtype=torch.float64, pin_memory=True)
-    host.copy_(field)
-    host_np = host.numpy().reshape((C, L, L, L))
-    out_pin = torch.empty(C * N, dtype=torch.float64, pin_memory=True)
-    out_np = out_pin.numpy().reshape((C, L, L, L))
-    K64 = max(8, min(256, K))
-    barrier()
-    tw = [time.perf_counter()]
-    ee = Engine(local)
-    j = ee.add("omega", (p_i, p_f), host_np, None, precision=FAST)
-    tw.append(time.perf_counter())                       # admission
-    for _ in range(K):
-        ee.step(1)
-        ee.stats(j)
-    tw.append(time.perf_counter())                       # K fp32c steps
-    ee.set_precision(j, "fp64")
-    tw.append(time.perf_counter())                       # switch
-    for _ in range(K64):
-        ee.step(1)
-        ee.stats(j)
-    tw.append(time.perf_counter())                       # K64 FP64 steps
-    ee._call("sky_engine_read", j, __import__("ctypes").c_void_p(out_np.ctypes.data), None, 0)
-    tw.append(time.perf_counter())                       # download
-    ee.close()
-    t_up, t32, t_sw, t64, t_down = max_over_ranks([tw[i + 1] - tw[i] for i in range(5)], device=dev)
-    e2e32_ms = t32 * 1e3 / K
-    e2e64_ms = t64 * 1e3 / K64
+    def ok(r):
+        return r is not None and math.isfinite(r["stats"].energy) and r["stats"].gabs <= GRAD_TOL
+
+    value = e2e_value = solve_s = None
+    final = None
+    if solve is not None:
+        dev_s, wall_s = max_over_ranks([solve["dev_s"], solve["wall_s"]], device=dev)
+        s = solve["stats"]
+        final = {"energy": s.energy, "baryon": s.baryon, "max_abs_gradient": s.gabs, "steps": solve["steps"],
+                 "fp32_steps": solve["fp32_steps"], "converged": ok(solve)}
+        if ok(ref):
+            r = ref["stats"]
+            final.update(reference={"schedule": "fp64 engine to max|g| <= %g" % GRAD_TOL, "energy": r.energy,
+                                    "baryon": r.baryon, "max_abs_gradient": r.gabs, "steps": ref["steps"]},
+                         rel_energy_error=abs(s.energy - r.energy) / abs(r.energy),
+                         baryon_error=abs(s.baryon - r.baryon),
+                         max_abs_gradient_error=abs(s.gabs - r.gabs))
+            final["within_tolerance"] = bool(final["rel_energy_error"] <= REL_ENERGY_TOL and
+                                             final["baryon_error"] <= 1e-4 and ok(solve))
+        if ok(solve):
+            value = world / dev_s
+            e2e_value = world / wall_s
+            solve_s = wall_s
+    plain = {"ms_per_step": plain_ms}
+    if ref is not None:
+        eng64_dev_s = max_over_ranks([ref["dev_s"]], device=dev)[0]
+        plain.update(engine_fp64_solve_s=eng64_dev_s, engine_fp64_steps=ref["steps"],
+                     engine_fp64_solves_per_s=world / eng64_dev_s if ok(ref) else None,
+                     engine_fp64_ms_per_step=1e3 * eng64_dev_s / ref["steps"],
+                     solves_per_s=world / (ref["steps"] * plain_ms * 1e-3) if ok(ref) else None,
+                     note="the drop-in path runs the FP64 engine's arithmetic in the reference layout; its "
+                          "solve takes the FP64 engine's observed step count at its own timed step rate")
+        if value and plain.get("solves_per_s"):
+            plain["speedup"] = value / plain["solves_per_s"]
+            plain["speedup_vs_engine_fp64"] = value / plain["engine_fp64_solves_per_s"]
     field_bytes = C * N * 8
-    s32 = cal.get(f"{SCHEDULE}_fp32_steps") if cal else None
-    s64p = cal.get(f"{SCHEDULE}_fp64_steps") if cal else None
-    s64 = cal.get("fp64_steps_to_converge") if cal else None
-    have = s32 is not None and s64p is not None
-
-    solve_s = (s32 * ms_step + s64p * eng64_ms) * 1e-3 if have else None
-    value = world / solve_s if have else None
-    e2e_solve_s = (t_up + s32 * e2e32_ms * 1e-3 + t_sw + s64p * e2e64_ms * 1e-3 + t_down) if have else None
-    e2e_value = world / e2e_solve_s if have else None
-    plain_value = world / (s64 * plain_ms * 1e-3) if s64 else None
-    eng64_value = world / (s64 * eng64_ms * 1e-3) if s64 else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "theory": "omega (C=5)", "sites": N, "instances_per_gpu": 1,
-                   "precision": f"timed steps: {FAST} (FP32 stencils, compensated hi+lo FP32 field"
+                   "precision": f"{FAST}: FP32 stencils, compensated hi+lo FP32 field"
                                 + (", FP64 defect correction every 16 steps" if FAST == "fp32d" else "")
-                                + "; FP64 compensated energy/baryon/arrest); schedule: that phase, then FP64 "
-                                  "to max|g| <= 1e-6",
+                                + "; FP64 compensated energy/baryon/arrest; FP64 phase only if the FP32 "
+                                  "phase stalls",
                    "dt": DT_FACTOR * H, "couplings": COUPLINGS,
-                   "steps_to_converge": {FAST: s32, "fp64_check": s64p, "plain_fp64": s64},
-                   "convergence": f"energy stays within {REL_ENERGY_TOL:g} rel. of the plain-FP64 energy at "
-                                  f"max|g| <= {GRAD_TOL:g} (profiles/convergence_omega_B4_128.json)",
+                   "solve": f"arrested Newton flow from the initial field until max|g| <= {GRAD_TOL:g}, "
+                            f"checked every {args.chunk} steps; value = 1 / device time of the solve's steps, "
+                            "e2e = 1 / wall time of Engine.add (pinned host field) + the steps + per-chunk "
+                            "statistics reads + the final field read into pinned host memory",
                    "l2": f"no flush: resident state {9 * C * N * 4 / 1e6:.0f} MB > 126 MB L2",
                    "parallelism": f"replicas x{world}"},
-        "latency_s": {"p50": solve_s, "p99": solve_s, "note": "one resident solve per GPU: every solve takes "
-                      "the same time; the serving mode (--serve) reports p50/p99 over a request stream"},
-        "site_steps_per_s": world * N * steps_per_s,
-        "hbm_gbs_step": step_bytes / (ms_step * 1e-3) / 1e9,
-        "roofline": {"bound": "hbm", "kernel": f"k_march_stage<Omega,float,{dom[-1]}>" + (" + k_march_defect" if dom == "stage1" and FAST == "fp32d" else ""), "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+        "latency_s": {"p50": solve_s, "p99": solve_s, "note": "one resident solve per GPU; the serving mode "
+                      "(--serve) reports p50/p99 over a request stream"},
+        "final": final,
+        "steps_rate": {"ms_per_step": ms_step, "site_steps_per_s": world * N * 1e3 / ms_step,
+                       "hbm_gbs_step": step_bytes / (ms_step * 1e-3) / 1e9},
+        "roofline": {"bound": "hbm", "kernel": f"k_march_stage<Omega,float,{dom[-1]}>"
+                     + (" + k_march_defect" if dom == "stage1" and FAST == "fp32d" else ""),
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                     "format_bytes_per_launch": fmt_bytes, "format_achieved": fmt_bytes / (stages[dom] * 1e-3) / 1e9,
                      "issue_active": load_issue_active(dom),
-                     "note": "the stencil stages are issue-bound, not HBM-bound: issue_active is the ncu "
-                             "fraction of scheduler cycles that issued (profiles/ncu_stage1_fp32d_omega128.md)",
+                     "note": "algorithmic bytes: the minimal fused schedule's passes of one C-component FP32 "
+                             "field (stage 1: 2, stage 2: 3, stage 3: 4, stage 4: 7); format bytes add the "
+                             "compensated field's low parts and the defect correction",
                      "launch_ms": stages[dom], "stage_ms": stages},
-        "plain_fp64": {"ms_per_step": plain_ms, "solves_per_s": plain_value, "steps_to_converge": s64,
-                       "engine_fp64_ms_per_step": eng64_ms, "engine_fp64_solves_per_s": eng64_value,
-                       "speedup": (value / plain_value) if (value and plain_value) else None},
+        "plain_fp64": plain,
         "e2e": {"value": e2e_value, "unit": UNIT,
-                "h2d_bytes_per_step": field_bytes / (s32 + s64p) if have else None,
-                "d2h_bytes_per_step": (48 * (s32 + s64p) + field_bytes) / (s32 + s64p) if have else None,
-                "ms_per_step": {FAST: e2e32_ms, "fp64": e2e64_ms},
-                "seconds": {"admit": t_up, "switch": t_sw, "download": t_down, "solve": e2e_solve_s},
-                "path": "Engine.add(pinned host FP64 field) + S32 x (Engine.step(1) + Engine.stats) + "
-                        "set_precision(fp64) + S64 x (step + stats) + field read into pinned memory; "
-                        "per-step times from K and K64 timed steps"},
+                "h2d_bytes_per_step": field_bytes / solve["steps"] if solve else None,
+                "d2h_bytes_per_step": (64 * (solve["steps"] // args.chunk + 1) + field_bytes) / solve["steps"]
+                if solve else None,
+                "seconds": {"admit": solve["admit_s"], "download": solve["download_s"], "solve": solve["wall_s"]}
+                if solve else None},
         "gpu_launches": launches,
-        "clocks": clk,
-        "final": {"energy": st.energy, "baryon": st.baryon, "max_abs_gradient": st.gabs, "step": st.step},
+        "clocks": clocks.stop(),
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline()
-        cval = cb["site_steps_per_s"] / N / s64 if s64 else None   # the CPU arm runs the plain FP64 schedule
+        nref = ref["steps"] if ok(ref) else None
+        cval = cb["site_steps_per_s"] / N / nref if nref else None   # the CPU arm runs the plain FP64 schedule
         line["cpu_baseline"] = {"value": cval, "unit": UNIT, "cores": cb["cores"], "kind": "port",
-                                "sample": cb["sample"], "site_steps_per_s": cb["site_steps_per_s"]}
-    eng.close()
+                                "sample": cb["sample"], "site_steps_per_s": cb["site_steps_per_s"],
+                                "steps_per_solve": nref}
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
@@ -915,6 +967,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--quick", action="store_true", help="skip the two timed solves (K-step rate only)")
+    ap.add_argument("--chunk", type=int, default=128, help="steps between convergence checks of a solve")
     ap.add_argument("--calibrate", action="store_true")
     ap.add_argument("--max-steps", type=int, default=240000)
     ap.add_argument("--out", default=None)

@@ -243,10 +243,12 @@ int sky_arrested_newton_step(int theory, const int32_t* p_i, int32_t n_pi, const
  * (they synchronise the device) between frames.  The eight RK4 slopes, the
  * stage field and the reduction scratch live in a 16 MiB static device array
  * that every GPU loading the library holds until exit, so the lattice is
- * limited to C*N <= 232488 values (e.g. 36^3 sites at C = 5); larger lattices
+ * limited to C*N <= 232488 values (e.g. 35^3 sites at C = 5); larger lattices
  * are rejected with SKY_ERR_INVALID before anything is launched.  The array's
- * device address is looked up on the first call on each device, so make that
- * first call before any stream capture.  All calls share the array: calls
+ * device address is looked up on the first call on each device, and again on
+ * the first call after the device's context was re-created (cudaDeviceReset
+ * reloads the library's module), so make that first call before any stream
+ * capture.  All calls share the array: calls
  * that overlap on the GPU (other streams, other threads) race.  The slopes are
  * not returned; velocity, field and energy_gradient are updated as by
  * sky_arrested_newton_step, and the new energy and err go to host pointers. */

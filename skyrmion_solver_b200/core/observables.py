@@ -124,10 +124,11 @@ def _sym(v6):
     return np.array([[a, b, c], [b, d, e], [c, e, f]], dtype=np.float64)
 
 
-def _nuclear_diag(theory_id, Field, gridsum_partial, p_i, p_f):
-    """(centre of mass, the 28 fused sums of sky_nuclear_diagnostics)."""
+def _nuclear_diag(theory_id, Field, gridsum_partial, p_i, p_f, moments=None):
+    """(centre of mass, the 28 fused sums of sky_nuclear_diagnostics).  `moments`: the nine
+    baryon moments of the same field when the caller already has them (sky_baryon_moments)."""
     import numpy as np
-    m = _moments(theory_id, Field, gridsum_partial, p_i, p_f)
+    m = _moments(theory_id, Field, gridsum_partial, p_i, p_f) if moments is None else moments
     com = np.zeros(3) if abs(m[0]) < 1.0e-30 else m[1:4] / m[0]
     hi, hf = host_params(p_i, p_f)
     scratch = pick_scratch(gridsum_partial)

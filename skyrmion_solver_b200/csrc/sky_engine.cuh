@@ -77,7 +77,7 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
                                               const T (&v0)[C], const T (&l1)[C], const T (&l2)[C],
                                               const T (&l3)[C], const T (&g)[C], T dtt, int nsky, int unit_length,
                                               S* __restrict__ Fo, S* __restrict__ Flo_out, S* __restrict__ Vo,
-                                              double& v2) {
+                                              T& v2) {
     T vv[C], inc[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
@@ -110,12 +110,12 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
             for (int c = 0; c < C; ++c)
                 if (c < nsky) vv[c] -= lm * fv[c];
         }
-        v2 = 0.0;
+        v2 = T(0);
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             Fo[c * N + s] = S(fv[c]);
             Vo[c * N + s] = S(vv[c]);
-            v2 += double(vv[c]) * double(vv[c]);
+            v2 += vv[c] * vv[c];
         }
     } else {
         // hi + lo + inc in FP64, with the two small terms summed in FP32 first: lo and the
@@ -154,13 +154,12 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
             for (int c = 0; c < C; ++c)
                 if (c < nsky) vv[c] -= lm * hi[c];
         }
-        T vs = T(0);
+        v2 = T(0);
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             Vo[c * N + s] = S(vv[c]);
-            vs += vv[c] * vv[c];
+            v2 += vv[c] * vv[c];
         }
-        v2 = double(vs);
     }
 }
 
@@ -171,7 +170,7 @@ __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __r
                                               const S* __restrict__ L1, const S* __restrict__ L2,
                                               const S* __restrict__ L3, const T (&g)[C], T dtt, int nsky,
                                               int unit_length, S* __restrict__ Fo, S* __restrict__ Flo_out,
-                                              S* __restrict__ Vo, double& v2) {
+                                              S* __restrict__ Vo, T& v2) {
     T f0[C], flo[C], v0[C], a1[C], a2[C], a3[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
@@ -274,9 +273,13 @@ struct EngineEpi {
     T dtt;
     int nsky;
     int unit_length;
-    double gmx, gab;
-    double hvol;  // h^3 / 2
-    KSum kin;     // (1/2) h^3 sum |V'|^2 over the sites of the tile
+    T gmx, gab;   // signed and absolute maxima of the thread's stage-4 gradients (exact in T)
+    T hvol;       // h^3 / 2
+    // (1/2) h^3 sum |V'|^2 over the thread's sites: compensated FP64 for an FP64 instance; an
+    // FP32 instance's per-site |V'|^2 is an FP32 value and its thread partial (at most one
+    // x-chunk of sites) is summed in FP32, then merged per block in FP64
+    KSum kin;
+    T kin_t;
     T* dlt;       // defect correction (null unless defect-corrected)
     int refresh;  // stage 1 of a refresh step: dlt holds g64 of the field; replace it by g64 - g32
     template <int C>
@@ -309,14 +312,23 @@ struct EngineEpi {
         }
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            const double gd = double(g[c]);
-            gmx = fmax(gmx, gd);
-            gab = fmax(gab, fabs(gd));
+            gmx = fmax(gmx, g[c]);
+            gab = fmax(gab, fabs(g[c]));
         }
-        double v2;
+        T v2;
         finalize_site<T, T, C>(s, N, fin_src[0], fin_src[1], fin_src[2], fin_src[3], fin_src[4], fin_src[5], g, dtt,
                                nsky, unit_length, out0, Flo_out, out1, v2);
-        ksum_add(kin, hvol * v2);
+        if constexpr (sizeof(T) == 8)
+            ksum_add(kin, hvol * v2);
+        else
+            kin_t += hvol * v2;
+    }
+    // the thread's kinetic partial as a compensated FP64 sum
+    __device__ __forceinline__ KSum kinetic() const {
+        if constexpr (sizeof(T) == 8)
+            return kin;
+        else
+            return KSum{double(kin_t), 0.0};
     }
 };
 
@@ -348,8 +360,8 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
                                 STAGE < 4 ? in.L[STAGE - 1] : in.F[parity ^ 1],
                                 STAGE < 4 ? nullptr : in.V[parity ^ 1],
                                 in.Flo[parity ^ 1],
-                                dtt, p.nsky, p.unit_length, -1.0e300, 0.0, 0.5 * p.vol, KSum{0.0, 0.0},
-                                in.Dlt, in.refresh};
+                                dtt, p.nsky, p.unit_length, T(-INFINITY), T(0), T(0.5 * p.vol), KSum{0.0, 0.0},
+                                T(0), in.Dlt, in.refresh};
         KSum es{0.0, 0.0}, bs{0.0, 0.0};
         march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE>, LO>(sm, p, src, a, b, xa, xe, y0, z0, epi, es,
                                                                          bs);
@@ -362,9 +374,10 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
             }
         }
         if (STAGE == 4) {
-            const double ga = block_max(epi.gmx, shm);
-            const double gb = block_max(epi.gab, shm);
-            const KSum kk = block_ksum(epi.kin, shk);
+            // a thread without sites keeps -inf, which block_max maps below every gradient
+            const double ga = block_max(fmax(double(epi.gmx), -1.0e300), shm);
+            const double gb = block_max(double(epi.gab), shm);
+            const KSum kk = block_ksum(epi.kinetic(), shk);
             if (threadIdx.x == 0 && threadIdx.y == 0) {
                 in.gpart[4 * lt] = ga;
                 in.gpart[4 * lt + 1] = gb;

@@ -388,6 +388,10 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
             const T* Pp2 = ring + slot * M::SLOT + lofs;
             const Mask mk = site_mask(p, x, y, z);
             const int64_t s = (int64_t)x * YZ + (int64_t)y * p.Z + z;
+            // baryon density of an FP32 stage input, from the FP32 derivatives the gradient uses
+            // (its FP64 sum needs no more than FP32 per-site accuracy; only the energy, which
+            // decides the arrest, is evaluated in FP64)
+            [[maybe_unused]] double b32 = 0.0;
             if constexpr (GRAD) {
             T phi[C], D[3][C], Sd[6][C], g[C];
 #pragma unroll
@@ -426,6 +430,7 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                 Sd[5][c] = (mk.my && mk.mz) ? k.mix[2] * mixed16<T>(f, M::HZ, 1) : T(0);
             }
             Th<T>::gradient(phi, D, Sd, p, g);
+            if constexpr (DENS != 0 && sizeof(T) == 4) b32 = double(Th<T>::baryon(phi, D, p));
             epi(s, N, phi, g);
             }
             if (DENS) {
@@ -466,7 +471,10 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
                 }
                 if constexpr (GRAD) {
                     ksum_add(esum, Th<double>::energy(phd, Dd, p));
-                    ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
+                    if constexpr (sizeof(T) == 4)
+                        ksum_add(bsum, b32);
+                    else
+                        ksum_add(bsum, Th<double>::baryon(phd, Dd, p));
                 } else if constexpr ((DENS & 16) != 0) {
                     epi.site(s, phd, Dd);  // the epilogue reads the FP64 field and first derivatives
                 } else {

@@ -24,25 +24,67 @@ constexpr int64_t kNoAllocDoubles = (int64_t)2 * 1024 * 1024;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
-// Device address of g_noalloc_scratch per device, looked up once per device
-// with that device current (host code must not use the symbol's name as an
-// address).
+// Device address of g_noalloc_scratch per device, looked up with that device
+// current (host code must not use the symbol's name as an address).  The
+// address belongs to the module loaded into the device's current context; after
+// cudaDeviceReset (or any re-creation of the primary context) the module is
+// loaded again, possibly elsewhere.  Each entry therefore records the unique id
+// of the context it was looked up in (cuCtxGetId, reached through the runtime's
+// driver entry points so that the library does not link libcuda), and a call
+// in a different context looks the address up again.
+typedef int (*PfnCtxGetCurrent)(void** ctx);
+typedef int (*PfnCtxGetId)(void* ctx, unsigned long long* id);
+
+struct NoAllocSlot {
+    double* ptr;
+    unsigned long long ctx_id;
+};
 static std::mutex g_noalloc_mutex;
-static double* g_noalloc_ptr[128] = {nullptr};
+static NoAllocSlot g_noalloc_slot[128] = {};
+
+// Unique id of the calling thread's current context (0 when it cannot be read).
+static unsigned long long current_context_id() {
+    static PfnCtxGetCurrent get_current = nullptr;
+    static PfnCtxGetId get_id = nullptr;
+    static bool resolved = false;
+    if (!resolved) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PfnCtxGetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PfnCtxGetId>(f);
+        cudaGetLastError();  // a missing entry point is not an error of the step
+        resolved = true;
+    }
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&ctx) == 0 && ctx != nullptr && get_id(ctx, &id) == 0) return id;
+    return 0;
+}
 
 static int noalloc_scratch(double** out) {
     int dev = 0;
     int rc = check_cuda(cudaGetDevice(&dev), "cudaGetDevice", __LINE__);
     if (rc) return rc;
     if (dev < 0 || dev >= 128) return invalid("device ordinal out of range for the static scratch table");
+    // make the device's primary context current (cudaSetDevice initialises it) before reading its id
+    if ((rc = check_cuda(cudaSetDevice(dev), "cudaSetDevice", __LINE__))) return rc;
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
+    NoAllocSlot& slot = g_noalloc_slot[dev];
+    // without a readable context id (ctx == 0) the address is looked up on every call
+    if (!slot.ptr || ctx == 0 || slot.ctx_id != ctx) {
         void* p = nullptr;
         rc = check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(static scratch)", __LINE__);
         if (rc) return rc;
-        g_noalloc_ptr[dev] = static_cast<double*>(p);
+        slot.ptr = static_cast<double*>(p);
+        slot.ctx_id = ctx;
     }
-    *out = g_noalloc_ptr[dev];
+    *out = slot.ptr;
     return SKY_OK;
 }
 

@@ -107,6 +107,8 @@ class Engine:
             try:
                 import torch
                 if isinstance(a, torch.Tensor) and a.is_cuda:
+                    if a.device.index != self.device:
+                        raise ValueError(f"device tensor on {a.device}, but the engine runs on cuda:{self.device}")
                     on_dev = 1
                     t = a.detach().to(torch.float64).contiguous()
                     keep.append(t)
@@ -124,7 +126,7 @@ class Engine:
         if on_dev:
             # the engine reads device inputs on its own stream: finish torch's pending work first
             import torch
-            torch.cuda.current_stream().synchronize()
+            torch.cuda.current_stream(torch.device("cuda", self.device)).synchronize()
         C = int(p_i[5])
         n = C * int(p_i[6])
         if (keep[0].numel() if hasattr(keep[0], "numel") else keep[0].size) != n:
@@ -223,13 +225,16 @@ class Engine:
         m = self.meta[iid]
         N = int(m["p_i"][6])
         dev = torch.device("cuda", self.device)
-        field = torch.empty(m["C"] * N, dtype=torch.float64, device=dev)
-        torch.cuda.current_stream(dev).synchronize()   # the engine writes on its own stream
-        self.read_device(iid, field)                   # synchronous on the engine's stream
-        en = torch.zeros(N, dtype=torch.float64, device=dev)
-        fn = "sky_baryon_density" if density == "baryon" else "sky_energy_density"
-        _lib.call(fn, m["theory"], i32p(m["p_i"]), len(m["p_i"]), f64p(m["p_f"]), len(m["p_f"]), _lib.dptr(en),
-                  _lib.dptr(field), _lib.stream_ptr(torch.cuda.current_stream(dev)))
+        # the C functions launch on the current device: make the engine's device current
+        with torch.cuda.device(dev):
+            stream = torch.cuda.current_stream(dev)
+            field = torch.empty(m["C"] * N, dtype=torch.float64, device=dev)
+            stream.synchronize()                           # the engine writes on its own stream
+            self.read_device(iid, field)                   # synchronous on the engine's stream
+            en = torch.zeros(N, dtype=torch.float64, device=dev)
+            fn = "sky_baryon_density" if density == "baryon" else "sky_energy_density"
+            _lib.call(fn, m["theory"], i32p(m["p_i"]), len(m["p_i"]), f64p(m["p_f"]), len(m["p_f"]), _lib.dptr(en),
+                      _lib.dptr(field), _lib.stream_ptr(stream))
         return field, en
 
     def diagnostics(self, iid: int) -> dict:
@@ -244,22 +249,24 @@ class Engine:
         m = self.meta[iid]
         p_i, p_f = m["p_i"], m["p_f"]
         dev = torch.device("cuda", self.device)
-        field = torch.empty(m["C"] * int(p_i[6]), dtype=torch.float64, device=dev)
-        torch.cuda.current_stream(dev).synchronize()
-        self.read_device(iid, field)
-        mom = ob._moments(m["theory"], field, None, p_i, p_f)
-        B = mom[0]
-        com = np.zeros(3) if abs(B) < 1.0e-30 else mom[1:4] / B
-        rms = 0.0
-        if abs(B) >= 1.0e-30:
-            num = mom[8] - 2.0 * float(np.dot(com, mom[5:8])) + float(np.dot(com, com)) * mom[4]
-            rms = math.sqrt(max(num / B, 0.0))
-        out = {"center_of_mass": com, "rms_radius": rms}
-        if m["theory"] == 0:
-            _, d = ob._nuclear_diag(0, field, None, p_i, p_f)
-            E = ob._total("sky_total_energy", 0, field, None, None, None, p_i, p_f)
-            out.update(U=ob._sym(d[0:6]), V=ob._sym(d[6:12]), W=d[12:21].reshape(3, 3).copy(),
-                       quadrupole=ob._sym(d[21:27]), D_term=-(2.0 / 5.0) * E * float(d[27]))
+        # the C functions launch on the current device and torch's current stream there
+        with torch.cuda.device(dev):
+            field = torch.empty(m["C"] * int(p_i[6]), dtype=torch.float64, device=dev)
+            torch.cuda.current_stream(dev).synchronize()
+            self.read_device(iid, field)
+            mom = ob._moments(m["theory"], field, None, p_i, p_f)
+            B = mom[0]
+            com = np.zeros(3) if abs(B) < 1.0e-30 else mom[1:4] / B
+            rms = 0.0
+            if abs(B) >= 1.0e-30:
+                num = mom[8] - 2.0 * float(np.dot(com, mom[5:8])) + float(np.dot(com, com)) * mom[4]
+                rms = math.sqrt(max(num / B, 0.0))
+            out = {"center_of_mass": com, "rms_radius": rms}
+            if m["theory"] == 0:
+                _, d = ob._nuclear_diag(0, field, None, p_i, p_f, moments=mom)
+                E = ob._total("sky_total_energy", 0, field, None, None, None, p_i, p_f)
+                out.update(U=ob._sym(d[0:6]), V=ob._sym(d[6:12]), W=d[12:21].reshape(3, 3).copy(),
+                           quadrupole=ob._sym(d[21:27]), D_term=-(2.0 / 5.0) * E * float(d[27]))
         return out
 
     def time_stages(self, nsteps: int) -> dict:

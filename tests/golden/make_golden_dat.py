@@ -17,7 +17,7 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE_ROOT = "/root/reference"
+REFERENCE_ROOT = os.environ.get("SKY_REFERENCE_ROOT", "/root/reference")
 DIRS = {"nuclear": "nuclear_skyrme", "omega": "omega_skyrme", "coulomb": "coulomb_skyrme", "rho": "rho_skyrme",
         "berger": "berger_skyrme", "lightly_bound": "lightly_bound_skyrme"}
 
