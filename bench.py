@@ -362,6 +362,8 @@ def run_ours(args):
         pg = dist
     warmup = max(3, args.warmup)
     K = args.steps
+    from skyrmion_solver_b200 import _lib
+    _lib.call("sky_set_option", 2, 1 if args.staging == "tma" else 0)
     th, p, p_i, p_f = workload_params()
     C, N = int(p_i[5]), int(p_i[6])
     field = workload_field_device(p_i, p_f, dev)
@@ -506,7 +508,7 @@ def run_ours(args):
                             "e2e = 1 / wall time of Engine.add (pinned host field) + the steps + per-chunk "
                             "statistics reads + the final field read into pinned host memory",
                    "l2": f"no flush: resident state {9 * C * N * 4 / 1e6:.0f} MB > 126 MB L2",
-                   "parallelism": f"replicas x{world}"},
+                   "staging": args.staging, "parallelism": f"replicas x{world}"},
         "latency_s": {"p50": solve_s, "p99": solve_s, "note": "one resident solve per GPU; the serving mode "
                       "(--serve) reports p50/p99 over a request stream"},
         "final": final,
@@ -969,6 +971,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--quick", action="store_true", help="skip the two timed solves (K-step rate only)")
     ap.add_argument("--chunk", type=int, default=128, help="steps between convergence checks of a solve")
+    ap.add_argument("--staging", choices=("tma", "cp.async"), default="tma",
+                    help="how the engine's stage kernels stage lattice planes in shared memory")
     ap.add_argument("--calibrate", action="store_true")
     ap.add_argument("--max-steps", type=int, default=240000)
     ap.add_argument("--out", default=None)

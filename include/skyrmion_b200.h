@@ -32,7 +32,8 @@ typedef enum {
     SKY_ERR_CUDA = 2,      /* a CUDA runtime call failed */
     SKY_ERR_NONFINITE = 3, /* reserved: non-finite energies are returned as values, as the
                               reference returns them (its step reports NaN, it does not raise) */
-    SKY_ERR_TIMEOUT = 4,   /* reserved: no kernel of the library waits on a flag or a peer */
+    SKY_ERR_TIMEOUT = 4,   /* a stage kernel gave up a bounded wait for a TMA plane copy (the
+                              engine's statistics calls report it; the step is not valid) */
     SKY_ERR_NOMEM = 5      /* caller-provided scratch too small / allocation failed */
 } sky_status;
 
@@ -52,7 +53,10 @@ const char* sky_last_error(void);
 /* Library-wide tuning options.  Key 0: kernel family of the reference-layout
  * gradient (sky_gradient_step / sky_arrested_newton_step) for theories with at
  * most five components: 1 = marching x-plane kernels (default), 0 = 3-D tile
- * kernels.  Key 1: x-chunk of those marching launches (0 = automatic).
+ * kernels.  Key 1: x-chunk of those marching launches (0 = automatic).  Key 2:
+ * staging of the resident engine's stage kernels, 1 = tensor-memory-accelerator
+ * box copies (default; lattices whose Z gives 16-byte row pitches), 0 = per-thread
+ * cp.async copies; it applies to instances admitted (or re-tiled) afterwards.
  * Process-wide; not synchronised with launches in flight on other threads. */
 int sky_set_option(int key, int value);
 int sky_get_option(int key);

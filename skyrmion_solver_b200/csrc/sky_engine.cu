@@ -39,6 +39,7 @@ struct HostInst {
     int ntiles = 0, tnz = 0, tny = 0, tnx = 0;
     int xc = 0;          // x-chunk of the marching kernels
     int xc_request = 0;  // x-chunk asked for by the caller (0: automatic)
+    bool tma = false;    // the stage kernels stage this instance with TMA box copies
     int group_slot = -1;
     int64_t steps = 0;  // host mirror of the device step counter
     bool active = true;
@@ -55,6 +56,7 @@ struct Group {
     bool any_comp = false;  // holds a compensated-field instance (stage 1 stages the low parts too)
     bool all_wide = true;   // every member can use the wide-row (16-byte staged) kernels
     bool any_defect = false;  // holds a defect-corrected instance (launch the defect refresh)
+    bool all_tma = false;     // every member has TMA plane maps (launch the TMA stage kernels)
 };
 
 struct Engine {
@@ -67,6 +69,7 @@ struct Engine {
     cudaGraphExec_t graph1 = nullptr;  // one step (the remainder of a step call)
     bool graph_valid = false;
     int64_t bytes = 0;
+    int* d_status = nullptr;  // device error word the stage kernels set (bit 0: a TMA wait gave up)
 };
 
 // ---------------------------------------------------------------------------
@@ -108,14 +111,21 @@ static bool wide_ok(int prec, int Z) { return Z % (prec ? 2 : 4) == 0; }
 
 // One-time kernel attribute setup (kept out of stream capture); returns the
 // number of resident blocks per SM.
-template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false>
+template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false>
+static size_t stage_smem() {
+    using M = MShape<Th, T, WIDE>;
+    return TMA ? M::template smem_bytes_tma<T>(LO ? 2 : stage_nsrc<STAGE>(), LO)
+               : M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
+}
+
+template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false>
 static int stage_setup_w(int* per_sm_out) {
     static int per_sm = 0;
     if (per_sm == 0) {
         int rc, n = 0;
         using M = MShape<Th, T, WIDE>;
-        auto kern = k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO>;
-        const size_t smem = M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
+        auto kern = k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO, TMA>;
+        const size_t smem = stage_smem<Th, T, STAGE, WIDE, LO, TMA>();
         rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                         "cudaFuncSetAttribute(march stage)", __LINE__);
         if (rc) return rc;
@@ -133,24 +143,38 @@ static int stage_setup(int* per_sm_out) {
     return stage_setup_w<Th, T, STAGE, true>(per_sm_out);
 }
 
-template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false>
+template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false>
 static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t st) {
     int per_sm = 1;
-    int rc = stage_setup_w<Th, T, STAGE, WIDE, LO>(&per_sm);
+    int rc = stage_setup_w<Th, T, STAGE, WIDE, LO, TMA>(&per_sm);
     if (rc) return rc;
     int n = t_end - t_begin;
     if (n <= 0) return SKY_OK;
     const int blocks = n < num_sms() * per_sm ? n : num_sms() * per_sm;
     InstDesc<T>* d = reinterpret_cast<InstDesc<T>*>(g.d_desc);
     using M = MShape<Th, T, WIDE>;
-    const size_t smem = M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
-    k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(
+    const size_t smem = stage_smem<Th, T, STAGE, WIDE, LO, TMA>();
+    k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO, TMA><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(
         d, g.d_tile_inst, t_begin, t_end);
     return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
 }
 
+// Whether the stage kernels of (Th, T) can stage with TMA: wide rows must be allowed.
+template <template <typename> class Th, typename T>
+constexpr bool tma_allowed() {
+    return march_wide_allowed<Th, T>();
+}
+
 template <template <typename> class Th, typename T, int STAGE>
 static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
+    if constexpr (tma_allowed<Th, T>()) {
+        if (g.all_tma) {
+            if constexpr (STAGE == 1 && sizeof(T) == 4 && Th<float>::C <= 5) {
+                if (g.any_comp) return launch_stage_w<Th, T, 1, true, true, true>(g, t_begin, t_end, st);
+            }
+            return launch_stage_w<Th, T, STAGE, true, false, true>(g, t_begin, t_end, st);
+        }
+    }
     // stage 1 of a group with compensated-field instances stages the low parts too,
     // in wide rows when two blocks per SM still fit (the two six-slot rings take
     // 112.5 KB per block for C = 5), else in narrow rows; rho's 13 components leave
@@ -194,6 +218,16 @@ static int setup_all() {
     if constexpr (sizeof(T) == 4 && Th<float>::C <= 5) {  // stage 1 with the low parts
         if ((rc = stage_setup_w<Th, T, 1, true, true>(&n)) || (rc = stage_setup_w<Th, T, 1, false, true>(&n)))
             return rc;
+    }
+    if constexpr (tma_allowed<Th, T>()) {
+        if ((rc = stage_setup_w<Th, T, 1, true, false, true>(&n)) ||
+            (rc = stage_setup_w<Th, T, 2, true, false, true>(&n)) ||
+            (rc = stage_setup_w<Th, T, 3, true, false, true>(&n)) ||
+            (rc = stage_setup_w<Th, T, 4, true, false, true>(&n)))
+            return rc;
+        if constexpr (sizeof(T) == 4 && Th<float>::C <= 5) {
+            if ((rc = stage_setup_w<Th, T, 1, true, true, true>(&n))) return rc;
+        }
     }
     return SKY_OK;
 }
@@ -355,6 +389,19 @@ __global__ void k_f32c_to_f64(int64_t n, const float* __restrict__ hi, const flo
 // ---------------------------------------------------------------------------
 // descriptors
 // ---------------------------------------------------------------------------
+// TMA plane maps of an instance's staged arrays (box: 40 z-values x (BY + 4) rows x 1
+// plane x C components, the marching kernels' wide-row plane).
+template <typename S>
+static int encode_maps(const HostInst& h, InstDesc<S>& d, int by) {
+    const void* arrs[kNumMaps] = {h.F[0], h.F[1], h.Flo[0], h.Flo[1], h.V[0], h.V[1], h.L[0], h.L[1], h.L[2]};
+    for (int k = 0; k < kNumMaps; ++k) {
+        if (!arrs[k]) continue;
+        int rc = encode_plane_map(&d.tm[k], arrs[k], (int)sizeof(S), h.p.X, h.p.Y, h.p.Z, h.C, 40, by + 4);
+        if (rc) return rc;
+    }
+    return SKY_OK;
+}
+
 template <typename S>
 static InstDesc<S> make_desc(const HostInst& h, int tile_begin) {
     InstDesc<S> d;
@@ -403,9 +450,20 @@ static int rebuild_group_t(Engine& e, Group& g) {
     g.any_comp = false;
     g.all_wide = true;
     g.any_defect = false;
+    g.all_tma = !g.members.empty();
     for (size_t k = 0; k < g.members.size(); ++k) {
         HostInst& h = e.insts[g.members[k]];
         InstDesc<S> d = make_desc<S>(h, tb);
+        d.status = e.d_status;
+        if (h.tma) {
+            int bz, by, tx, per_sm;
+            int rc = tile_shape(h.theory, h.prec, bz, by, tx, per_sm);
+            if (!rc) rc = encode_maps<S>(h, d, by);
+            if (rc) return rc;
+            d.tma = 1;
+        } else {
+            g.all_tma = false;
+        }
         if (h.group_slot >= 0 && h.group_slot < (int)dev_old.size()) {
             const InstDesc<S>& o = dev_old[h.group_slot];
             d.e_prev = o.e_prev;
@@ -468,8 +526,16 @@ static void free_inst(HostInst& h) {
     h.stats = nullptr;
 }
 
+// Whether an instance's planes can be staged by TMA box copies: the option is on,
+// the row pitch Z * sizeof(T) is a multiple of 16 bytes, and its (theory,
+// precision) uses wide rows (every one but FP64 rho).
+static bool tma_ok_for(const HostInst& h) {
+    return option(2) == 1 && wide_ok(h.prec, h.p.Z) && !(h.prec && theory_components(h.theory) > 5);
+}
+
 static int alloc_inst(Engine& e, HostInst& h) {
     const size_t es = h.prec ? sizeof(double) : sizeof(float);
+    h.tma = tma_ok_for(h);
     const size_t fb = es * (size_t)h.C * (size_t)h.N;
     int bz, by, tx, per_sm;
     int rc0 = tile_shape(h.theory, h.prec, bz, by, tx, per_sm);
@@ -649,6 +715,16 @@ static int build_graph(Engine& e) {
     return SKY_OK;
 }
 
+// A statistics record written while the engine's error word was set: a stage
+// kernel gave up waiting for a TMA copy, so the step's results are not valid.
+static int status_error(const StepStats& st) {
+    if (st.status == 0) return SKY_OK;
+    char msg[160];
+    snprintf(msg, sizeof(msg), "engine error word 0x%x: a stage kernel gave up waiting for a TMA plane copy",
+             (unsigned)st.status);
+    return fail(SKY_ERR_TIMEOUT, msg);
+}
+
 static HostInst* find(Engine* e, int id) {
     auto it = e->insts.find(id);
     return it == e->insts.end() ? nullptr : &it->second;
@@ -737,7 +813,11 @@ int sky_engine_create(int device, void** out) {
     e->device = device;
     int rc = check_cuda(cudaSetDevice(device), "cudaSetDevice", __LINE__);
     if (!rc) rc = check_cuda(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "stream", __LINE__);
+    if (!rc) rc = check_cuda(cudaMalloc(&e->d_status, sizeof(int)), "cudaMalloc(status)", __LINE__);
+    if (!rc) rc = check_cuda(cudaMemset(e->d_status, 0, sizeof(int)), "memset(status)", __LINE__);
     if (rc) {
+        if (e->d_status) cudaFree(e->d_status);
+        if (e->stream) cudaStreamDestroy(e->stream);
         delete e;
         return rc;
     }
@@ -763,6 +843,7 @@ int sky_engine_destroy(void* handle) {
             if (e->groups[t][p].d_desc) cudaFree(e->groups[t][p].d_desc);
             if (e->groups[t][p].d_tile_inst) cudaFree(e->groups[t][p].d_tile_inst);
         }
+    if (e->d_status) cudaFree(e->d_status);
     cudaStreamDestroy(e->stream);
     delete e;
     return SKY_OK;
@@ -961,6 +1042,7 @@ int sky_engine_retile(void* handle, int id, int xc) {
     h.xc = nxc;
     h.tnx = (h.p.X + nxc - 1) / nxc;
     h.ntiles = ntiles;
+    h.tma = tma_ok_for(h);
     Group& g = e->groups[h.theory][h.prec];
     if ((rc = rebuild_group(*e, g))) return rc;
     return init_instance(*e, h, 2);
@@ -1070,6 +1152,7 @@ int sky_engine_stats(void* handle, int id, int64_t step, double* out6) {
                         "read stats", __LINE__);
     if (rc) return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__))) return rc;
+    if ((rc = status_error(st))) return rc;
     out6[0] = st.energy;
     out6[1] = st.baryon;
     out6[2] = st.err;
@@ -1092,6 +1175,7 @@ int sky_engine_stats_ex(void* handle, int id, int64_t step, double* out8) {
                         "read stats", __LINE__);
     if (rc) return rc;
     if ((rc = check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__))) return rc;
+    if ((rc = status_error(st))) return rc;
     out8[0] = st.energy;
     out8[1] = st.baryon;
     out8[2] = st.err;
@@ -1121,6 +1205,8 @@ int sky_engine_stats_all(void* handle, int* ids_out, double* out7, int cap, int*
     }
     int rc = check_cuda(cudaStreamSynchronize(e->stream), "sync", __LINE__);
     if (rc) return rc;
+    for (int i = 0; i < k; ++i)
+        if ((rc = status_error(st[i]))) return rc;
     for (int i = 0; i < k; ++i) {
         if (ids_out) ids_out[i] = hs[i]->id;
         if (out7) {

@@ -36,11 +36,19 @@ struct StepStats {
     int arrested;       // velocity treated as zero in step n+1
     int step;           // n
     double kinetic;     // (1/2) h^3 sum |V'|^2 of the velocity step n produced (before any arrest)
+    int status;         // the engine's error word when the record was written (0: no error)
+    int reserved;
 };
+
+// Roles of an instance's TMA plane maps (InstDesc::tm).
+enum { kMapF = 0, kMapFlo = 2, kMapV = 4, kMapL = 6, kNumMaps = 9 };
 
 // Device-resident state of one instance.
 template <typename S>
 struct InstDesc {
+    TmaMap tm[kNumMaps];  // plane maps of F[0..1], Flo[0..1], V[0..1], L[0..2] (when tma is set)
+    int tma;              // the stage kernels stage this instance's planes with TMA
+    int* status;          // the engine's error word (bit 0: a wait for a TMA copy gave up)
     Params p;
     S* F[2];           // ping-pong field
     S* Flo[2];         // ping-pong low parts of a compensated FP32 field (null otherwise)
@@ -235,6 +243,7 @@ __global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict_
         }
         st.arrested = arrest;
         st.step = n;
+        st.status = in.status ? *in.status : 0;
         in.arrested = arrest;
         in.e_prev = en;
     }
@@ -332,14 +341,22 @@ struct EngineEpi {
     }
 };
 
-template <template <typename> class Th, class M, typename T, int STAGE, int MINB, bool LO = false>
+// TMA: planes staged by tensor-memory-accelerator box copies (every instance of
+// the launch has its maps encoded; wide rows).
+template <template <typename> class Th, class M, typename T, int STAGE, int MINB, bool LO = false, bool TMA = false>
 __global__ void __launch_bounds__(M::NTHREADS, MINB)
     k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
     constexpr int NSRC = STAGE == 1 ? (LO ? 2 : 1) : (STAGE == 2 ? 2 : 3);
-    extern __shared__ __align__(16) unsigned char smraw[];
+    extern __shared__ __align__(128) unsigned char smraw[];
     T* sm = reinterpret_cast<T*>(smraw);
     __shared__ KSum shk[M::NTHREADS / 32];  // one entry per warp (kept small: two blocks
     __shared__ double shm[M::NTHREADS / 32];  // per SM need all but 1 KB of shared memory)
+    __shared__ uint64_t tma_bar;
+    TmaTile tt{&tma_bar, 0u, {nullptr, nullptr, nullptr}, nullptr};
+    if constexpr (TMA) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) mbar_init(&tma_bar, 1);
+        __syncthreads();
+    }
     for (int t = t_begin + blockIdx.x; t < t_end; t += gridDim.x) {
         const int ii = __ldg(tile_inst + t);
         const InstDesc<T>& in = insts[ii];
@@ -363,8 +380,15 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
                                 dtt, p.nsky, p.unit_length, T(-INFINITY), T(0), T(0.5 * p.vol), KSum{0.0, 0.0},
                                 T(0), in.Dlt, in.refresh};
         KSum es{0.0, 0.0}, bs{0.0, 0.0};
-        march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE>, LO>(sm, p, src, a, b, xa, xe, y0, z0, epi, es,
-                                                                         bs);
+        if constexpr (TMA) {
+            tt.map[0] = &in.tm[kMapF + parity];
+            tt.map[1] = LO ? &in.tm[kMapFlo + parity] : (V != nullptr ? &in.tm[kMapV + parity] : nullptr);
+            tt.map[2] = NSRC > 2 ? &in.tm[kMapL + (STAGE == 3 ? 0 : 1)] : nullptr;
+            tt.status = in.status;
+        }
+        if (!march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE>, LO, T, true, TMA>(
+                sm, p, src, a, b, xa, xe, y0, z0, epi, es, bs, TMA ? &tt : nullptr))
+            return;  // a copy did not arrive: the block's error bit is set, its partials stay stale
         if (STAGE == 1) {
             const KSum be = block_ksum(es, shk);
             const KSum bb = block_ksum(bs, shk);

@@ -10,6 +10,7 @@ namespace sky {
 
 int check_cuda(cudaError_t e, const char* what, int line);
 int invalid(const char* msg);
+int fail(int code, const char* msg);  // records msg as the last error and returns code
 const char* last_error();
 int theory_components(int theory);
 int pack_core(const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf, Params* out, bool need_f);

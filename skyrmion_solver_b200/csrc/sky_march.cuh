@@ -24,6 +24,7 @@
 #include <type_traits>
 
 #include "sky_kernels.cuh"
+#include "sky_tma.cuh"
 
 namespace sky {
 
@@ -60,6 +61,24 @@ struct MarchShape {
     static constexpr size_t smem_bytes(int nsrc, bool lo = false) {
         return size_t(RING) * (lo ? 2 : 1) * SLOT * sizeof(T) + size_t(staged<T, S>(nsrc)) * SLOT * sizeof(S);
     }
+    // TMA staging (wide rows): a six-slot ring into which the copy engine writes
+    // the first source (and, for a compensated field, a second six-slot ring for
+    // the low parts), plus one staging slot for each further source
+    template <typename T>
+    static constexpr size_t smem_bytes_tma(int nsrc, bool lo = false) {
+        return (lo ? 12 : 6 + (nsrc - 1)) * size_t(SLOT) * sizeof(T);
+    }
+};
+
+// Per-tile TMA state of a marching kernel: the kernel's mbarrier (initialised
+// once per launch), the parity of the phase the next plane completes, the maps
+// of the tile's sources (null: the source reads as zero) and the launch-wide
+// error word that a timed-out wait sets.
+struct TmaTile {
+    uint64_t* bar;
+    uint32_t phase;
+    const TmaMap* map[3];
+    int* status;
 };
 
 // ---------------------------------------------------------------------------
@@ -289,10 +308,18 @@ __device__ __forceinline__ T diff5(const T* f, int st) {
 // potential of the RK4 dynamics when DENS & 4, else energy when DENS & 1, else
 // baryon) is passed to epi.density(s, value); with DENS & 16 the site's FP64
 // field values and first derivatives go to epi.site(s, phi, D) instead.
+// TMA: the planes are copied by the tensor-memory accelerator (one thread issues
+// one box copy per source and plane; sky_tma.cuh) instead of per-thread cp.async;
+// wide rows and S = T only.  The first source goes straight into a six-slot ring,
+// further sources into staging slots that are added into the ring slot, and one
+// barrier per plane orders the copies with the readers.  Returns false (every
+// thread of the block) when a wait for a copy gave up (the block's error bit is
+// then set in tma->status).
 template <template <typename> class Th, class M, typename T, int NSRC, int DENS, class Epi, bool LO = false,
-          typename S = T, bool GRAD = true>
-__device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, const S* const (&src)[3], T a, T b,
-                                           int xa, int xe, int y0, int z0, Epi& epi, KSum& esum, KSum& bsum) {
+          typename S = T, bool GRAD = true, bool TMA = false>
+__device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, const S* const (&src)[3], T a, T b,
+                                           int xa, int xe, int y0, int z0, Epi& epi, KSum& esum, KSum& bsum,
+                                           TmaTile* tma = nullptr) {
     constexpr int C = M::C;
     constexpr int CT = Th<double>::C;  // components of the theory
     // register queues of the y / z first-difference sums for C <= 5; with more
@@ -305,12 +332,14 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
     constexpr bool DIRECT = (NSRC == 1 || LO) && std::is_same<S, T>::value;
     constexpr int NST = M::template staged<T, S>(NSRC);  // sources staged in shared memory
     static_assert(NST == NSRC || !M::WIDE, "the unstaged third source is read with narrow-row offsets");
-    constexpr int R = DIRECT ? M::RING + 1 : M::RING;  // ring slots
+    static_assert(!TMA || (M::WIDE && std::is_same<S, T>::value && NST == NSRC), "TMA staging: wide rows, S = T");
+    constexpr int R = (DIRECT || TMA) ? M::RING + 1 : M::RING;  // ring slots
     constexpr int DST = DIRECT ? R * M::SLOT : M::SLOT;  // distance between the sources' copies
     // shared memory: DIRECT: ring (R slots) [+ low-part ring (R slots)];
+    // TMA: ring (6 slots) + NSRC - 1 staging slots;
     // otherwise: ring (5 slots) + NSRC staging slots of S
     T* ring = sm;
-    S* stage = reinterpret_cast<S*>(sm + M::RING * M::SLOT);
+    S* stage = reinterpret_cast<S*>(sm + (TMA ? R : M::RING) * M::SLOT);
     T* ring_lo = sm + R * M::SLOT;
 
     const int64_t N = n_sites(p);
@@ -341,17 +370,87 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
             if constexpr (NST < NSRC) plane_prefetch_l2<M, S>(po, src[2], base, xok);
         }
     };
+    // TMA: thread 0 copies plane qq of every present source (a plane outside the
+    // lattice arrives as zeros); source 0 into ring slot dslot, the low parts into the
+    // low-part ring, further sources into the staging slots
+    const int tid0 = threadIdx.x + M::BZ * threadIdx.y;
+    auto issue_tma = [&](int qq, int dslot) {
+        if (tid0 != 0) return;
+        constexpr uint32_t box = uint32_t(M::SLOT * sizeof(T));
+        uint32_t n = 1;
+#pragma unroll
+        for (int k = 1; k < NSRC; ++k) n += tma->map[k] != nullptr ? 1u : 0u;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(tma->bar, n * box);
+        const int zc = z0 - M::ZOFF, yc = y0 - 2;
+        tma_load_plane(ring + dslot * M::SLOT, tma->map[0], zc, yc, qq, 0, tma->bar);
+#pragma unroll
+        for (int k = 1; k < NSRC; ++k) {
+            if (tma->map[k] == nullptr) continue;
+            T* dst = LO ? ring_lo + dslot * M::SLOT : reinterpret_cast<T*>(stage) + (k - 1) * M::SLOT;
+            tma_load_plane(dst, tma->map[k], zc, yc, qq, 0, tma->bar);
+        }
+    };
     __syncthreads();
-    issue((int64_t)q0 * YZ, q0 >= 0 && q0 < p.X, 0);
+    if constexpr (TMA)
+        issue_tma(q0, 0);
+    else
+        issue((int64_t)q0 * YZ, q0 >= 0 && q0 < p.X, 0);
     int slot = 0;  // ring slot of plane q
     for (int q = q0; q <= q1; ++q) {
-        cp_async_wait_all();
-        // (A) plane q has landed for every thread, and every thread finished the
-        // previous centre: the slot of plane q - 5 (staging: the staging area) is free
-        __syncthreads();
-        if constexpr (DIRECT) {
+        if constexpr (TMA) {
+            // plane q has landed; for further sources, add a V + b L into the ring slot
+            const bool ok = mbar_wait_bounded(tma->bar, tma->phase);
+            tma->phase ^= 1u;
+            if constexpr (!DIRECT) {
+                using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+                constexpr int VW = 16 / int(sizeof(T));
+                constexpr int NV = M::SLOT / VW;
+                static_assert(M::SLOT % VW == 0, "slot of whole 16-byte vectors");
+                V4* dstv = reinterpret_cast<V4*>(ring + slot * M::SLOT);
+                const V4* s1 = reinterpret_cast<const V4*>(stage);
+                const V4* s2 = reinterpret_cast<const V4*>(stage) + NV;
+                const bool h1 = tma->map[1] != nullptr;
+                const bool h2 = NSRC > 2 && tma->map[2] != nullptr;
+                if (h1 || h2) {
+                    for (int i = tid0; i < NV; i += M::NTHREADS) {
+                        V4 v = dstv[i];
+                        T* e = reinterpret_cast<T*>(&v);
+                        if (h1) {
+                            const V4 u = s1[i];
+                            const T* f = reinterpret_cast<const T*>(&u);
+#pragma unroll
+                            for (int j = 0; j < VW; ++j) e[j] += a * f[j];
+                        }
+                        if (h2) {
+                            const V4 u = s2[i];
+                            const T* f = reinterpret_cast<const T*>(&u);
+#pragma unroll
+                            for (int j = 0; j < VW; ++j) e[j] += b * f[j];
+                        }
+                        dstv[i] = v;
+                    }
+                }
+            }
+            // every thread has its plane q (and finished the centre of plane q - 1):
+            // the slot of plane q - 5 and the staging slots are free for plane q + 1
+            if (__syncthreads_or(ok ? 0 : 1)) {
+                if (tid0 == 0) {
+                    atomicOr(tma->status, 1);
+                    mbar_wait_bounded(tma->bar, tma->phase ^ 1u);  // let a late copy land before exiting
+                }
+                return false;
+            }
+            if (q < q1) issue_tma(q + 1, slot + 1 == R ? 0 : slot + 1);
+        } else if constexpr (DIRECT) {
+            cp_async_wait_all();
+            // (A) plane q has landed for every thread, and every thread finished the
+            // previous centre: the slot of plane q - 5 (staging: the staging area) is free
+            __syncthreads();
             if (q < q1) issue((int64_t)(q + 1) * YZ, q + 1 >= 0 && q + 1 < p.X, slot + 1 == R ? 0 : slot + 1);
         } else {
+            cp_async_wait_all();
+            __syncthreads();  // (A), as above
             if constexpr (NST < NSRC) {
                 if constexpr (!M::WIDE)
                     plane_combine_g<M, T, S>(ring + slot * M::SLOT, stage, a, b, po, src[2], (int64_t)q * YZ,
@@ -490,6 +589,7 @@ __device__ __forceinline__ void march_tile(T* __restrict__ sm, const Params& p, 
         }
         slot = (slot + 1) % R;
     }
+    return true;
 }
 
 // ---------------------------------------------------------------------------

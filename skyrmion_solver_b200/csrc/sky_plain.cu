@@ -183,6 +183,11 @@ int invalid(const char* msg) {
     return SKY_ERR_INVALID;
 }
 
+int fail(int code, const char* msg) {
+    snprintf(g_err, sizeof(g_err), "%s", msg);
+    return code;
+}
+
 const char* last_error() { return g_err; }
 
 int theory_components(int theory) {
@@ -314,8 +319,9 @@ int choose_xc(int X, int tiles_yz, int resident) {
 
 // Library options (sky_set_option): key 0 = kernel family of the
 // reference-layout gradient and densities (1 = marching kernels, 0 = 3-D tile
-// kernels); key 1 = x-chunk of those marching launches (0 = automatic).
-static int g_options[4] = {1, 0, 0, 0};
+// kernels); key 1 = x-chunk of those marching launches (0 = automatic); key 2 =
+// staging of the engine's stage kernels (1 = TMA box copies, 0 = cp.async).
+static int g_options[4] = {1, 0, 1, 0};
 int option(int key) { return (key >= 0 && key < 4) ? g_options[key] : 0; }
 
 // ---------------------------------------------------------------------------
@@ -641,7 +647,8 @@ const char* sky_version(void) { return "skyrmion_b200 0.2 (sm_100a)"; }
 int sky_set_option(int key, int value) {
     if (key == 0 && value != 0 && value != 1) return invalid("option 0 takes 0 (tile kernels) or 1 (marching kernels)");
     if (key == 1 && value < 0) return invalid("option 1 (x-chunk) must be >= 0");
-    if (key < 0 || key > 1) return invalid("unknown option key");
+    if (key == 2 && value != 0 && value != 1) return invalid("option 2 takes 0 (cp.async staging) or 1 (TMA staging)");
+    if (key < 0 || key > 2) return invalid("unknown option key");
     g_options[key] = value;
     return SKY_OK;
 }
