@@ -114,7 +114,8 @@ static bool wide_ok(int prec, int Z) { return Z % (prec ? 2 : 4) == 0; }
 template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false>
 static size_t stage_smem() {
     using M = MShape<Th, T, WIDE>;
-    return TMA ? M::template smem_bytes_tma<T>(LO ? 2 : stage_nsrc<STAGE>(), LO)
+    // TMA: 128 bytes of slack to start the ring on a 128-byte boundary
+    return TMA ? M::template smem_bytes_tma<T>(LO ? 2 : stage_nsrc<STAGE>(), LO) + 128
                : M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
 }
 

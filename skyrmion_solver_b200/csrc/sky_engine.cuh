@@ -348,7 +348,9 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
     k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
     constexpr int NSRC = STAGE == 1 ? (LO ? 2 : 1) : (STAGE == 2 ? 2 : 3);
     extern __shared__ __align__(128) unsigned char smraw[];
-    T* sm = reinterpret_cast<T*>(smraw);
+    // TMA box copies land on 128-byte boundaries: the launch adds 128 bytes of slack
+    // and the ring starts at the first 128-byte boundary of the dynamic segment
+    T* sm = reinterpret_cast<T*>(smraw + (TMA ? ((128u - (smem_addr(smraw) & 127u)) & 127u) : 0u));
     __shared__ KSum shk[M::NTHREADS / 32];  // one entry per warp (kept small: two blocks
     __shared__ double shm[M::NTHREADS / 32];  // per SM need all but 1 KB of shared memory)
     __shared__ uint64_t tma_bar;
