@@ -121,8 +121,8 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
         v2 = T(0);
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            Fo[c * N + s] = S(fv[c]);
-            Vo[c * N + s] = S(vv[c]);
+            __stcg(Fo + c * N + s, S(fv[c]));
+            __stcg(Vo + c * N + s, S(vv[c]));
             v2 += vv[c] * vv[c];
         }
     } else {
@@ -150,8 +150,8 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             hi[c] = T(fd[c]);
-            Fo[c * N + s] = S(hi[c]);
-            Flo_out[c * N + s] = S(fd[c] - double(hi[c]));
+            __stcg(Fo + c * N + s, S(hi[c]));
+            __stcg(Flo_out + c * N + s, S(fd[c] - double(hi[c])));
         }
         if (unit_length) {
             T lm = T(0);
@@ -165,7 +165,7 @@ __device__ __forceinline__ void finalize_vals(int64_t s, int64_t N, const T (&f0
         v2 = T(0);
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            Vo[c * N + s] = S(vv[c]);
+            __stcg(Vo + c * N + s, S(vv[c]));
             v2 += vv[c] * vv[c];
         }
     }
@@ -179,16 +179,19 @@ __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __r
                                               const S* __restrict__ L3, const T (&g)[C], T dtt, int nsky,
                                               int unit_length, S* __restrict__ Fo, S* __restrict__ Flo_out,
                                               S* __restrict__ Vo, T& v2) {
+    // the arrays are read-only during stage 4 (it writes the other halves of the
+    // ping-pong pairs): non-coherent global loads (the pointers come from the
+    // descriptor in global memory, so the compiler cannot infer the space itself)
     T f0[C], flo[C], v0[C], a1[C], a2[C], a3[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
         const int64_t j = c * N + s;
-        f0[c] = T(F[j]);
-        flo[c] = Flo_in ? T(Flo_in[j]) : T(0);
-        v0[c] = V ? T(V[j]) : T(0);
-        a1[c] = T(L1[j]);
-        a2[c] = T(L2[j]);
-        a3[c] = T(L3[j]);
+        f0[c] = T(__ldg(F + j));
+        flo[c] = Flo_in ? T(__ldg(Flo_in + j)) : T(0);
+        v0[c] = V ? T(__ldg(V + j)) : T(0);
+        a1[c] = T(__ldg(L1 + j));
+        a2[c] = T(__ldg(L2 + j));
+        a3[c] = T(__ldg(L3 + j));
     }
     finalize_vals<T, S, C>(s, N, f0, flo, Flo_in != nullptr, v0, a1, a2, a3, g, dtt, nsky, unit_length, Fo, Flo_out,
                            Vo, v2);
@@ -271,8 +274,10 @@ __global__ void k_engine_advance(InstDesc<S>* __restrict__ insts, int ninst) {
 // x-planes are staged (sky_march.cuh); the epilogue writes l_s, or applies the
 // RK4 update at stage 4.
 // ---------------------------------------------------------------------------
-template <typename T, int STAGE>
+// CC: components of the theory; the defect correction exists only for CC <= 5.
+template <typename T, int STAGE, int CC>
 struct EngineEpi {
+    static constexpr bool kDefect = CC <= 5;  // instances of this theory can carry a correction
     // inputs of the stage-4 update, read from global memory at the site (prefetching them
     // into shared memory with cp.async measured slower: more instructions and shared memory)
     const T* fin_src[6];  // F, F_lo (null unless compensated), V (null when arrested), l1, l2, l3
@@ -291,32 +296,40 @@ struct EngineEpi {
     T kin_t;
     T* dlt;       // defect correction (null unless defect-corrected)
     int refresh;  // stage 1 of a refresh step: dlt holds g64 of the field; replace it by g64 - g32
+    T d[kDefect ? CC : 1];  // the site's correction
+    // the correction's loads are issued at the start of the site, so that their latency
+    // overlaps the stencil and point arithmetic instead of stalling the epilogue
+    __device__ __forceinline__ void begin_site(int64_t s, int64_t N) {
+        if constexpr (kDefect) {
+            if (dlt) {
+#pragma unroll
+                for (int c = 0; c < CC; ++c) d[c] = __ldcg(dlt + c * N + s);
+            }
+        }
+    }
     template <int C>
     __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g32)[C]) {
+        static_assert(C == CC, "component count");
         T g[C];
-        if (dlt) {
-            // all C loads first (one latency, not C: a store to dlt between them would
-            // keep the compiler from batching them)
-            T d[C];
 #pragma unroll
-            for (int c = 0; c < C; ++c) d[c] = dlt[c * N + s];
-            if (STAGE == 1 && refresh) {   // d = g64(F): the correction becomes g64 - g32(F)
+        for (int c = 0; c < C; ++c) g[c] = g32[c];
+        if constexpr (kDefect) {
+            if (dlt) {
+                if (STAGE == 1 && refresh) {   // d = g64(F): the correction becomes g64 - g32(F)
 #pragma unroll
-                for (int c = 0; c < C; ++c) {
-                    dlt[c * N + s] = d[c] - g32[c];
-                    g[c] = d[c];
+                    for (int c = 0; c < C; ++c) {
+                        __stcg(dlt + c * N + s, d[c] - g32[c]);
+                        g[c] = d[c];
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < C; ++c) g[c] = g32[c] + d[c];
                 }
-            } else {
-#pragma unroll
-                for (int c = 0; c < C; ++c) g[c] = g32[c] + d[c];
             }
-        } else {
-#pragma unroll
-            for (int c = 0; c < C; ++c) g[c] = g32[c];
         }
         if (STAGE < 4) {
 #pragma unroll
-            for (int c = 0; c < C; ++c) out0[c * N + s] = -dtt * g[c];
+            for (int c = 0; c < C; ++c) __stcg(out0 + c * N + s, -dtt * g[c]);
             return;
         }
 #pragma unroll
@@ -341,8 +354,6 @@ struct EngineEpi {
     }
 };
 
-// TMA: planes staged by tensor-memory-accelerator box copies (every instance of
-// the launch has its maps encoded; wide rows).
 template <template <typename> class Th, class M, typename T, int STAGE, int MINB, bool LO = false, bool TMA = false>
 __global__ void __launch_bounds__(M::NTHREADS, MINB)
     k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
@@ -353,10 +364,13 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
     T* sm = reinterpret_cast<T*>(smraw + (TMA ? ((128u - (smem_addr(smraw) & 127u)) & 127u) : 0u));
     __shared__ KSum shk[M::NTHREADS / 32];  // one entry per warp (kept small: two blocks
     __shared__ double shm[M::NTHREADS / 32];  // per SM need all but 1 KB of shared memory)
-    __shared__ uint64_t tma_bar;
-    TmaTile tt{&tma_bar, 0u, {nullptr, nullptr, nullptr}, nullptr};
+    __shared__ uint64_t tma_bar[2];
+    TmaTile tt{tma_bar, 0u, {nullptr, nullptr, nullptr}, nullptr};
     if constexpr (TMA) {
-        if (threadIdx.x == 0 && threadIdx.y == 0) mbar_init(&tma_bar, 1);
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            mbar_init(&tma_bar[0], 1);
+            mbar_init(&tma_bar[1], 1);
+        }
         __syncthreads();
     }
     for (int t = t_begin + blockIdx.x; t < t_end; t += gridDim.x) {
@@ -375,7 +389,7 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
         const T* const src[3] = {F, LO ? in.Flo[parity] : V, STAGE == 3 ? in.L[0] : in.L[1]};
         const T a = STAGE == 4 ? dtt : hdt;
         const T b = STAGE == 3 ? T(0.25) * dtt : T(0.5) * dtt;
-        EngineEpi<T, STAGE> epi{{F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2]},
+        EngineEpi<T, STAGE, M::C> epi{{F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2]},
                                 STAGE < 4 ? in.L[STAGE - 1] : in.F[parity ^ 1],
                                 STAGE < 4 ? nullptr : in.V[parity ^ 1],
                                 in.Flo[parity ^ 1],
@@ -388,7 +402,7 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
             tt.map[2] = NSRC > 2 ? &in.tm[kMapL + (STAGE == 3 ? 0 : 1)] : nullptr;
             tt.status = in.status;
         }
-        if (!march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE>, LO, T, true, TMA>(
+        if (!march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE, M::C>, LO, T, true, TMA>(
                 sm, p, src, a, b, xa, xe, y0, z0, epi, es, bs, TMA ? &tt : nullptr))
             return;  // a copy did not arrive: the block's error bit is set, its partials stay stale
         if (STAGE == 1) {

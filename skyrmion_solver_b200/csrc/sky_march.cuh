@@ -61,19 +61,36 @@ struct MarchShape {
     static constexpr size_t smem_bytes(int nsrc, bool lo = false) {
         return size_t(RING) * (lo ? 2 : 1) * SLOT * sizeof(T) + size_t(staged<T, S>(nsrc)) * SLOT * sizeof(S);
     }
-    // TMA staging (wide rows): a six-slot ring into which the copy engine writes
-    // the first source (and, for a compensated field, a second six-slot ring for
-    // the low parts), plus one staging slot for each further source
+    // TMA staging (wide rows): a ring into which the copy engine writes the first
+    // source (5 + LA slots for LA planes in flight; a compensated field's low parts
+    // get a second ring), plus LA staging slots for each further source.  Two planes
+    // are kept in flight when that fits one block's shared memory, else one.
+    static constexpr size_t tma_slots(int nsrc, bool lo, int la) {
+        return lo ? 2 * size_t(RING + la) : size_t(RING + la) + size_t(la) * size_t(nsrc - 1);
+    }
+    template <typename T>
+    static constexpr int tma_lookahead(int nsrc, bool lo = false) {
+        return (!lo && tma_slots(nsrc, lo, 2) * SLOT * sizeof(T) + 128 <= kMaxSmemPerBlock) ? 2 : 1;
+    }
     template <typename T>
     static constexpr size_t smem_bytes_tma(int nsrc, bool lo = false) {
-        return (lo ? 12 : 6 + (nsrc - 1)) * size_t(SLOT) * sizeof(T);
+        return tma_slots(nsrc, lo, tma_lookahead<T>(nsrc, lo)) * size_t(SLOT) * sizeof(T);
     }
 };
 
-// Per-tile TMA state of a marching kernel: the kernel's mbarrier (initialised
-// once per launch), the parity of the phase the next plane completes, the maps
-// of the tile's sources (null: the source reads as zero) and the launch-wide
-// error word that a timed-out wait sets.
+// Whether an epilogue wants a call at the start of each site (before the stencil
+// arithmetic), e.g. to issue the global loads its operator() will consume.
+template <class E, class = void>
+struct HasBeginSite : std::false_type {};
+template <class E>
+struct HasBeginSite<E, std::void_t<decltype(std::declval<E&>().begin_site(int64_t(0), int64_t(0)))>>
+    : std::true_type {};
+
+// Per-tile TMA state of a marching kernel: the kernel's two mbarriers
+// (initialised once per launch; planes alternate between them when two are in
+// flight), the parity bit of the phase each one completes next, the maps of the
+// tile's sources (null: the source reads as zero) and the launch-wide error word
+// that a timed-out wait sets.
 struct TmaTile {
     uint64_t* bar;
     uint32_t phase;
@@ -333,10 +350,12 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
     constexpr int NST = M::template staged<T, S>(NSRC);  // sources staged in shared memory
     static_assert(NST == NSRC || !M::WIDE, "the unstaged third source is read with narrow-row offsets");
     static_assert(!TMA || (M::WIDE && std::is_same<S, T>::value && NST == NSRC), "TMA staging: wide rows, S = T");
-    constexpr int R = (DIRECT || TMA) ? M::RING + 1 : M::RING;  // ring slots
+    // planes in flight ahead of the one being consumed (TMA), and ring slots
+    constexpr int LA = TMA ? M::template tma_lookahead<T>(NSRC, LO) : 1;
+    constexpr int R = TMA ? M::RING + LA : (DIRECT ? M::RING + 1 : M::RING);
     constexpr int DST = DIRECT ? R * M::SLOT : M::SLOT;  // distance between the sources' copies
     // shared memory: DIRECT: ring (R slots) [+ low-part ring (R slots)];
-    // TMA: ring (6 slots) + NSRC - 1 staging slots;
+    // TMA: ring (R slots) + LA buffers of NSRC - 1 staging slots;
     // otherwise: ring (5 slots) + NSRC staging slots of S
     T* ring = sm;
     S* stage = reinterpret_cast<S*>(sm + (TMA ? R : M::RING) * M::SLOT);
@@ -374,42 +393,48 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
     // lattice arrives as zeros); source 0 into ring slot dslot, the low parts into the
     // low-part ring, further sources into the staging slots
     const int tid0 = threadIdx.x + M::BZ * threadIdx.y;
-    auto issue_tma = [&](int qq, int dslot) {
+    // buffer b (mbarrier b, staging buffer b) carries planes q0 + b, q0 + b + LA, ...
+    auto issue_tma = [&](int qq, int dslot, int b) {
         if (tid0 != 0) return;
         constexpr uint32_t box = uint32_t(M::SLOT * sizeof(T));
         uint32_t n = 1;
 #pragma unroll
         for (int k = 1; k < NSRC; ++k) n += tma->map[k] != nullptr ? 1u : 0u;
+        uint64_t* bar = tma->bar + b;
+        T* stg = reinterpret_cast<T*>(stage) + b * (NSRC - 1) * M::SLOT;
         fence_proxy_async_smem();
-        mbar_arrive_expect_tx(tma->bar, n * box);
+        mbar_arrive_expect_tx(bar, n * box);
         const int zc = z0 - M::ZOFF, yc = y0 - 2;
-        tma_load_plane(ring + dslot * M::SLOT, tma->map[0], zc, yc, qq, 0, tma->bar);
+        tma_load_plane(ring + dslot * M::SLOT, tma->map[0], zc, yc, qq, 0, bar);
 #pragma unroll
         for (int k = 1; k < NSRC; ++k) {
             if (tma->map[k] == nullptr) continue;
-            T* dst = LO ? ring_lo + dslot * M::SLOT : reinterpret_cast<T*>(stage) + (k - 1) * M::SLOT;
-            tma_load_plane(dst, tma->map[k], zc, yc, qq, 0, tma->bar);
+            T* dst = LO ? ring_lo + dslot * M::SLOT : stg + (k - 1) * M::SLOT;
+            tma_load_plane(dst, tma->map[k], zc, yc, qq, 0, bar);
         }
     };
     __syncthreads();
-    if constexpr (TMA)
-        issue_tma(q0, 0);
-    else
+    if constexpr (TMA) {
+        issue_tma(q0, 0, 0);
+        if (LA > 1 && q0 + 1 <= q1) issue_tma(q0 + 1, 1, 1);
+    } else {
         issue((int64_t)q0 * YZ, q0 >= 0 && q0 < p.X, 0);
+    }
     int slot = 0;  // ring slot of plane q
     for (int q = q0; q <= q1; ++q) {
         if constexpr (TMA) {
             // plane q has landed; for further sources, add a V + b L into the ring slot
-            const bool ok = mbar_wait_bounded(tma->bar, tma->phase);
-            tma->phase ^= 1u;
+            const int b = LA > 1 ? ((q - q0) & 1) : 0;
+            const bool ok = mbar_wait_bounded(tma->bar + b, (tma->phase >> b) & 1u);
+            tma->phase ^= 1u << b;
             if constexpr (!DIRECT) {
                 using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
                 constexpr int VW = 16 / int(sizeof(T));
                 constexpr int NV = M::SLOT / VW;
                 static_assert(M::SLOT % VW == 0, "slot of whole 16-byte vectors");
                 V4* dstv = reinterpret_cast<V4*>(ring + slot * M::SLOT);
-                const V4* s1 = reinterpret_cast<const V4*>(stage);
-                const V4* s2 = reinterpret_cast<const V4*>(stage) + NV;
+                const V4* s1 = reinterpret_cast<const V4*>(stage) + b * (NSRC - 1) * NV;
+                const V4* s2 = s1 + NV;
                 const bool h1 = tma->map[1] != nullptr;
                 const bool h2 = NSRC > 2 && tma->map[2] != nullptr;
                 if (h1 || h2) {
@@ -432,16 +457,17 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
                     }
                 }
             }
-            // every thread has its plane q (and finished the centre of plane q - 1):
-            // the slot of plane q - 5 and the staging slots are free for plane q + 1
+            // every thread has its plane q (and finished the centre of plane q - 1): the
+            // ring slot of plane q - 5 and staging buffer b are free for plane q + LA
             if (__syncthreads_or(ok ? 0 : 1)) {
                 if (tid0 == 0) {
                     atomicOr(tma->status, 1);
-                    mbar_wait_bounded(tma->bar, tma->phase ^ 1u);  // let a late copy land before exiting
+                    // let late copies land before the block exits
+                    for (int k = 0; k < LA; ++k) mbar_wait_bounded(tma->bar + k, (tma->phase >> k) & 1u);
                 }
                 return false;
             }
-            if (q < q1) issue_tma(q + 1, slot + 1 == R ? 0 : slot + 1);
+            if (q + LA <= q1) issue_tma(q + LA, (slot + LA) % R, b);
         } else if constexpr (DIRECT) {
             cp_async_wait_all();
             // (A) plane q has landed for every thread, and every thread finished the
@@ -491,6 +517,7 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
             // (its FP64 sum needs no more than FP32 per-site accuracy; only the energy, which
             // decides the arrest, is evaluated in FP64)
             [[maybe_unused]] double b32 = 0.0;
+            if constexpr (HasBeginSite<Epi>::value) epi.begin_site(s, N);
             if constexpr (GRAD) {
             T phi[C], D[3][C], Sd[6][C], g[C];
 #pragma unroll
