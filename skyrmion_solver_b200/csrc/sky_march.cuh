@@ -393,15 +393,16 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
     // lattice arrives as zeros); source 0 into ring slot dslot, the low parts into the
     // low-part ring, further sources into the staging slots
     const int tid0 = threadIdx.x + M::BZ * threadIdx.y;
-    // buffer b (mbarrier b, staging buffer b) carries planes q0 + b, q0 + b + LA, ...
-    auto issue_tma = [&](int qq, int dslot, int b) {
+    // buffer nb (mbarrier nb, staging buffer nb) carries planes q0 + nb, q0 + nb + LA, ...
+    // (named apart from the combine weight b of the third source)
+    auto issue_tma = [&](int qq, int dslot, int nb) {
         if (tid0 != 0) return;
         constexpr uint32_t box = uint32_t(M::SLOT * sizeof(T));
         uint32_t n = 1;
 #pragma unroll
         for (int k = 1; k < NSRC; ++k) n += tma->map[k] != nullptr ? 1u : 0u;
-        uint64_t* bar = tma->bar + b;
-        T* stg = reinterpret_cast<T*>(stage) + b * (NSRC - 1) * M::SLOT;
+        uint64_t* bar = tma->bar + nb;
+        T* stg = reinterpret_cast<T*>(stage) + nb * (NSRC - 1) * M::SLOT;
         fence_proxy_async_smem();
         mbar_arrive_expect_tx(bar, n * box);
         const int zc = z0 - M::ZOFF, yc = y0 - 2;
@@ -424,16 +425,16 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
     for (int q = q0; q <= q1; ++q) {
         if constexpr (TMA) {
             // plane q has landed; for further sources, add a V + b L into the ring slot
-            const int b = LA > 1 ? ((q - q0) & 1) : 0;
-            const bool ok = mbar_wait_bounded(tma->bar + b, (tma->phase >> b) & 1u);
-            tma->phase ^= 1u << b;
+            const int nb = LA > 1 ? ((q - q0) & 1) : 0;
+            const bool ok = mbar_wait_bounded(tma->bar + nb, (tma->phase >> nb) & 1u);
+            tma->phase ^= 1u << nb;
             if constexpr (!DIRECT) {
                 using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
                 constexpr int VW = 16 / int(sizeof(T));
                 constexpr int NV = M::SLOT / VW;
                 static_assert(M::SLOT % VW == 0, "slot of whole 16-byte vectors");
                 V4* dstv = reinterpret_cast<V4*>(ring + slot * M::SLOT);
-                const V4* s1 = reinterpret_cast<const V4*>(stage) + b * (NSRC - 1) * NV;
+                const V4* s1 = reinterpret_cast<const V4*>(stage) + nb * (NSRC - 1) * NV;
                 const V4* s2 = s1 + NV;
                 const bool h1 = tma->map[1] != nullptr;
                 const bool h2 = NSRC > 2 && tma->map[2] != nullptr;
@@ -457,8 +458,13 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
                     }
                 }
             }
+            // the ring slots are written by ordinary stores (the combine above) and read by
+            // ordinary loads, and later overwritten by the copy engine: every thread orders
+            // its own generic accesses before those async-proxy writes, and the barrier
+            // then orders all threads' accesses before the next copy is issued
+            fence_proxy_async_smem();
             // every thread has its plane q (and finished the centre of plane q - 1): the
-            // ring slot of plane q - 5 and staging buffer b are free for plane q + LA
+            // ring slot of plane q - 5 and staging buffer nb are free for plane q + LA
             if (__syncthreads_or(ok ? 0 : 1)) {
                 if (tid0 == 0) {
                     atomicOr(tma->status, 1);
@@ -467,7 +473,7 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
                 }
                 return false;
             }
-            if (q + LA <= q1) issue_tma(q + LA, (slot + LA) % R, b);
+            if (q + LA <= q1) issue_tma(q + LA, (slot + LA) % R, nb);
         } else if constexpr (DIRECT) {
             cp_async_wait_all();
             // (A) plane q has landed for every thread, and every thread finished the
