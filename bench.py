@@ -301,6 +301,90 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# the reference's own Numba-CUDA run on this GPU (installed under baseline/_ref)
+# ---------------------------------------------------------------------------
+
+NUMBA_STEPS = 3        # reference steps compared step by step with the drop-in path
+NUMBA_TIMED = 10       # reference steps timed after them
+
+
+def run_numba_reference(args):
+    """Worker: the reference's unmodified Simulation (core/simulation.py:287-308, do_arrested_newton_flow of
+    core/integrator.py:284-410) with its own omega theory kernels, compiled by Numba for this GPU, on the
+    workload field read from args.field.  Prints one JSON line: per-step (energy, err) of the first
+    NUMBA_STEPS steps, the wall time per step of NUMBA_TIMED more (each step ends in cuda.synchronize)."""
+    import numpy as np
+    out = {"impl": "reference-numba-cuda", "workload": WORKLOAD}
+    try:
+        from tests import _reference as R
+        if not R.available():
+            raise RuntimeError("the reference is not installed under baseline/_ref")
+        from numba import cuda
+        theories, Simulation, _ = R.load(("omega",))
+        th = theories["omega"]
+        p = th.params.Params(xlen=L, ylen=L, zlen=L, lsx=H, lsy=H, lsz=H, xsize=H * (L - 1), ysize=H * (L - 1),
+                             zsize=H * (L - 1), time_step=DT_FACTOR * H, **COUPLINGS)
+        sim = Simulation(p, th)
+        field = np.load(args.field)
+        sim.Field.copy_to_device(np.ascontiguousarray(field.ravel()))
+        sim.Velocity.copy_to_device(np.zeros(field.size))
+        e = sim.observables()["energy"]
+        out["energy0"] = e
+        t0 = time.perf_counter()
+        steps = []
+        for _ in range(NUMBA_STEPS):       # the first includes Numba's compilation of every kernel
+            e, err = sim.step(e)
+            steps.append((float(e), float(err)))
+        cuda.synchronize()
+        out["first_steps_s"] = time.perf_counter() - t0
+        out["steps"] = steps
+        t0 = time.perf_counter()
+        for _ in range(NUMBA_TIMED):
+            e, err = sim.step(e)
+        cuda.synchronize()
+        out["ms_per_step"] = (time.perf_counter() - t0) * 1e3 / NUMBA_TIMED
+        out["timed_steps"] = NUMBA_TIMED
+        out["device"] = cuda.get_current_device().name.decode() if isinstance(
+            cuda.get_current_device().name, bytes) else str(cuda.get_current_device().name)
+    except Exception as ex:  # reported as unavailable, with the reason
+        out["unavailable"] = f"{type(ex).__name__}: {ex}"[:400]
+    emit(out)
+    return 0
+
+
+def numba_reference_record(field, p, th, timeout_s=900):
+    """Run the Numba-CUDA reference on `field` in a child process and compare its first steps with the
+    drop-in path (this package's FP64 reference-layout kernels) from the same field."""
+    import numpy as np
+    import torch
+    from skyrmion_solver_b200.core.simulation import Simulation
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "field.npy")
+        np.save(path, field.detach().cpu().numpy())
+        try:
+            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--numba-reference", "--field", path],
+                               capture_output=True, text=True, timeout=timeout_s, cwd=ROOT)
+            lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+            rec = json.loads(lines[-1]) if lines else {"unavailable": (r.stderr or r.stdout)[-400:]}
+        except subprocess.TimeoutExpired:
+            rec = {"unavailable": f"the reference's Numba-CUDA run did not finish within {timeout_s} s"}
+    if "steps" in rec:
+        sim = Simulation(p, th)
+        sim.Field.copy_(field)
+        sim.Velocity.zero_()
+        e = sim.observables()["energy"]
+        rel = [abs(e - rec["energy0"]) / abs(rec["energy0"])]
+        for (er, errr) in rec["steps"]:
+            e, err = sim.step(e)
+            rel.append(abs(e - er) / abs(er))
+        torch.cuda.synchronize()
+        rec["drop_in_max_rel_energy_diff"] = max(rel)
+        rec["drop_in_energy_diffs"] = rel
+        del sim
+    return rec
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 
@@ -424,6 +508,9 @@ def run_ours(args):
     plain_ms = max_over_ranks([t0.elapsed_time(t1) / nplain], device=dev)[0]
     del sim
 
+    numba_ref = None
+    if not args.quick and not args.no_numba and rank == 0:
+        numba_ref = numba_reference_record(field, p, th)
     solve = None
     ref = None
     if not args.quick:
@@ -492,6 +579,11 @@ def run_ours(args):
         if value and plain.get("solves_per_s"):
             plain["speedup"] = value / plain["solves_per_s"]
             plain["speedup_vs_engine_fp64"] = value / plain["engine_fp64_solves_per_s"]
+    if numba_ref is not None and numba_ref.get("ms_per_step") and ok(ref):
+        # the reference's own plain FP64 run takes the FP64 engine's observed step count
+        numba_ref["solves_per_s"] = world / (ref["steps"] * numba_ref["ms_per_step"] * 1e-3)
+        if value:
+            numba_ref["value_over_this"] = value / numba_ref["solves_per_s"]
     field_bytes = C * N * 8
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": warmup,
@@ -525,6 +617,7 @@ def run_ours(args):
                              "compensated field's low parts and the defect correction",
                      "launch_ms": stages[dom], "stage_ms": stages},
         "plain_fp64": plain,
+        "reference_numba_cuda": numba_ref,
         "e2e": {"value": e2e_value, "unit": UNIT,
                 "h2d_bytes_per_step": field_bytes / solve["steps"] if solve else None,
                 "d2h_bytes_per_step": (64 * (solve["steps"] // args.chunk + 1) + field_bytes) / solve["steps"]
@@ -970,6 +1063,9 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--quick", action="store_true", help="skip the two timed solves (K-step rate only)")
+    ap.add_argument("--no-numba", action="store_true", help="skip the reference's Numba-CUDA run")
+    ap.add_argument("--numba-reference", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--field", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--chunk", type=int, default=128, help="steps between convergence checks of a solve")
     ap.add_argument("--staging", choices=("tma", "cp.async"), default="tma",
                     help="how the engine's stage kernels stage lattice planes in shared memory")
@@ -1012,6 +1108,8 @@ def main():
         if args.max_steps == 240000:
             args.max_steps = 60000
         return run_serve(args)
+    if args.numba_reference:
+        return run_numba_reference(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -63,14 +63,21 @@ struct MarchShape {
     }
     // TMA staging (wide rows): a ring into which the copy engine writes the first
     // source (5 + LA slots for LA planes in flight; a compensated field's low parts
-    // get a second ring), plus LA staging slots for each further source.  Two planes
-    // are kept in flight when that fits one block's shared memory, else one.
+    // get a second ring), plus LA staging slots for each further source.
+    // kTmaPlanesInFlight planes are kept in flight when that fits one block's shared
+    // memory.  One is the default: on the omega 128^3 FP32 stages two planes in flight
+    // measured no faster for stages 2 and 3 (80.5 against 79.5 us, 80.8 against 82.3 us)
+    // and slower for stage 4 (152 against 140 us), whose larger shared-memory share
+    // leaves less L1 for the update's global loads.
+    static constexpr int kTmaPlanesInFlight = 1;
     static constexpr size_t tma_slots(int nsrc, bool lo, int la) {
         return lo ? 2 * size_t(RING + la) : size_t(RING + la) + size_t(la) * size_t(nsrc - 1);
     }
     template <typename T>
     static constexpr int tma_lookahead(int nsrc, bool lo = false) {
-        return (!lo && tma_slots(nsrc, lo, 2) * SLOT * sizeof(T) + 128 <= kMaxSmemPerBlock) ? 2 : 1;
+        return (kTmaPlanesInFlight > 1 && !lo && tma_slots(nsrc, lo, 2) * SLOT * sizeof(T) + 128 <= kMaxSmemPerBlock)
+                   ? 2
+                   : 1;
     }
     template <typename T>
     static constexpr size_t smem_bytes_tma(int nsrc, bool lo = false) {

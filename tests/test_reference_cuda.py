@@ -1,0 +1,81 @@
+"""The reference's own code on the GPU (Numba-CUDA), from the copy installed under baseline/_ref.
+
+1. Drop-in: the reference's unmodified ``Simulation`` class (core/simulation.py) built with this
+   package's theory module (params, kernels, observables).  Its ``step`` runs the reference's own
+   ``do_arrested_newton_flow`` (core/integrator.py:284-410), its own Numba RK4 stage and finalize
+   kernels and its own max reduction, and calls this package's gradient launchable and energy
+   observable on Numba device arrays.  Three steps from the golden inputs match the golden steps
+   that the reference produced (1e-10 relative per step, as the other step parity tests).
+2. The reference's own theory kernels (its Numba gradient, energy and norm kernels) and this
+   package's drop-in path agree step by step from the same field (1e-10 relative energy).
+
+Skipped when the reference is not installed (``tests/_reference.py`` says how to install it).
+"""
+import numpy as np
+import pytest
+
+from tests import _golden as G
+from tests import _reference as R
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not R.available(), reason="the reference is not installed under baseline/_ref")]
+
+STEP_TOL = 1e-10
+
+
+@pytest.mark.parametrize("name", ["nuclear", "omega", "rho"])
+def test_reference_simulation_drives_this_packages_theory(name):
+    from skyrmion_solver_b200 import theories as T
+    from tests.golden.make_golden import theory_params
+    _, Simulation, _ = R.load(())
+    th = T.by_short_name(name)
+    d = G.load(name)
+    sim = Simulation(theory_params(name, th).resolved(), th)      # the reference's own class
+    assert np.array_equal(sim.p_i_h, d["p_i"]) and np.array_equal(sim.p_f_h, d["p_f"])
+    shp = d["field0"].shape
+    sim.Field.copy_to_device(np.ascontiguousarray(d["field0"].ravel()))
+    sim.Velocity.copy_to_device(np.ascontiguousarray(d["velocity0"].ravel()))
+    for s in range(len(d["energies"])):
+        E, err = sim.step(float(d[f"prev{s}"]))
+        assert abs(E - d["energies"][s]) <= STEP_TOL * abs(d["energies"][s]), (s, E, d["energies"][s])
+        assert abs(err - d["errs"][s]) <= STEP_TOL * abs(d["errs"][s])
+        assert G.rel_err(sim.Field.copy_to_host().reshape(shp), d[f"field{s + 1}"]) <= STEP_TOL
+        v = sim.Velocity.copy_to_host().reshape(shp)
+        if np.any(d[f"velocity{s + 1}"]):
+            assert G.rel_err(v, d[f"velocity{s + 1}"]) <= STEP_TOL
+        else:
+            assert not np.any(v)
+
+
+@pytest.mark.parametrize("name", ["omega"])
+def test_reference_kernels_and_drop_in_agree(name):
+    """The reference's own theory on a 40 x 36 x 44 lattice with seeded off-sphere inputs against
+    this package's Simulation (the same reference layout, FP64), three steps."""
+    import torch
+    from skyrmion_solver_b200 import theories as T
+    from skyrmion_solver_b200.core.simulation import Simulation as OurSimulation
+    from tests.test_march import inputs
+    theories, Simulation, _ = R.load((name,))
+    ref_th = theories[name]
+    dims, h = (40, 36, 44), (0.2, 0.2, 0.2)
+    kw = dict(xlen=dims[0], ylen=dims[1], zlen=dims[2], lsx=h[0], lsy=h[1], lsz=h[2], xsize=h[0] * (dims[0] - 1),
+              ysize=h[1] * (dims[1] - 1), zsize=h[2] * (dims[2] - 1), time_step=0.04)
+    ref = Simulation(ref_th.params.Params(**kw), ref_th)
+    ours = OurSimulation(T.by_short_name(name).params.default_params(**kw), T.by_short_name(name))
+    assert np.array_equal(ref.p_i_h, ours.p_i_h) and np.array_equal(ref.p_f_h, ours.p_f_h)
+    F, V = inputs(int(ref.p_i_h[5]), dims, h=h, seed=11)
+    ref.Field.copy_to_device(np.ascontiguousarray(F.ravel()))
+    ref.Velocity.copy_to_device(np.ascontiguousarray(V.ravel()))
+    ours.Field.copy_(torch.from_numpy(F.ravel()))
+    ours.Velocity.copy_(torch.from_numpy(V.ravel()))
+    er = ref.observables()["energy"]
+    eo = ours.observables()["energy"]
+    assert abs(er - eo) <= STEP_TOL * abs(er)
+    for s in range(3):
+        er, errr = ref.step(er)
+        eo, erro = ours.step(eo)
+        assert abs(er - eo) <= STEP_TOL * abs(er), (s, er, eo)
+        assert abs(errr - erro) <= STEP_TOL * max(1.0, abs(errr)), (s, errr, erro)
+    fr = ref.Field.copy_to_host()
+    fo = ours.Field.cpu().numpy()
+    assert G.rel_err(fo, fr) <= STEP_TOL
