@@ -114,9 +114,7 @@ static bool wide_ok(int prec, int Z) { return Z % (prec ? 2 : 4) == 0; }
 template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false>
 static size_t stage_smem() {
     using M = MShape<Th, T, WIDE>;
-    // TMA: 128 bytes of slack to start the ring on a 128-byte boundary
-    return TMA ? M::template smem_bytes_tma<T>(LO ? 2 : stage_nsrc<STAGE>(), LO) + 128
-               : M::template smem_bytes<T>(LO ? 2 : stage_nsrc<STAGE>(), LO);
+    return stage_smem_bytes<M, T, STAGE, march_minb<Th, T>(), LO, TMA>();
 }
 
 template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false>
@@ -394,10 +392,15 @@ __global__ void k_f32c_to_f64(int64_t n, const float* __restrict__ hi, const flo
 // plane x C components, the marching kernels' wide-row plane).
 template <typename S>
 static int encode_maps(const HostInst& h, InstDesc<S>& d, int by) {
-    const void* arrs[kNumMaps] = {h.F[0], h.F[1], h.Flo[0], h.Flo[1], h.V[0], h.V[1], h.L[0], h.L[1], h.L[2]};
-    for (int k = 0; k < kNumMaps; ++k) {
+    const void* arrs[kNumCentreMaps] = {h.F[0], h.F[1], h.Flo[0], h.Flo[1], h.V[0], h.V[1],
+                                        h.L[0], h.L[1], h.L[2], h.Dlt};
+    for (int k = 0; k < kNumCentreMaps; ++k) {
         if (!arrs[k]) continue;
-        int rc = encode_plane_map(&d.tm[k], arrs[k], (int)sizeof(S), h.p.X, h.p.Y, h.p.Z, h.C, 40, by + 4);
+        int rc = SKY_OK;
+        if (k < kNumMaps)
+            rc = encode_plane_map(&d.tm[k], arrs[k], (int)sizeof(S), h.p.X, h.p.Y, h.p.Z, h.C, 40, by + 4);
+        // centre box: the tile's 32 z-values x BY rows, no halo
+        if (!rc) rc = encode_plane_map(&d.tmc[k], arrs[k], (int)sizeof(S), h.p.X, h.p.Y, h.p.Z, h.C, 32, by);
         if (rc) return rc;
     }
     return SKY_OK;

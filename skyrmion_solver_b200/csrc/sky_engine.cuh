@@ -41,12 +41,16 @@ struct StepStats {
 };
 
 // Roles of an instance's TMA plane maps (InstDesc::tm).
-enum { kMapF = 0, kMapFlo = 2, kMapV = 4, kMapL = 6, kNumMaps = 9 };
+// Plane maps (tm) cover a tile's haloed plane, centre maps (tmc) its BY x 32 sites
+// (the stage-4 update's operands, which need no halo); the centre maps add the
+// defect correction at kMapDlt.
+enum { kMapF = 0, kMapFlo = 2, kMapV = 4, kMapL = 6, kNumMaps = 9, kMapDlt = 9, kNumCentreMaps = 10 };
 
 // Device-resident state of one instance.
 template <typename S>
 struct InstDesc {
     TmaMap tm[kNumMaps];  // plane maps of F[0..1], Flo[0..1], V[0..1], L[0..2] (when tma is set)
+    TmaMap tmc[kNumCentreMaps];  // centre maps of the same arrays and of Dlt (when tma is set)
     int tma;              // the stage kernels stage this instance's planes with TMA
     int* status;          // the engine's error word (bit 0: a wait for a TMA copy gave up)
     Params p;
@@ -274,8 +278,25 @@ __global__ void k_engine_advance(InstDesc<S>* __restrict__ insts, int ninst) {
 // x-planes are staged (sky_march.cuh); the epilogue writes l_s, or applies the
 // RK4 update at stage 4.
 // ---------------------------------------------------------------------------
+// The stage-4 update's operands for one plane of a tile, staged by TMA centre-box
+// copies into shared memory (k_march_stage with TMA; sky_march.cuh, the plane_begin
+// hook): F, F_lo, V, l1, l2, l3 and the defect correction, each C x BY x 32 values in
+// [c][y][z] order; a null map means the operand is absent (reads as zero).
+template <typename T>
+struct CentreStage {
+    T* buf;                     // kCentreArrays boxes
+    uint64_t* bar;              // the mbarrier the copies complete on
+    const TmaMap* map[7];       // F, F_lo, V, l1, l2, l3, Dlt
+    int* status;                // the engine's error word (bit 1: a centre-box wait gave up)
+    int z0, y0, box;            // tile origin; values per box
+    uint32_t phase;             // parity of the copies' next phase
+    uint32_t pending;           // parity of the phase this plane's copies complete
+};
+constexpr int kCentreArrays = 7;
+
 // CC: components of the theory; the defect correction exists only for CC <= 5.
-template <typename T, int STAGE, int CC>
+// CENTRE: stage 4 reads the update's operands from shared memory (CentreStage).
+template <typename T, int STAGE, int CC, bool CENTRE = false>
 struct EngineEpi {
     static constexpr bool kDefect = CC <= 5;  // instances of this theory can carry a correction
     // inputs of the stage-4 update, read from global memory at the site (prefetching them
@@ -296,14 +317,46 @@ struct EngineEpi {
     T kin_t;
     T* dlt;       // defect correction (null unless defect-corrected)
     int refresh;  // stage 1 of a refresh step: dlt holds g64 of the field; replace it by g64 - g32
-    T d[kDefect ? CC : 1];  // the site's correction
-    // the correction's loads are issued at the start of the site, so that their latency
-    // overlaps the stencil and point arithmetic instead of stalling the epilogue
-    __device__ __forceinline__ void begin_site(int64_t s, int64_t N) {
+    CentreStage<T>* cs = nullptr;  // CENTRE: the plane's staged operands
+    T d[kDefect ? CC : 1];   // the site's correction
+    T dn[kDefect ? CC : 1];  // the correction of the thread's site on the next plane, in flight
+    int64_t dn_site = -1;    // the site dn belongs to
+    // CENTRE: thread 0 copies the update's operands of plane x (every thread calls this
+    // right after the plane barrier, before the stencil arithmetic).
+    __device__ __forceinline__ void plane_begin(int x) {
+        if constexpr (CENTRE) {
+            cs->pending = cs->phase;
+            cs->phase ^= 1u;
+            if (threadIdx.x == 0 && threadIdx.y == 0) {
+                uint32_t n = 0;
+#pragma unroll
+                for (int k = 0; k < kCentreArrays; ++k) n += cs->map[k] != nullptr ? 1u : 0u;
+                mbar_arrive_expect_tx(cs->bar, n * uint32_t(cs->box * sizeof(T)));
+#pragma unroll
+                for (int k = 0; k < kCentreArrays; ++k)
+                    if (cs->map[k]) tma_load_plane(cs->buf + k * cs->box, cs->map[k], cs->z0, cs->y0, x, 0, cs->bar);
+            }
+        }
+    }
+    // A thread walks its (y, z) column along x.  The correction of the next plane's
+    // site is loaded while this site is computed, so that its global-memory latency
+    // overlaps a whole plane of stencil and point arithmetic.
+    __device__ __forceinline__ void begin_site(int64_t s, int64_t N, int64_t next) {
+        if constexpr (CENTRE) return;  // the correction comes with the staged operands
         if constexpr (kDefect) {
             if (dlt) {
+                if (dn_site == s) {
 #pragma unroll
-                for (int c = 0; c < CC; ++c) d[c] = __ldcg(dlt + c * N + s);
+                    for (int c = 0; c < CC; ++c) d[c] = dn[c];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < CC; ++c) d[c] = __ldcg(dlt + c * N + s);
+                }
+                if (next >= 0) {
+#pragma unroll
+                    for (int c = 0; c < CC; ++c) dn[c] = __ldcg(dlt + c * N + next);
+                }
+                dn_site = next;
             }
         }
     }
@@ -313,6 +366,38 @@ struct EngineEpi {
         T g[C];
 #pragma unroll
         for (int c = 0; c < C; ++c) g[c] = g32[c];
+        if constexpr (CENTRE) {
+            static_assert(STAGE == 4, "staged operands are the stage-4 update's");
+            if (!mbar_wait_bounded(cs->bar, cs->pending)) atomicOr(cs->status, 2);
+            // the thread's site within the staged boxes: [c][ty][tx]
+            const int o = threadIdx.y * 32 + threadIdx.x;
+            const int bx = cs->box / C;
+            T f0[C], flo[C], v0[C], a1[C], a2[C], a3[C];
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const int j = c * bx + o;
+                f0[c] = cs->buf[j];
+                flo[c] = cs->map[1] ? cs->buf[cs->box + j] : T(0);
+                v0[c] = cs->map[2] ? cs->buf[2 * cs->box + j] : T(0);
+                a1[c] = cs->buf[3 * cs->box + j];
+                a2[c] = cs->buf[4 * cs->box + j];
+                a3[c] = cs->buf[5 * cs->box + j];
+                if (cs->map[6]) g[c] += cs->buf[6 * cs->box + j];
+            }
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                gmx = fmax(gmx, g[c]);
+                gab = fmax(gab, fabs(g[c]));
+            }
+            T v2;
+            finalize_vals<T, T, C>(s, N, f0, flo, cs->map[1] != nullptr, v0, a1, a2, a3, g, dtt, nsky, unit_length,
+                                   out0, Flo_out, out1, v2);
+            if constexpr (sizeof(T) == 8)
+                ksum_add(kin, hvol * v2);
+            else
+                kin_t += hvol * v2;
+            return;
+        }
         if constexpr (kDefect) {
             if (dlt) {
                 if (STAGE == 1 && refresh) {   // d = g64(F): the correction becomes g64 - g32(F)
@@ -354,24 +439,57 @@ struct EngineEpi {
     }
 };
 
+// Shared memory of a stage launch: the plane pipeline (sky_march.cuh), plus for a TMA
+// stage 4 the staged update operands when they fit (two FP32 blocks per SM keep
+// 2 x (dynamic + 1.3 KB) within the SM's 228 KB).
+template <class M, typename T>
+constexpr size_t centre_bytes() {
+    return size_t(kCentreArrays) * M::C * M::BY * M::BZ * sizeof(T);
+}
+template <class M, typename T, int STAGE, int MINB, bool TMA>
+constexpr bool stage_centre() {
+    return STAGE == 4 && TMA &&
+           M::template smem_bytes_tma<T>(3) + centre_bytes<M, T>() + 128 <= (MINB >= 2 ? 115000 : kMaxSmemPerBlock);
+}
+template <class M, typename T, int STAGE, int MINB, bool LO, bool TMA>
+constexpr size_t stage_smem_bytes() {
+    constexpr int nsrc = LO ? 2 : (STAGE == 1 ? 1 : (STAGE == 2 ? 2 : 3));
+    return TMA ? M::template smem_bytes_tma<T>(nsrc, LO) + 128 +
+                     (stage_centre<M, T, STAGE, MINB, TMA>() ? centre_bytes<M, T>() : 0)
+               : M::template smem_bytes<T>(nsrc, LO);
+}
+
+// TMA: planes staged by tensor-memory-accelerator box copies (every instance of
+// the launch has its maps encoded; wide rows), and for stage 4 the update's
+// operands too when they fit (stage_centre).
 template <template <typename> class Th, class M, typename T, int STAGE, int MINB, bool LO = false, bool TMA = false>
 __global__ void __launch_bounds__(M::NTHREADS, MINB)
     k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
     constexpr int NSRC = STAGE == 1 ? (LO ? 2 : 1) : (STAGE == 2 ? 2 : 3);
+    constexpr bool CENTRE = stage_centre<M, T, STAGE, MINB, TMA>();
     extern __shared__ __align__(128) unsigned char smraw[];
     // TMA box copies land on 128-byte boundaries: the launch adds 128 bytes of slack
     // and the ring starts at the first 128-byte boundary of the dynamic segment
     T* sm = reinterpret_cast<T*>(smraw + (TMA ? ((128u - (smem_addr(smraw) & 127u)) & 127u) : 0u));
     __shared__ KSum shk[M::NTHREADS / 32];  // one entry per warp (kept small: two blocks
     __shared__ double shm[M::NTHREADS / 32];  // per SM need all but 1 KB of shared memory)
-    __shared__ uint64_t tma_bar[2];
+    __shared__ uint64_t tma_bar[3];
     TmaTile tt{tma_bar, 0u, {nullptr, nullptr, nullptr}, nullptr};
+    CentreStage<T> cst;
     if constexpr (TMA) {
         if (threadIdx.x == 0 && threadIdx.y == 0) {
             mbar_init(&tma_bar[0], 1);
             mbar_init(&tma_bar[1], 1);
+            if (CENTRE) mbar_init(&tma_bar[2], 1);
         }
         __syncthreads();
+    }
+    if constexpr (CENTRE) {
+        cst.buf = sm + M::template smem_bytes_tma<T>(3) / sizeof(T);
+        cst.bar = &tma_bar[2];
+        cst.box = M::C * M::BY * M::BZ;
+        cst.phase = 0u;
+        cst.pending = 0u;
     }
     for (int t = t_begin + blockIdx.x; t < t_end; t += gridDim.x) {
         const int ii = __ldg(tile_inst + t);
@@ -389,7 +507,7 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
         const T* const src[3] = {F, LO ? in.Flo[parity] : V, STAGE == 3 ? in.L[0] : in.L[1]};
         const T a = STAGE == 4 ? dtt : hdt;
         const T b = STAGE == 3 ? T(0.25) * dtt : T(0.5) * dtt;
-        EngineEpi<T, STAGE, M::C> epi{{F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2]},
+        EngineEpi<T, STAGE, M::C, CENTRE> epi{{F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2]},
                                 STAGE < 4 ? in.L[STAGE - 1] : in.F[parity ^ 1],
                                 STAGE < 4 ? nullptr : in.V[parity ^ 1],
                                 in.Flo[parity ^ 1],
@@ -402,7 +520,20 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
             tt.map[2] = NSRC > 2 ? &in.tm[kMapL + (STAGE == 3 ? 0 : 1)] : nullptr;
             tt.status = in.status;
         }
-        if (!march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE, M::C>, LO, T, true, TMA>(
+        if constexpr (CENTRE) {
+            cst.map[0] = &in.tmc[kMapF + parity];
+            cst.map[1] = in.Flo[parity] != nullptr ? &in.tmc[kMapFlo + parity] : nullptr;
+            cst.map[2] = V != nullptr ? &in.tmc[kMapV + parity] : nullptr;
+            cst.map[3] = &in.tmc[kMapL];
+            cst.map[4] = &in.tmc[kMapL + 1];
+            cst.map[5] = &in.tmc[kMapL + 2];
+            cst.map[6] = in.Dlt != nullptr ? &in.tmc[kMapDlt] : nullptr;
+            cst.status = in.status;
+            cst.z0 = z0;
+            cst.y0 = y0;
+            epi.cs = &cst;
+        }
+        if (!march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE, M::C, CENTRE>, LO, T, true, TMA>(
                 sm, p, src, a, b, xa, xe, y0, z0, epi, es, bs, TMA ? &tt : nullptr))
             return;  // a copy did not arrive: the block's error bit is set, its partials stay stale
         if (STAGE == 1) {

@@ -87,10 +87,19 @@ struct MarchShape {
 
 // Whether an epilogue wants a call at the start of each site (before the stencil
 // arithmetic), e.g. to issue the global loads its operator() will consume.
+// plane_begin(x): called by every thread once per computed plane x, right after the
+// plane barrier (TMA staging only).
+template <class E, class = void>
+struct HasPlaneBegin : std::false_type {};
+template <class E>
+struct HasPlaneBegin<E, std::void_t<decltype(std::declval<E&>().plane_begin(0))>> : std::true_type {};
+
+// begin_site(s, N, next): s is the site about to be computed and next the same
+// thread's site on the following plane of the tile (-1 on the tile's last plane).
 template <class E, class = void>
 struct HasBeginSite : std::false_type {};
 template <class E>
-struct HasBeginSite<E, std::void_t<decltype(std::declval<E&>().begin_site(int64_t(0), int64_t(0)))>>
+struct HasBeginSite<E, std::void_t<decltype(std::declval<E&>().begin_site(int64_t(0), int64_t(0), int64_t(0)))>>
     : std::true_type {};
 
 // Per-tile TMA state of a marching kernel: the kernel's two mbarriers
@@ -481,6 +490,9 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
                 return false;
             }
             if (q + LA <= q1) issue_tma(q + LA, (slot + LA) % R, nb);
+            if constexpr (HasPlaneBegin<Epi>::value) {
+                if (q - 2 >= xa) epi.plane_begin(q - 2);
+            }
         } else if constexpr (DIRECT) {
             cp_async_wait_all();
             // (A) plane q has landed for every thread, and every thread finished the
@@ -530,7 +542,7 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
             // (its FP64 sum needs no more than FP32 per-site accuracy; only the energy, which
             // decides the arrest, is evaluated in FP64)
             [[maybe_unused]] double b32 = 0.0;
-            if constexpr (HasBeginSite<Epi>::value) epi.begin_site(s, N);
+            if constexpr (HasBeginSite<Epi>::value) epi.begin_site(s, N, x + 1 < xe ? s + YZ : int64_t(-1));
             if constexpr (GRAD) {
             T phi[C], D[3][C], Sd[6][C], g[C];
 #pragma unroll
