@@ -543,59 +543,28 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
             // decides the arrest, is evaluated in FP64)
             [[maybe_unused]] double b32 = 0.0;
             if constexpr (HasBeginSite<Epi>::value) epi.begin_site(s, N, x + 1 < xe ? s + YZ : int64_t(-1));
-            // FUSED64 (stage 1 of a compensated FP32 field): the FP64 first derivatives of
-            // hi + lo that the energy density needs are formed in the gradient's tap loop,
-            // from the same high-part taps and FP32 differences (each FP32 difference is the
-            // sum of Knuth's TwoSum, whose error term absorbs the low parts' difference)
-            constexpr bool FUSED64 = GRAD && DENS != 0 && LO && sizeof(T) == 4;
-            [[maybe_unused]] double phd64[FUSED64 ? C : 1], Dd64[3][FUSED64 ? C : 1];
             if constexpr (GRAD) {
             T phi[C], D[3][C], Sd[6][C], g[C];
-            [[maybe_unused]] StencilCoef<double> kd64;
-            if constexpr (FUSED64) kd64.init(p);
-            [[maybe_unused]] const ptrdiff_t dl = ring_lo - ring;
-            // exact difference of two hi + lo taps in FP64, given the FP32 difference sd = hu - hv
-            [[maybe_unused]] auto dif64 = [&](const T* u, const T* v, T sd) -> double {
-                const T hu = u[0], hv = -v[0];
-                const T bb = sd - hu;
-                const T e = (hu - (sd - bb)) + (hv - bb);
-                return double(sd) + double(e + (u[dl] - v[dl]));
-            };
 #pragma unroll
             for (int c = 0; c < C; ++c) {
                 const int co = c * M::PLANE;
                 const T* f = P0 + co;
                 const T f0 = f[0];
                 phi[c] = f0;
-                if constexpr (FUSED64) phd64[c] = double(f0) + double(f[dl]);
                 {
                     const T fm2 = Pm2[co], fm1 = Pm1[co], fp1 = Pp1[co], fp2 = Pp2[co];
-                    const T s1 = fp1 - fm1, s2 = fp2 - fm2;
-                    D[0][c] = mk.px ? k.d1a[0] * s1 - k.d1b[0] * s2 : T(0);
+                    D[0][c] = mk.px ? k.d1a[0] * (fp1 - fm1) - k.d1b[0] * (fp2 - fm2) : T(0);
                     Sd[0][c] = mk.px ? k.d2a[0] * (fp1 + fm1) - k.d2b[0] * (fp2 + fm2) - k.d2c[0] * f0 : T(0);
-                    if constexpr (FUSED64)
-                        Dd64[0][c] = mk.px ? kd64.d1a[0] * dif64(Pp1 + co, Pm1 + co, s1) -
-                                                 kd64.d1b[0] * dif64(Pp2 + co, Pm2 + co, s2)
-                                           : 0.0;
                 }
                 {
                     const T fm2 = f[-2 * M::HZ], fm1 = f[-M::HZ], fp1 = f[M::HZ], fp2 = f[2 * M::HZ];
-                    const T s1 = fp1 - fm1, s2 = fp2 - fm2;
-                    D[1][c] = mk.py ? k.d1a[1] * s1 - k.d1b[1] * s2 : T(0);
+                    D[1][c] = mk.py ? k.d1a[1] * (fp1 - fm1) - k.d1b[1] * (fp2 - fm2) : T(0);
                     Sd[1][c] = mk.py ? k.d2a[1] * (fp1 + fm1) - k.d2b[1] * (fp2 + fm2) - k.d2c[1] * f0 : T(0);
-                    if constexpr (FUSED64)
-                        Dd64[1][c] = mk.py ? kd64.d1a[1] * dif64(f + M::HZ, f - M::HZ, s1) -
-                                                 kd64.d1b[1] * dif64(f + 2 * M::HZ, f - 2 * M::HZ, s2)
-                                           : 0.0;
                 }
                 {
                     const T fm2 = f[-2], fm1 = f[-1], fp1 = f[1], fp2 = f[2];
-                    const T s1 = fp1 - fm1, s2 = fp2 - fm2;
-                    D[2][c] = mk.pz ? k.d1a[2] * s1 - k.d1b[2] * s2 : T(0);
+                    D[2][c] = mk.pz ? k.d1a[2] * (fp1 - fm1) - k.d1b[2] * (fp2 - fm2) : T(0);
                     Sd[2][c] = mk.pz ? k.d2a[2] * (fp1 + fm1) - k.d2b[2] * (fp2 + fm2) - k.d2c[2] * f0 : T(0);
-                    if constexpr (FUSED64)
-                        Dd64[2][c] = mk.pz ? kd64.d1a[2] * dif64(f + 1, f - 1, s1) - kd64.d1b[2] * dif64(f + 2, f - 2, s2)
-                                           : 0.0;
                 }
                 T sxy, sxz;
                 if constexpr (QUEUE) {
@@ -615,17 +584,7 @@ __device__ __forceinline__ bool march_tile(T* __restrict__ sm, const Params& p, 
             if constexpr (DENS != 0 && sizeof(T) == 4) b32 = double(Th<T>::baryon(phi, D, p));
             epi(s, N, phi, g);
             }
-            if constexpr (FUSED64) {
-                double phd[CT], Dd[3][CT];
-#pragma unroll
-                for (int c = 0; c < CT; ++c) {
-                    phd[c] = c < C ? phd64[c < C ? c : 0] : 0.0;
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) Dd[i][c] = c < C ? Dd64[i][c < C ? c : 0] : 0.0;
-                }
-                ksum_add(esum, Th<double>::energy(phd, Dd, p));
-                ksum_add(bsum, b32);
-            } else if (DENS) {
+            if (DENS) {
                 // FP64 energy and baryon densities of the stage input (stage 1: the field itself),
                 // evaluated after the gradient so their registers do not overlap
                 StencilCoef<double> kd;
