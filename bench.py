@@ -835,6 +835,18 @@ def run_serve(args):
            if served[k].status == "converged" and serial[k]["status"] == "converged"]
     n_serial = sum(v["status"] == "converged" for v in serial.values())
     serial_sps = n_serial / t_all if t_all > 0 else None
+    # per theory: counts by outcome and time-to-converged percentiles, served and serial
+    by_theory = {}
+    for th_name in sorted({r.theory for r, _, _ in reqs}):
+        ks = [r.rid for r, _, _ in reqs if r.theory == th_name]
+        lat = np.array([served[k].latency for k in ks if served[k].status == "converged"])
+        by_theory[th_name] = {
+            "requests": len(ks),
+            "served": {st: sum(served[k].status == st for k in ks) for st in ("converged", "failed", "not_converged")},
+            "serial": {st: sum(serial[k]["status"] == st for k in ks) for st in ("converged", "failed",
+                                                                                  "not_converged")},
+            "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
+            "p99_s": float(np.percentile(lat, 99)) if lat.size else None}
     line = {"mode": "serve", "metric": METRIC, "unit": UNIT,
             "config": {"workload": "poisson_stream", "requests": args.requests, "rate_per_s": args.rate,
                        "mix": mix, "B": f"1..{args.bmax}", "max_side": args.max_side,
@@ -844,6 +856,7 @@ def run_serve(args):
                                     "fp32d": "fp32d until max|g| <= tol or a stall, then fp64"}.get(
                            args.schedule, f"{args.schedule} until twice the FP32 gradient floor, then fp64")},
             "served": summ,
+            "by_theory": by_theory,
             "serial_plain_fp64": {"converged": n_serial, "seconds": t_all, "solves_per_s": serial_sps},
             "speedup_solves_per_s": (summ["solves_per_s"] / serial_sps) if (summ["solves_per_s"] and serial_sps)
             else None,
@@ -1076,11 +1089,12 @@ def main():
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--mix", default="nuclear:1")
-    ap.add_argument("--bmax", type=int, default=1)
+    ap.add_argument("--mix", default="nuclear:0.4,omega:0.3,rho:0.2,coulomb:0.1",
+                    help="serving: theory weights (the serving stream's mix by default)")
+    ap.add_argument("--bmax", type=int, default=12, help="serving: baryon numbers drawn from 1..bmax")
     ap.add_argument("--schedule", choices=("fp32d", "fp32c", "fp32", "fp64"), default="fp64",
                     help="serving precision schedule: FP32 phase then FP64, or FP64 throughout")
-    ap.add_argument("--max-side", type=int, default=64)
+    ap.add_argument("--max-side", type=int, default=192)
     ap.add_argument("--defect-period", type=int, default=None,
                     help="serving: steps between refreshes of the fp32d correction (default 16)")
     ap.add_argument("--render", action="store_true", help="headless viewer: volume builder and ray-march")
@@ -1106,7 +1120,7 @@ def main():
         return run_calibrate(args)
     if args.serve:
         if args.max_steps == 240000:
-            args.max_steps = 60000
+            args.max_steps = 20000
         return run_serve(args)
     if args.numba_reference:
         return run_numba_reference(args)
