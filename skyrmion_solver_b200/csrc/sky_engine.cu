@@ -40,6 +40,7 @@ struct HostInst {
     int xc = 0;          // x-chunk of the marching kernels
     int xc_request = 0;  // x-chunk asked for by the caller (0: automatic)
     bool tma = false;    // the stage kernels stage this instance with TMA box copies
+    bool pair = false;   // ... with z-pair tiles (FP32 theories without mixed derivatives, option 3)
     int group_slot = -1;
     int64_t steps = 0;  // host mirror of the device step counter
     bool active = true;
@@ -57,6 +58,7 @@ struct Group {
     bool all_wide = true;   // every member can use the wide-row (16-byte staged) kernels
     bool any_defect = false;  // holds a defect-corrected instance (launch the defect refresh)
     bool all_tma = false;     // every member has TMA plane maps (launch the TMA stage kernels)
+    bool all_pair = false;    // ... and runs as z-pair tiles (option 3 at admission)
 };
 
 struct Engine {
@@ -117,18 +119,19 @@ static size_t stage_smem() {
     return stage_smem_bytes<M, T, STAGE, march_minb<Th, T>(), LO, TMA>();
 }
 
-template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false>
+template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false,
+          bool PAIR = false>
 static int stage_setup_w(int* per_sm_out) {
     static int per_sm = 0;
     if (per_sm == 0) {
         int rc, n = 0;
         using M = MShape<Th, T, WIDE>;
-        auto kern = k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO, TMA>;
+        auto kern = k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO, TMA, PAIR>;
         const size_t smem = stage_smem<Th, T, STAGE, WIDE, LO, TMA>();
         rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                         "cudaFuncSetAttribute(march stage)", __LINE__);
         if (rc) return rc;
-        rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, M::NTHREADS, smem),
+        rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, stage_threads<M, PAIR>(), smem),
                         "occupancy query", __LINE__);
         if (rc) return rc;
         per_sm = n < 1 ? 1 : n;
@@ -142,10 +145,11 @@ static int stage_setup(int* per_sm_out) {
     return stage_setup_w<Th, T, STAGE, true>(per_sm_out);
 }
 
-template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false>
+template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false,
+          bool PAIR = false>
 static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t st) {
     int per_sm = 1;
-    int rc = stage_setup_w<Th, T, STAGE, WIDE, LO, TMA>(&per_sm);
+    int rc = stage_setup_w<Th, T, STAGE, WIDE, LO, TMA, PAIR>(&per_sm);
     if (rc) return rc;
     int n = t_end - t_begin;
     if (n <= 0) return SKY_OK;
@@ -153,9 +157,17 @@ static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t s
     InstDesc<T>* d = reinterpret_cast<InstDesc<T>*>(g.d_desc);
     using M = MShape<Th, T, WIDE>;
     const size_t smem = stage_smem<Th, T, STAGE, WIDE, LO, TMA>();
-    k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO, TMA><<<blocks, dim3(M::BZ, M::BY), smem, st>>>(
+    const dim3 block(PAIR ? PairShape<M>::TZ : M::BZ, M::BY);
+    k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO, TMA, PAIR><<<blocks, block, smem, st>>>(
         d, g.d_tile_inst, t_begin, t_end);
     return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
+}
+
+// Whether the FP32 stages of Th run as z-pair tiles (option 3, TMA groups, theories
+// without mixed second derivatives).
+template <template <typename> class Th, typename T>
+constexpr bool pair_allowed() {
+    return sizeof(T) == 4 && !Th<float>::kMixed && Th<float>::C <= 5;
 }
 
 // Whether the stage kernels of (Th, T) can stage with TMA: wide rows must be allowed.
@@ -168,6 +180,14 @@ template <template <typename> class Th, typename T, int STAGE>
 static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
     if constexpr (tma_allowed<Th, T>()) {
         if (g.all_tma) {
+            if constexpr (pair_allowed<Th, T>()) {
+                if (g.all_pair) {
+                    if constexpr (STAGE == 1) {
+                        if (g.any_comp) return launch_stage_w<Th, T, 1, true, true, true, true>(g, t_begin, t_end, st);
+                    }
+                    return launch_stage_w<Th, T, STAGE, true, false, true, true>(g, t_begin, t_end, st);
+                }
+            }
             if constexpr (STAGE == 1 && sizeof(T) == 4 && Th<float>::C <= 5) {
                 if (g.any_comp) return launch_stage_w<Th, T, 1, true, true, true>(g, t_begin, t_end, st);
             }
@@ -227,6 +247,14 @@ static int setup_all() {
         if constexpr (sizeof(T) == 4 && Th<float>::C <= 5) {
             if ((rc = stage_setup_w<Th, T, 1, true, true, true>(&n))) return rc;
         }
+    }
+    if constexpr (tma_allowed<Th, T>() && pair_allowed<Th, T>()) {
+        if ((rc = stage_setup_w<Th, T, 1, true, false, true, true>(&n)) ||
+            (rc = stage_setup_w<Th, T, 2, true, false, true, true>(&n)) ||
+            (rc = stage_setup_w<Th, T, 3, true, false, true, true>(&n)) ||
+            (rc = stage_setup_w<Th, T, 4, true, false, true, true>(&n)) ||
+            (rc = stage_setup_w<Th, T, 1, true, true, true, true>(&n)))
+            return rc;
     }
     return SKY_OK;
 }
@@ -455,6 +483,7 @@ static int rebuild_group_t(Engine& e, Group& g) {
     g.all_wide = true;
     g.any_defect = false;
     g.all_tma = !g.members.empty();
+    g.all_pair = !g.members.empty();
     for (size_t k = 0; k < g.members.size(); ++k) {
         HostInst& h = e.insts[g.members[k]];
         InstDesc<S> d = make_desc<S>(h, tb);
@@ -468,6 +497,7 @@ static int rebuild_group_t(Engine& e, Group& g) {
         } else {
             g.all_tma = false;
         }
+        if (!h.pair) g.all_pair = false;
         if (h.group_slot >= 0 && h.group_slot < (int)dev_old.size()) {
             const InstDesc<S>& o = dev_old[h.group_slot];
             d.e_prev = o.e_prev;
@@ -540,6 +570,7 @@ static bool tma_ok_for(const HostInst& h) {
 static int alloc_inst(Engine& e, HostInst& h) {
     const size_t es = h.prec ? sizeof(double) : sizeof(float);
     h.tma = tma_ok_for(h);
+    h.pair = h.tma && option(3) == 1 && h.prec == 0 && h.theory == SKY_THEORY_OMEGA;
     const size_t fb = es * (size_t)h.C * (size_t)h.N;
     int bz, by, tx, per_sm;
     int rc0 = tile_shape(h.theory, h.prec, bz, by, tx, per_sm);
@@ -1047,6 +1078,7 @@ int sky_engine_retile(void* handle, int id, int xc) {
     h.tnx = (h.p.X + nxc - 1) / nxc;
     h.ntiles = ntiles;
     h.tma = tma_ok_for(h);
+    h.pair = h.tma && option(3) == 1 && h.prec == 0 && h.theory == SKY_THEORY_OMEGA;
     Group& g = e->groups[h.theory][h.prec];
     if ((rc = rebuild_group(*e, g))) return rc;
     return init_instance(*e, h, 2);

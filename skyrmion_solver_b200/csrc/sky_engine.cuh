@@ -23,6 +23,7 @@
 
 #include "sky_kernels.cuh"
 #include "sky_march.cuh"
+#include "sky_march_pair.cuh"
 
 namespace sky {
 
@@ -296,7 +297,8 @@ constexpr int kCentreArrays = 7;
 
 // CC: components of the theory; the defect correction exists only for CC <= 5.
 // CENTRE: stage 4 reads the update's operands from shared memory (CentreStage).
-template <typename T, int STAGE, int CC, bool CENTRE = false>
+// NL: sites per thread (2 for the z-pair tiles: lane l is the thread's site l).
+template <typename T, int STAGE, int CC, bool CENTRE = false, int NL = 1>
 struct EngineEpi {
     static constexpr bool kDefect = CC <= 5;  // instances of this theory can carry a correction
     // inputs of the stage-4 update, read from global memory at the site (prefetching them
@@ -318,9 +320,10 @@ struct EngineEpi {
     T* dlt;       // defect correction (null unless defect-corrected)
     int refresh;  // stage 1 of a refresh step: dlt holds g64 of the field; replace it by g64 - g32
     CentreStage<T>* cs = nullptr;  // CENTRE: the plane's staged operands
-    T d[kDefect ? CC : 1];   // the site's correction
-    T dn[kDefect ? CC : 1];  // the correction of the thread's site on the next plane, in flight
-    int64_t dn_site = -1;    // the site dn belongs to
+    int zbase = 0;                 // z of the thread's first site within the tile
+    T d[NL][kDefect ? CC : 1];     // the site's correction
+    T dn[NL][kDefect ? CC : 1];    // the correction of the thread's site on the next plane, in flight
+    int64_t dn_tag[NL];            // 1 + the site dn belongs to (0: none; value-initialised)
     // CENTRE: thread 0 copies the update's operands of plane x (every thread calls this
     // right after the plane barrier, before the stencil arithmetic).
     __device__ __forceinline__ void plane_begin(int x) {
@@ -341,27 +344,27 @@ struct EngineEpi {
     // A thread walks its (y, z) column along x.  The correction of the next plane's
     // site is loaded while this site is computed, so that its global-memory latency
     // overlaps a whole plane of stencil and point arithmetic.
-    __device__ __forceinline__ void begin_site(int64_t s, int64_t N, int64_t next) {
+    __device__ __forceinline__ void begin_site(int64_t s, int64_t N, int64_t next, int l = 0) {
         if constexpr (CENTRE) return;  // the correction comes with the staged operands
         if constexpr (kDefect) {
             if (dlt) {
-                if (dn_site == s) {
+                if (dn_tag[l] == s + 1) {
 #pragma unroll
-                    for (int c = 0; c < CC; ++c) d[c] = dn[c];
+                    for (int c = 0; c < CC; ++c) d[l][c] = dn[l][c];
                 } else {
 #pragma unroll
-                    for (int c = 0; c < CC; ++c) d[c] = __ldcg(dlt + c * N + s);
+                    for (int c = 0; c < CC; ++c) d[l][c] = __ldcg(dlt + c * N + s);
                 }
                 if (next >= 0) {
 #pragma unroll
-                    for (int c = 0; c < CC; ++c) dn[c] = __ldcg(dlt + c * N + next);
+                    for (int c = 0; c < CC; ++c) dn[l][c] = __ldcg(dlt + c * N + next);
                 }
-                dn_site = next;
+                dn_tag[l] = next + 1;
             }
         }
     }
     template <int C>
-    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g32)[C]) {
+    __device__ __forceinline__ void operator()(int64_t s, int64_t N, const T (&)[C], const T (&g32)[C], int l = 0) {
         static_assert(C == CC, "component count");
         T g[C];
 #pragma unroll
@@ -369,8 +372,8 @@ struct EngineEpi {
         if constexpr (CENTRE) {
             static_assert(STAGE == 4, "staged operands are the stage-4 update's");
             if (!mbar_wait_bounded(cs->bar, cs->pending)) atomicOr(cs->status, 2);
-            // the thread's site within the staged boxes: [c][ty][tx]
-            const int o = threadIdx.y * 32 + threadIdx.x;
+            // the site within the staged boxes: [c][y - y0][z - z0]
+            const int o = threadIdx.y * 32 + zbase + l;
             const int bx = cs->box / C;
             T f0[C], flo[C], v0[C], a1[C], a2[C], a3[C];
 #pragma unroll
@@ -403,12 +406,12 @@ struct EngineEpi {
                 if (STAGE == 1 && refresh) {   // d = g64(F): the correction becomes g64 - g32(F)
 #pragma unroll
                     for (int c = 0; c < C; ++c) {
-                        __stcg(dlt + c * N + s, d[c] - g32[c]);
-                        g[c] = d[c];
+                        __stcg(dlt + c * N + s, d[l][c] - g32[c]);
+                        g[c] = d[l][c];
                     }
                 } else {
 #pragma unroll
-                    for (int c = 0; c < C; ++c) g[c] = g32[c] + d[c];
+                    for (int c = 0; c < C; ++c) g[c] = g32[c] + d[l][c];
                 }
             }
         }
@@ -461,10 +464,18 @@ constexpr size_t stage_smem_bytes() {
 
 // TMA: planes staged by tensor-memory-accelerator box copies (every instance of
 // the launch has its maps encoded; wide rows), and for stage 4 the update's
-// operands too when they fit (stage_centre).
-template <template <typename> class Th, class M, typename T, int STAGE, int MINB, bool LO = false, bool TMA = false>
-__global__ void __launch_bounds__(M::NTHREADS, MINB)
+// operands too when they fit (stage_centre).  PAIR: z-pair tiles (FP32, TMA,
+// theories without mixed derivatives; sky_march_pair.cuh), 16 x BY threads.
+template <class M, bool PAIR>
+constexpr int stage_threads() {
+    return PAIR ? PairShape<M>::NT : M::NTHREADS;
+}
+
+template <template <typename> class Th, class M, typename T, int STAGE, int MINB, bool LO = false, bool TMA = false,
+          bool PAIR = false>
+__global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
     k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
+    static_assert(!PAIR || (TMA && sizeof(T) == 4), "z-pair tiles: FP32 with TMA staging");
     constexpr int NSRC = STAGE == 1 ? (LO ? 2 : 1) : (STAGE == 2 ? 2 : 3);
     constexpr bool CENTRE = stage_centre<M, T, STAGE, MINB, TMA>();
     extern __shared__ __align__(128) unsigned char smraw[];
@@ -507,7 +518,8 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
         const T* const src[3] = {F, LO ? in.Flo[parity] : V, STAGE == 3 ? in.L[0] : in.L[1]};
         const T a = STAGE == 4 ? dtt : hdt;
         const T b = STAGE == 3 ? T(0.25) * dtt : T(0.5) * dtt;
-        EngineEpi<T, STAGE, M::C, CENTRE> epi{{F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2]},
+        using Epi = EngineEpi<T, STAGE, M::C, CENTRE, PAIR ? 2 : 1>;
+        Epi epi{{F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2]},
                                 STAGE < 4 ? in.L[STAGE - 1] : in.F[parity ^ 1],
                                 STAGE < 4 ? nullptr : in.V[parity ^ 1],
                                 in.Flo[parity ^ 1],
@@ -533,9 +545,14 @@ __global__ void __launch_bounds__(M::NTHREADS, MINB)
             cst.y0 = y0;
             epi.cs = &cst;
         }
-        if (!march_tile<Th, M, T, NSRC, STAGE == 1, EngineEpi<T, STAGE, M::C, CENTRE>, LO, T, true, TMA>(
-                sm, p, src, a, b, xa, xe, y0, z0, epi, es, bs, TMA ? &tt : nullptr))
-            return;  // a copy did not arrive: the block's error bit is set, its partials stay stale
+        epi.zbase = PAIR ? 2 * int(threadIdx.x) : int(threadIdx.x);
+        bool ok;
+        if constexpr (PAIR)
+            ok = march_tile_pair<Th, M, NSRC, STAGE == 1, Epi, LO>(sm, p, a, b, xa, xe, y0, z0, epi, es, bs, &tt);
+        else
+            ok = march_tile<Th, M, T, NSRC, STAGE == 1, Epi, LO, T, true, TMA>(sm, p, src, a, b, xa, xe, y0, z0, epi,
+                                                                             es, bs, TMA ? &tt : nullptr);
+        if (!ok) return;  // a copy did not arrive: the block's error bit is set, its partials stay stale
         if (STAGE == 1) {
             const KSum be = block_ksum(es, shk);
             const KSum bb = block_ksum(bs, shk);

@@ -320,8 +320,9 @@ int choose_xc(int X, int tiles_yz, int resident) {
 // Library options (sky_set_option): key 0 = kernel family of the
 // reference-layout gradient and densities (1 = marching kernels, 0 = 3-D tile
 // kernels); key 1 = x-chunk of those marching launches (0 = automatic); key 2 =
-// staging of the engine's stage kernels (1 = TMA box copies, 0 = cp.async).
-static int g_options[4] = {1, 0, 1, 0};
+// staging of the engine's stage kernels (1 = TMA box copies, 0 = cp.async); key 3 =
+// z-pair tiles for the FP32 stages of theories without mixed derivatives (1 = on).
+static int g_options[4] = {1, 0, 1, 1};
 int option(int key) { return (key >= 0 && key < 4) ? g_options[key] : 0; }
 
 // ---------------------------------------------------------------------------
@@ -648,7 +649,8 @@ int sky_set_option(int key, int value) {
     if (key == 0 && value != 0 && value != 1) return invalid("option 0 takes 0 (tile kernels) or 1 (marching kernels)");
     if (key == 1 && value < 0) return invalid("option 1 (x-chunk) must be >= 0");
     if (key == 2 && value != 0 && value != 1) return invalid("option 2 takes 0 (cp.async staging) or 1 (TMA staging)");
-    if (key < 0 || key > 2) return invalid("unknown option key");
+    if (key == 3 && value != 0 && value != 1) return invalid("option 3 takes 0 (one site per thread) or 1 (z-pairs)");
+    if (key < 0 || key > 3) return invalid("unknown option key");
     g_options[key] = value;
     return SKY_OK;
 }

@@ -117,6 +117,8 @@ __device__ __forceinline__ void cs_coupling(T* out, const T* phi, const T (&D)[3
 // ===========================================================================
 template <typename T>
 struct Nuclear {
+    // whether gradient() reads the mixed second derivatives S[3..5]
+    static constexpr bool kMixed = true;
     static constexpr int C = 4;
     static constexpr int kId = SKY_THEORY_NUCLEAR;
     // th/nuclear_skyrme/kernels.py:1035-1150
@@ -153,6 +155,8 @@ struct Nuclear {
 // ===========================================================================
 template <typename T>
 struct Omega {
+    // whether gradient() reads the mixed second derivatives S[3..5]
+    static constexpr bool kMixed = false;
     static constexpr int C = 5;
     static constexpr int kId = SKY_THEORY_OMEGA;
     // th/omega_skyrme/kernels.py:587-743
@@ -192,6 +196,8 @@ struct Omega {
 // ===========================================================================
 template <typename T>
 struct Coulomb {
+    // whether gradient() reads the mixed second derivatives S[3..5]
+    static constexpr bool kMixed = true;
     static constexpr int C = 5;
     static constexpr int kId = SKY_THEORY_COULOMB;
     // th/coulomb_skyrme/kernels.py:585-767.  The 2*g store at :684-685 is
@@ -244,6 +250,8 @@ __host__ __device__ constexpr int eps3(int i, int j, int k) {
 
 template <typename T>
 struct Rho {
+    // whether gradient() reads the mixed second derivatives S[3..5]
+    static constexpr bool kMixed = true;
     static constexpr int C = 13;
     static constexpr int kId = SKY_THEORY_RHO;
 
@@ -390,6 +398,8 @@ __device__ __forceinline__ T oc(const T* a, const T* b) { return a[0] * b[3] + a
 
 template <typename T>
 struct Berger {
+    // whether gradient() reads the mixed second derivatives S[3..5]
+    static constexpr bool kMixed = true;
     static constexpr int C = 4;
     static constexpr int kId = SKY_THEORY_BERGER;
     // th/berger_skyrme/kernels.py:554-736
@@ -457,6 +467,8 @@ struct Berger {
 // ===========================================================================
 template <typename T>
 struct LightlyBound {
+    // whether gradient() reads the mixed second derivatives S[3..5]
+    static constexpr bool kMixed = true;
     static constexpr int C = 4;
     static constexpr int kId = SKY_THEORY_LIGHTLY_BOUND;
     // th/lightly_bound_skyrme/kernels.py:567-684
