@@ -26,7 +26,9 @@ def _run(name, dims, precision, staging, nsteps, seed=5):
     th, p_i, p_f = params_for(name, dims)
     F, V = inputs(int(p_i[5]), dims, seed=seed)
     old = int(_lib.load().sky_get_option(2))
+    old_pair = int(_lib.load().sky_get_option(3))
     _lib.call("sky_set_option", 2, 1 if staging == "tma" else 0)
+    _lib.call("sky_set_option", 3, 0)   # one site per thread in both stagings (z-pairs: below)
     try:
         with Engine(0) as eng:
             i = eng.add(name, (p_i, p_f), F, V, precision=precision)
@@ -38,6 +40,7 @@ def _run(name, dims, precision, staging, nsteps, seed=5):
             f, v = eng.read(i)
     finally:
         _lib.call("sky_set_option", 2, old)
+        _lib.call("sky_set_option", 3, old_pair)
     return recs, f, v, (F, V, p_i, p_f)
 
 
