@@ -57,6 +57,9 @@ const char* sky_last_error(void);
  * staging of the resident engine's stage kernels, 1 = tensor-memory-accelerator
  * box copies (default; lattices whose Z gives 16-byte row pitches), 0 = per-thread
  * cp.async copies; it applies to instances admitted (or re-tiled) afterwards.
+ * Key 3: 1 = the FP32 stages of theories whose gradient needs no mixed second
+ * derivatives (omega) compute two adjacent z-sites per thread with packed FP32x2
+ * arithmetic; 0 = one site per thread (default).  Applies at admission.
  * Process-wide; not synchronised with launches in flight on other threads. */
 int sky_set_option(int key, int value);
 int sky_get_option(int key);
