@@ -48,7 +48,7 @@ UNIT = "solves/s"
 WORKLOAD = "omega_B4_rational_map_128^3_h0.15"
 CALIBRATION = os.path.join(ROOT, "profiles", "convergence_omega_B4_128.json")
 TRAFFIC = [os.path.join(ROOT, "profiles", f) for f in ("ncu_stage1_fp32d_omega128.md",
-                                                        "ncu_engine_stages_omega128_fp32.md")]
+                                                        "ncu_stage4_fp32d_omega128.md")]
 L = 128
 H = 0.15
 FAST = "fp32d"   # precision of the timed steps (the FP32 phase of the schedule)
