@@ -353,11 +353,14 @@ int sky_engine_read(void* engine, int id, double* field, double* velocity, int o
 
 /* Run nsteps steps without graph capture, timing each launch kind with CUDA
  * events on the engine stream; ms_out[6] = average milliseconds per step spent
- * in [stage 1 (with the defect refresh, if any), stage 2, stage 3, stage 4 +
- * update, control, advance]. */
+ * in [stage 1 (with the defect refresh and the folded control), stage 2, stage 3,
+ * stage 4 + update (with the folded advance), 0, 0]: the last two entries (the
+ * separate control and advance launches) are kept for compatibility. */
 int sky_engine_time_stages(void* engine, int nsteps, double* ms_out);
 
-/* Kernel launches one step issues (6 per non-empty (theory, precision) group). */
+/* Kernel launches one step issues: 4 per non-empty (theory, precision) group
+ * (stages 2, 3, 4 and 1; stage 4's last block per instance advances it and stage
+ * 1's runs its control), 5 when the group holds a defect-corrected instance. */
 int sky_engine_launches_per_step(void* engine);
 
 int sky_engine_count(void* engine);

@@ -147,7 +147,7 @@ static int stage_setup(int* per_sm_out) {
 
 template <template <typename> class Th, typename T, int STAGE, bool WIDE, bool LO = false, bool TMA = false,
           bool PAIR = false>
-static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t st) {
+static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t st, int tail) {
     int per_sm = 1;
     int rc = stage_setup_w<Th, T, STAGE, WIDE, LO, TMA, PAIR>(&per_sm);
     if (rc) return rc;
@@ -159,7 +159,7 @@ static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t s
     const size_t smem = stage_smem<Th, T, STAGE, WIDE, LO, TMA>();
     const dim3 block(PAIR ? PairShape<M>::TZ : M::BZ, M::BY);
     k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO, TMA, PAIR><<<blocks, block, smem, st>>>(
-        d, g.d_tile_inst, t_begin, t_end);
+        d, g.d_tile_inst, t_begin, t_end, tail);
     return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
 }
 
@@ -177,21 +177,21 @@ constexpr bool tma_allowed() {
 }
 
 template <template <typename> class Th, typename T, int STAGE>
-static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st) {
+static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st, int tail) {
     if constexpr (tma_allowed<Th, T>()) {
         if (g.all_tma) {
             if constexpr (pair_allowed<Th, T>()) {
                 if (g.all_pair) {
                     if constexpr (STAGE == 1) {
-                        if (g.any_comp) return launch_stage_w<Th, T, 1, true, true, true, true>(g, t_begin, t_end, st);
+                        if (g.any_comp) return launch_stage_w<Th, T, 1, true, true, true, true>(g, t_begin, t_end, st, tail);
                     }
-                    return launch_stage_w<Th, T, STAGE, true, false, true, true>(g, t_begin, t_end, st);
+                    return launch_stage_w<Th, T, STAGE, true, false, true, true>(g, t_begin, t_end, st, tail);
                 }
             }
             if constexpr (STAGE == 1 && sizeof(T) == 4 && Th<float>::C <= 5) {
-                if (g.any_comp) return launch_stage_w<Th, T, 1, true, true, true>(g, t_begin, t_end, st);
+                if (g.any_comp) return launch_stage_w<Th, T, 1, true, true, true>(g, t_begin, t_end, st, tail);
             }
-            return launch_stage_w<Th, T, STAGE, true, false, true>(g, t_begin, t_end, st);
+            return launch_stage_w<Th, T, STAGE, true, false, true>(g, t_begin, t_end, st, tail);
         }
     }
     // stage 1 of a group with compensated-field instances stages the low parts too,
@@ -204,28 +204,29 @@ static int launch_stage(const Group& g, int t_begin, int t_end, cudaStream_t st)
                 int n = 0;
                 const int rc = stage_setup_w<Th, T, 1, true, true>(&n);
                 if (rc) return rc;
-                if (n >= 2) return launch_stage_w<Th, T, 1, true, true>(g, t_begin, t_end, st);
+                if (n >= 2) return launch_stage_w<Th, T, 1, true, true>(g, t_begin, t_end, st, tail);
             }
-            return launch_stage_w<Th, T, 1, false, true>(g, t_begin, t_end, st);
+            return launch_stage_w<Th, T, 1, false, true>(g, t_begin, t_end, st, tail);
         }
     }
-    if (g.all_wide) return launch_stage_w<Th, T, STAGE, true>(g, t_begin, t_end, st);
-    return launch_stage_w<Th, T, STAGE, false>(g, t_begin, t_end, st);
+    if (g.all_wide) return launch_stage_w<Th, T, STAGE, true>(g, t_begin, t_end, st, tail);
+    return launch_stage_w<Th, T, STAGE, false>(g, t_begin, t_end, st, tail);
 }
 
 template <template <typename> class Th, typename T>
-static int launch_stage_any(int stage, const Group& g, int tb, int te, cudaStream_t st) {
+static int launch_stage_any(int stage, const Group& g, int tb, int te, cudaStream_t st, int tail) {
     switch (stage) {
-        case 1: return launch_stage<Th, T, 1>(g, tb, te, st);
-        case 2: return launch_stage<Th, T, 2>(g, tb, te, st);
-        case 3: return launch_stage<Th, T, 3>(g, tb, te, st);
-        default: return launch_stage<Th, T, 4>(g, tb, te, st);
+        case 1: return launch_stage<Th, T, 1>(g, tb, te, st, tail);
+        case 2: return launch_stage<Th, T, 2>(g, tb, te, st, tail);
+        case 3: return launch_stage<Th, T, 3>(g, tb, te, st, tail);
+        default: return launch_stage<Th, T, 4>(g, tb, te, st, tail);
     }
 }
 
 template <template <typename> class Th>
-static int stage_dispatch_prec(int prec, int stage, const Group& g, int tb, int te, cudaStream_t st) {
-    return prec ? launch_stage_any<Th, double>(stage, g, tb, te, st) : launch_stage_any<Th, float>(stage, g, tb, te, st);
+static int stage_dispatch_prec(int prec, int stage, const Group& g, int tb, int te, cudaStream_t st, int tail) {
+    return prec ? launch_stage_any<Th, double>(stage, g, tb, te, st, tail)
+                : launch_stage_any<Th, float>(stage, g, tb, te, st, tail);
 }
 
 template <template <typename> class Th, typename T>
@@ -276,14 +277,16 @@ static int setup_group(const Group& g) {
     return invalid("unknown theory id");
 }
 
-static int launch_stage_group(int stage, const Group& g, int tb, int te, cudaStream_t st) {
+// tail = 1: stage 4 also advances each instance and stage 1 also runs its control
+// (the step's launch sequence); 0: the stage alone (admission, precision change).
+static int launch_stage_group(int stage, const Group& g, int tb, int te, cudaStream_t st, int tail = 0) {
     switch (g.theory) {
-        case SKY_THEORY_NUCLEAR: return stage_dispatch_prec<Nuclear>(g.prec, stage, g, tb, te, st);
-        case SKY_THEORY_OMEGA: return stage_dispatch_prec<Omega>(g.prec, stage, g, tb, te, st);
-        case SKY_THEORY_COULOMB: return stage_dispatch_prec<Coulomb>(g.prec, stage, g, tb, te, st);
-        case SKY_THEORY_RHO: return stage_dispatch_prec<Rho>(g.prec, stage, g, tb, te, st);
-        case SKY_THEORY_BERGER: return stage_dispatch_prec<Berger>(g.prec, stage, g, tb, te, st);
-        case SKY_THEORY_LIGHTLY_BOUND: return stage_dispatch_prec<LightlyBound>(g.prec, stage, g, tb, te, st);
+        case SKY_THEORY_NUCLEAR: return stage_dispatch_prec<Nuclear>(g.prec, stage, g, tb, te, st, tail);
+        case SKY_THEORY_OMEGA: return stage_dispatch_prec<Omega>(g.prec, stage, g, tb, te, st, tail);
+        case SKY_THEORY_COULOMB: return stage_dispatch_prec<Coulomb>(g.prec, stage, g, tb, te, st, tail);
+        case SKY_THEORY_RHO: return stage_dispatch_prec<Rho>(g.prec, stage, g, tb, te, st, tail);
+        case SKY_THEORY_BERGER: return stage_dispatch_prec<Berger>(g.prec, stage, g, tb, te, st, tail);
+        case SKY_THEORY_LIGHTLY_BOUND: return stage_dispatch_prec<LightlyBound>(g.prec, stage, g, tb, te, st, tail);
     }
     return invalid("unknown theory id");
 }
@@ -322,16 +325,6 @@ static int launch_control(const Group& g, int ib, int ie, int mode, cudaStream_t
     return check_cuda(cudaGetLastError(), "launch engine control", __LINE__);
 }
 
-static int launch_advance(const Group& g, cudaStream_t st) {
-    const int n = (int)g.members.size();
-    if (n == 0) return SKY_OK;
-    const int b = (n + 127) / 128;
-    if (g.prec)
-        k_engine_advance<double><<<b, 128, 0, st>>>(reinterpret_cast<InstDesc<double>*>(g.d_desc), n);
-    else
-        k_engine_advance<float><<<b, 128, 0, st>>>(reinterpret_cast<InstDesc<float>*>(g.d_desc), n);
-    return check_cuda(cudaGetLastError(), "launch engine advance", __LINE__);
-}
 
 // Defect refresh of the group's defect-corrected FP32 instances (those whose
 // refresh flag the advance kernel just set; the others' tiles are skipped).
@@ -687,11 +680,11 @@ static int launch_kind(Engine& e, int kind) {
             switch (kind) {
                 case kKindS2: rc = launch_stage_group(2, g, 0, g.ntiles, e.stream); break;
                 case kKindS3: rc = launch_stage_group(3, g, 0, g.ntiles, e.stream); break;
-                case kKindS4: rc = launch_stage_group(4, g, 0, g.ntiles, e.stream); break;
-                case kKindAdvance: rc = launch_advance(g, e.stream); break;
+                case kKindS4: rc = launch_stage_group(4, g, 0, g.ntiles, e.stream, 1); break;
+                case kKindAdvance: break;  // folded into stage 4
                 case kKindDefect: rc = launch_defect(g, e.stream); break;
-                case kKindS1: rc = launch_stage_group(1, g, 0, g.ntiles, e.stream); break;
-                default: rc = launch_control(g, 0, (int)g.members.size(), 0, e.stream); break;
+                case kKindS1: rc = launch_stage_group(1, g, 0, g.ntiles, e.stream, 1); break;
+                default: break;  // the control is folded into stage 1
             }
             if (rc) return rc;
         }
@@ -711,7 +704,7 @@ static int count_launches(Engine& e) {
     for (int t = 0; t < 6; ++t)
         for (int pr = 0; pr < 2; ++pr)
             if (!e.groups[t][pr].members.empty())
-                n += kNumKinds - ((pr == 0 && e.groups[t][pr].any_defect) ? 0 : 1);
+                n += 4 + ((pr == 0 && e.groups[t][pr].any_defect) ? 1 : 0);  // stages 2, 3, 4, [defect,] 1
     return n;
 }
 

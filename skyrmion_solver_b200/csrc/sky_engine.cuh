@@ -12,7 +12,8 @@
 // fly from F, V and the previous slope and writes only l_s; stage 4 applies the
 // update into the other half of a ping-pong pair.
 //
-// One step is: stage 2, stage 3, stage 4 (+ update), advance, stage 1, control.
+// One step is: stage 2, stage 3, stage 4 (+ update; its tail advances each instance),
+// [the defect refresh,] stage 1 (its tail runs each instance's control).
 // Stage 1 runs on the freshly updated field, so besides l1 (needed by the next
 // step) it evaluates that field's energy and baryon density in FP64; the
 // control launch reduces them (compensated, fixed order), records the step's
@@ -77,6 +78,7 @@ struct InstDesc {
     int cur;           // which half of the F / V ping-pong pairs is current
     int refresh;       // this step's stage 1 refreshes the defect correction
     int refresh_period;  // steps between refreshes of the defect correction
+    int tiles_done;    // tiles of the current stage launch finished (0 between launches)
 };
 
 // RK4 update of one site (core/integrator.py:163-175): V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,
@@ -209,24 +211,21 @@ __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __r
 // ---------------------------------------------------------------------------
 // mode 0: end of a step (arrest decision); 1: admission (step 0, no arrest);
 // 2: resume after a precision change (keeps the pending arrest decision).
+// The control work of one instance, by one whole block (the control kernel, or the
+// block that finished an instance's last stage-1 tile).  The partials are read through
+// L2: in the stage kernel they were written by other blocks of the same launch.
 template <typename S>
-__global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict__ insts, int i_begin, int i_end,
-                                                        int mode) {
-    __shared__ KSum shk[32];
-    __shared__ double shm[32];
-    const int ii = i_begin + blockIdx.x;
-    if (ii >= i_end) return;
-    InstDesc<S>& in = insts[ii];
-    if (!in.active) return;
-    const int tid = threadIdx.x;
+__device__ __forceinline__ void engine_control_body(InstDesc<S>& in, int mode, KSum* shk, double* shm) {
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
     KSum e{0.0, 0.0}, b{0.0, 0.0}, kin{0.0, 0.0};
     double gm = -1.0e300, ga = 0.0;
-    for (int t = tid; t < in.ntiles; t += blockDim.x) {
-        ksum_merge(e, in.epart[t]);
-        ksum_merge(b, in.bpart[t]);
-        gm = fmax(gm, in.gpart[4 * t]);
-        ga = fmax(ga, in.gpart[4 * t + 1]);
-        ksum_merge(kin, KSum{in.gpart[4 * t + 2], in.gpart[4 * t + 3]});
+    for (int t = tid; t < in.ntiles; t += nthreads) {
+        ksum_merge(e, KSum{__ldcg(&in.epart[t].s), __ldcg(&in.epart[t].c)});
+        ksum_merge(b, KSum{__ldcg(&in.bpart[t].s), __ldcg(&in.bpart[t].c)});
+        gm = fmax(gm, __ldcg(&in.gpart[4 * t]));
+        ga = fmax(ga, __ldcg(&in.gpart[4 * t + 1]));
+        ksum_merge(kin, KSum{__ldcg(&in.gpart[4 * t + 2]), __ldcg(&in.gpart[4 * t + 3])});
     }
     KSum E = block_ksum(e, shk);
     KSum B = block_ksum(b, shk);
@@ -257,22 +256,41 @@ __global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Control: one block per instance.  Reduces the stage-1 partials (energy and
+// baryon number of the field entering this step) and the previous step's
+// stage-4 gradient partials, records StepStats and sets the arrest flag.
+// ---------------------------------------------------------------------------
+// mode 0: end of a step (arrest decision); 1: admission (step 0, no arrest);
+// 2: resume after a precision change (keeps the pending arrest decision).
+// (The steps themselves fold mode 0 into stage 1: k_march_stage with tail.)
+template <typename S>
+__global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict__ insts, int i_begin, int i_end,
+                                                        int mode) {
+    __shared__ KSum shk[32];
+    __shared__ double shm[32];
+    const int ii = i_begin + blockIdx.x;
+    if (ii >= i_end) return;
+    InstDesc<S>& in = insts[ii];
+    if (!in.active) return;
+    engine_control_body(in, mode, shk, shm);
+}
+
 // Default number of steps between refreshes of the defect correction of an FP32
 // instance (sky_engine_set_defect_period changes it per instance).
 constexpr int kDefectRefresh = 16;
 
-// Flip the ping-pong halves and advance the step counter (after stage 4); flag the
-// defect refresh of the step that now begins.
+// Flip the ping-pong halves and advance the step counter (the tail of stage 4); flag
+// the defect refresh of the step that now begins.
 template <typename S>
-__global__ void k_engine_advance(InstDesc<S>* __restrict__ insts, int ninst) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < ninst && insts[i].active) {
-        insts[i].step += 1;
-        insts[i].cur ^= 1;
-        const int period = insts[i].refresh_period > 0 ? insts[i].refresh_period : kDefectRefresh;
-        insts[i].refresh = (insts[i].Dlt != nullptr && insts[i].step % period == 0) ? 1 : 0;
-    }
+__device__ __forceinline__ void engine_advance_one(InstDesc<S>& in) {
+    in.step += 1;
+    in.cur ^= 1;
+    const int period = in.refresh_period > 0 ? in.refresh_period : kDefectRefresh;
+    in.refresh = (in.Dlt != nullptr && in.step % period == 0) ? 1 : 0;
 }
+
+
 
 // ---------------------------------------------------------------------------
 // Marching stage kernel (C <= 5 theories): the stage input is built while the
@@ -474,7 +492,8 @@ constexpr int stage_threads() {
 template <template <typename> class Th, class M, typename T, int STAGE, int MINB, bool LO = false, bool TMA = false,
           bool PAIR = false>
 __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
-    k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
+    k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end,
+                  int tail) {
     static_assert(!PAIR || (TMA && sizeof(T) == 4), "z-pair tiles: FP32 with TMA staging");
     constexpr int NSRC = STAGE == 1 ? (LO ? 2 : 1) : (STAGE == 2 ? 2 : 3);
     constexpr bool CENTRE = stage_centre<M, T, STAGE, MINB, TMA>();
@@ -485,6 +504,7 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
     __shared__ KSum shk[M::NTHREADS / 32];  // one entry per warp (kept small: two blocks
     __shared__ double shm[M::NTHREADS / 32];  // per SM need all but 1 KB of shared memory)
     __shared__ uint64_t tma_bar[3];
+    __shared__ int last_tile;  // this block finished its instance's last tile (tail)
     TmaTile tt{tma_bar, 0u, {nullptr, nullptr, nullptr}, nullptr};
     CentreStage<T> cst;
     if constexpr (TMA) {
@@ -506,6 +526,13 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
         const int ii = __ldg(tile_inst + t);
         const InstDesc<T>& in = insts[ii];
         if (!in.active) continue;  // uniform across the block
+        // An arrested step treats the velocity as zero, so its stage-2 input F + (dt/2) V is
+        // the field itself: l2 = l1, and stage 2 has nothing to compute.  Stages 3 and 4 then
+        // read l1 where they read l2.  Not after a defect refresh: that stage 1 formed l1 from
+        // the FP64 gradient, and stage 2's FP32 gradient plus the new correction may differ
+        // from it in the last bit.
+        const bool l2_is_l1 = in.arrested && !in.refresh;
+        if (STAGE == 2 && l2_is_l1) continue;
         const Params p = in.p;
         const int parity = in.cur;
         const int lt = t - in.tile_begin;
@@ -515,11 +542,12 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
         const T* F = in.F[parity];
         const T* V = in.arrested ? nullptr : in.V[parity];
         const T dtt = T(p.dt), hdt = T(0.5 * p.dt);
-        const T* const src[3] = {F, LO ? in.Flo[parity] : V, STAGE == 3 ? in.L[0] : in.L[1]};
+        T* const L2 = l2_is_l1 ? in.L[0] : in.L[1];  // the step's l2
+        const T* const src[3] = {F, LO ? in.Flo[parity] : V, STAGE == 3 ? in.L[0] : L2};
         const T a = STAGE == 4 ? dtt : hdt;
         const T b = STAGE == 3 ? T(0.25) * dtt : T(0.5) * dtt;
         using Epi = EngineEpi<T, STAGE, M::C, CENTRE, PAIR ? 2 : 1>;
-        Epi epi{{F, in.Flo[parity], V, in.L[0], in.L[1], in.L[2]},
+        Epi epi{{F, in.Flo[parity], V, in.L[0], L2, in.L[2]},
                                 STAGE < 4 ? in.L[STAGE - 1] : in.F[parity ^ 1],
                                 STAGE < 4 ? nullptr : in.V[parity ^ 1],
                                 in.Flo[parity ^ 1],
@@ -529,7 +557,7 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
         if constexpr (TMA) {
             tt.map[0] = &in.tm[kMapF + parity];
             tt.map[1] = LO ? &in.tm[kMapFlo + parity] : (V != nullptr ? &in.tm[kMapV + parity] : nullptr);
-            tt.map[2] = NSRC > 2 ? &in.tm[kMapL + (STAGE == 3 ? 0 : 1)] : nullptr;
+            tt.map[2] = NSRC > 2 ? &in.tm[kMapL + (STAGE == 3 || l2_is_l1 ? 0 : 1)] : nullptr;
             tt.status = in.status;
         }
         if constexpr (CENTRE) {
@@ -537,7 +565,7 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
             cst.map[1] = in.Flo[parity] != nullptr ? &in.tmc[kMapFlo + parity] : nullptr;
             cst.map[2] = V != nullptr ? &in.tmc[kMapV + parity] : nullptr;
             cst.map[3] = &in.tmc[kMapL];
-            cst.map[4] = &in.tmc[kMapL + 1];
+            cst.map[4] = &in.tmc[kMapL + (l2_is_l1 ? 0 : 1)];
             cst.map[5] = &in.tmc[kMapL + 2];
             cst.map[6] = in.Dlt != nullptr ? &in.tmc[kMapDlt] : nullptr;
             cst.status = in.status;
@@ -552,8 +580,8 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
         else
             ok = march_tile<Th, M, T, NSRC, STAGE == 1, Epi, LO, T, true, TMA>(sm, p, src, a, b, xa, xe, y0, z0, epi,
                                                                              es, bs, TMA ? &tt : nullptr);
-        if (!ok) return;  // a copy did not arrive: the block's error bit is set, its partials stay stale
-        if (STAGE == 1) {
+        // !ok: a copy did not arrive; the block's error bit is set and its partials stay stale
+        if (ok && STAGE == 1) {
             const KSum be = block_ksum(es, shk);
             const KSum bb = block_ksum(bs, shk);
             if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -561,7 +589,7 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
                 in.bpart[lt] = bb;
             }
         }
-        if (STAGE == 4) {
+        if (ok && STAGE == 4) {
             // a thread without sites keeps -inf, which block_max maps below every gradient
             const double ga = block_max(fmax(double(epi.gmx), -1.0e300), shm);
             const double gb = block_max(double(epi.gab), shm);
@@ -573,6 +601,29 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
                 in.gpart[4 * lt + 3] = kk.c;
             }
         }
+        // tail: the block that finishes an instance's last tile does that instance's advance
+        // (stage 4) or its control (stage 1: reduction, statistics, arrest decision), so a
+        // step needs no separate launches for them.  Each block publishes its tile's
+        // partials (fence) before counting the tile; the counter returns to 0.
+        if constexpr (STAGE == 1 || STAGE == 4) {
+            if (tail) {
+                if (threadIdx.x == 0 && threadIdx.y == 0) {
+                    __threadfence();
+                    last_tile = atomicAdd(&insts[ii].tiles_done, 1) == in.ntiles - 1 ? 1 : 0;
+                }
+                __syncthreads();
+                if (last_tile) {
+                    __threadfence();
+                    if constexpr (STAGE == 4) {
+                        if (threadIdx.x == 0 && threadIdx.y == 0) engine_advance_one(insts[ii]);
+                    } else {
+                        engine_control_body(insts[ii], 0, shk, shm);
+                    }
+                    if (threadIdx.x == 0 && threadIdx.y == 0) insts[ii].tiles_done = 0;
+                }
+            }
+        }
+        if (!ok) return;
     }
 }
 
