@@ -284,8 +284,8 @@ int sky_engine_destroy(void* engine);
  * steps an FP64 gradient of hi + lo is evaluated and the difference to the FP32
  * gradient of the same field is added to every stage's FP32 gradient until the
  * next refresh, so the flow's fixed point is the FP64 one while the stencils stay
- * FP32 (theories with at most five components; rho runs 3 as 2).  field / velocity
- * are FP64 in the reference layout (host pointers,
+ * FP32 (every theory; rho's thirteen-component FP64 refresh walks 4-row sub-tiles).
+ * field / velocity are FP64 in the reference layout (host pointers,
  * or device pointers when on_device != 0); velocity may be NULL (zero).  The
  * energy of the admitted field is evaluated immediately (stats record 0). */
 int sky_engine_add(void* engine, int theory, const int32_t* p_i, int32_t n_pi, const double* p_f, int32_t n_pf,

@@ -22,7 +22,7 @@ struct HostInst {
     int theory = 0;
     int prec = 0;  // storage: 0 = FP32 storage/arithmetic, 1 = FP64
     int comp = 0;    // FP32 storage with a compensated (hi + lo) field
-    int defect = 0;  // ... and a defect-corrected gradient (precision 3; marching theories only)
+    int defect = 0;  // ... and a defect-corrected gradient (precision 3)
     int defect_period = kDefectRefresh;  // steps between refreshes of the correction
     Params p{};
     int64_t N = 0;
@@ -330,8 +330,8 @@ static int launch_control(const Group& g, int ib, int ie, int mode, cudaStream_t
 // refresh flag the advance kernel just set; the others' tiles are skipped).
 template <template <typename> class Th, bool WIDE>
 static int launch_defect_t(const Group& g, cudaStream_t st) {
-    using M = MarchShape<Th<double>::C, kMarchBY, WIDE>;
-    auto kern = k_march_defect<Th, M>;
+    using M = MarchShape<Th<double>::C, march_by<Th, double>(), WIDE && march_wide_allowed<Th, double>()>;
+    auto kern = k_march_defect<Th, M, march_by<Th, float>()>;
     const size_t smem = M::template smem_bytes<double, float>(2);
     static int per_sm = 0;
     if (per_sm == 0) {
@@ -365,6 +365,7 @@ static int launch_defect(const Group& g, cudaStream_t st) {
         case SKY_THEORY_COULOMB: return launch_defect_w<Coulomb>(g, st);
         case SKY_THEORY_BERGER: return launch_defect_w<Berger>(g, st);
         case SKY_THEORY_LIGHTLY_BOUND: return launch_defect_w<LightlyBound>(g, st);
+        case SKY_THEORY_RHO: return launch_defect_w<Rho>(g, st);
         default: return SKY_OK;
     }
 }
@@ -892,7 +893,7 @@ int sky_engine_add(void* handle, int theory, const int32_t* p_i, int32_t n_pi, c
     h.theory = theory;
     h.prec = precision == 1 ? 1 : 0;
     h.comp = precision >= 2 ? 1 : 0;
-    h.defect = (precision == 3 && theory_components(theory) <= 5) ? 1 : 0;
+    h.defect = precision == 3 ? 1 : 0;
     h.N = n_sites(h.p);
     h.C = h.p.C;
     if ((rc = alloc_inst(*e, h))) return rc;
@@ -935,10 +936,8 @@ int sky_engine_set_precision(void* handle, int id, int precision) {
     HostInst* hp = find(e, id);
     if (!hp) return invalid("unknown instance id");
     if (precision < 0 || precision > 3) return invalid("precision must be 0, 1, 2 or 3");
-    const int defect_new = (precision == 3 && theory_components(hp->theory) <= 5) ? 1 : 0;
-    if ((hp->comp ? 2 + hp->defect : hp->prec) == precision ||
-        (precision == 3 && hp->comp && !defect_new))
-        return SKY_OK;
+    const int defect_new = precision == 3 ? 1 : 0;
+    if ((hp->comp ? 2 + hp->defect : hp->prec) == precision) return SKY_OK;
     cudaSetDevice(e->device);
     cudaStreamSynchronize(e->stream);
     HostInst& h = *hp;

@@ -313,12 +313,14 @@ struct CentreStage {
 };
 constexpr int kCentreArrays = 7;
 
-// CC: components of the theory; the defect correction exists only for CC <= 5.
+// CC: components of the theory.
 // CENTRE: stage 4 reads the update's operands from shared memory (CentreStage).
 // NL: sites per thread (2 for the z-pair tiles: lane l is the thread's site l).
 template <typename T, int STAGE, int CC, bool CENTRE = false, int NL = 1>
 struct EngineEpi {
-    static constexpr bool kDefect = CC <= 5;  // instances of this theory can carry a correction
+    // the correction of the thread's next site is held in registers (prefetched a plane
+    // ahead) for CC <= 5; with more components it is read at the site
+    static constexpr bool kPrefetch = CC <= 5;
     // inputs of the stage-4 update, read from global memory at the site (prefetching them
     // into shared memory with cp.async measured slower: more instructions and shared memory)
     const T* fin_src[6];  // F, F_lo (null unless compensated), V (null when arrested), l1, l2, l3
@@ -339,8 +341,8 @@ struct EngineEpi {
     int refresh;  // stage 1 of a refresh step: dlt holds g64 of the field; replace it by g64 - g32
     CentreStage<T>* cs = nullptr;  // CENTRE: the plane's staged operands
     int zbase = 0;                 // z of the thread's first site within the tile
-    T d[NL][kDefect ? CC : 1];     // the site's correction
-    T dn[NL][kDefect ? CC : 1];    // the correction of the thread's site on the next plane, in flight
+    T d[NL][kPrefetch ? CC : 1];   // the site's correction
+    T dn[NL][kPrefetch ? CC : 1];  // the correction of the thread's site on the next plane, in flight
     int64_t dn_tag[NL];            // 1 + the site dn belongs to (0: none; value-initialised)
     // CENTRE: thread 0 copies the update's operands of plane x (every thread calls this
     // right after the plane barrier, before the stencil arithmetic).
@@ -364,7 +366,7 @@ struct EngineEpi {
     // overlaps a whole plane of stencil and point arithmetic.
     __device__ __forceinline__ void begin_site(int64_t s, int64_t N, int64_t next, int l = 0) {
         if constexpr (CENTRE) return;  // the correction comes with the staged operands
-        if constexpr (kDefect) {
+        if constexpr (kPrefetch) {
             if (dlt) {
                 if (dn_tag[l] == s + 1) {
 #pragma unroll
@@ -419,18 +421,24 @@ struct EngineEpi {
                 kin_t += hvol * v2;
             return;
         }
-        if constexpr (kDefect) {
-            if (dlt) {
-                if (STAGE == 1 && refresh) {   // d = g64(F): the correction becomes g64 - g32(F)
+        if (dlt) {
+            T dd[C];
 #pragma unroll
-                    for (int c = 0; c < C; ++c) {
-                        __stcg(dlt + c * N + s, d[l][c] - g32[c]);
-                        g[c] = d[l][c];
-                    }
-                } else {
+            for (int c = 0; c < C; ++c) {
+                if constexpr (kPrefetch)
+                    dd[c] = d[l][c];
+                else
+                    dd[c] = __ldcg(dlt + c * N + s);
+            }
+            if (STAGE == 1 && refresh) {   // dd = g64(F): the correction becomes g64 - g32(F)
 #pragma unroll
-                    for (int c = 0; c < C; ++c) g[c] = g32[c] + d[l][c];
+                for (int c = 0; c < C; ++c) {
+                    __stcg(dlt + c * N + s, dd[c] - g32[c]);
+                    g[c] = dd[c];
                 }
+            } else {
+#pragma unroll
+                for (int c = 0; c < C; ++c) g[c] = g32[c] + dd[c];
             }
         }
         if (STAGE < 4) {
@@ -642,9 +650,12 @@ struct DefectEpi {
     }
 };
 
-template <template <typename> class Th, class M>
+// TBY: rows of the engine's FP32 tiles; the FP64 ring walks each as TBY / M::BY sub-tiles
+// (4-row sub-tiles for 13 components, whose FP64 ring of 8-row planes would not fit).
+template <template <typename> class Th, class M, int TBY>
 __global__ void __launch_bounds__(M::NTHREADS, 1)
     k_march_defect(InstDesc<float>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end) {
+    static_assert(TBY % M::BY == 0, "sub-tiles of the engine tile's rows");
     extern __shared__ __align__(16) unsigned char smraw[];
     double* sm = reinterpret_cast<double*>(smraw);
     for (int t = t_begin + blockIdx.x; t < t_end; t += gridDim.x) {
@@ -655,12 +666,13 @@ __global__ void __launch_bounds__(M::NTHREADS, 1)
         const int lt = t - in.tile_begin;
         const MarchGrid mg{in.tiles_nz, in.tiles_ny, in.tiles_nx, in.xc};
         int xa, xe, y0, z0;
-        march_origin(mg, lt, M::BY, xa, xe, y0, z0, p.X);
+        march_origin(mg, lt, TBY, xa, xe, y0, z0, p.X);
         const float* const src[3] = {in.F[in.cur], in.Flo[in.cur], nullptr};
         DefectEpi epi{in.Dlt};
         KSum es{0.0, 0.0}, bs{0.0, 0.0};
-        march_tile<Th, M, double, 2, false, DefectEpi, false, float>(sm, p, src, 1.0, 0.0, xa, xe, y0, z0, epi, es,
-                                                                     bs);
+        for (int sy = 0; sy < TBY && y0 + sy < p.Y; sy += M::BY)
+            march_tile<Th, M, double, 2, false, DefectEpi, false, float>(sm, p, src, 1.0, 0.0, xa, xe, y0 + sy, z0,
+                                                                         epi, es, bs);
     }
 }
 

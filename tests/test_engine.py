@@ -289,10 +289,13 @@ def test_rk4_dynamics_and_kinetic_energy(engine, name):
         engine.remove(iid)
 
 
-def test_fp32d_tracks_fp64(engine):
-    d, F, V, p_i, p_f = _inputs("omega")
-    a = engine.add("omega", (p_i, p_f), F, V, precision="fp64")
-    b = engine.add("omega", (p_i, p_f), F, V, precision="fp32d")
+@pytest.mark.parametrize("name", ["omega", "rho"])
+def test_fp32d_tracks_fp64(engine, name):
+    """Defect-corrected FP32 against FP64 over twenty steps (a refresh of the correction at step
+    16); rho's refresh is the thirteen-component FP64 gradient walked in 4-row sub-tiles."""
+    d, F, V, p_i, p_f = _inputs(name)
+    a = engine.add(name, (p_i, p_f), F, V, precision="fp64")
+    b = engine.add(name, (p_i, p_f), F, V, precision="fp32d")
     try:
         engine.step(20)        # crosses a defect refresh at step 16
         sa, sb = engine.stats(a), engine.stats(b)

@@ -45,7 +45,7 @@ def _run(name, dims, precision, staging, nsteps, seed=5):
 
 
 @pytest.mark.parametrize("name,precision", [("omega", "fp32d"), ("omega", "fp32"), ("nuclear", "fp32c"),
-                                            ("coulomb", "fp32"), ("berger", "fp32d"), ("rho", "fp32"),
+                                            ("coulomb", "fp32"), ("berger", "fp32d"), ("rho", "fp32"), ("rho", "fp32d"),
                                             ("omega", "fp64"), ("nuclear", "fp64")])
 def test_tma_staging_equals_cp_async_staging(name, precision):
     dims = (23, 13, 44)
