@@ -795,7 +795,8 @@ def run_serve(args):
                           args.max_steps)
     # 1. continuous batching on the resident engine
     with Engine(0) as eng:
-        srv = Server(eng, chunk=64, fp32_mode=args.schedule, defect_period=args.defect_period)
+        srv = Server(eng, chunk=64, fp32_mode=args.schedule, defect_period=args.defect_period,
+                     switch_factor=args.switch_factor, plateau_chunks=args.plateau_chunks)
         for r, _, _ in reqs:
             srv.submit(r)
         torch.cuda.synchronize()
@@ -804,7 +805,7 @@ def run_serve(args):
     # 2. the same requests solved one after another on the plain FP64 drop-in path
     serial = {}
     t_all = 0.0
-    for r, prm, th in reqs:
+    for r, prm, th in ([] if args.no_serial else reqs):
         sim = Simulation(prm, th)
         f0 = build_device_field(r.theory, r.p_i, r.p_f, r.init)      # the same field the server built
         if r.theory == "omega":
@@ -831,6 +832,8 @@ def run_serve(args):
         serial[r.rid] = dict(status=status, steps=n, energy=e, seconds=dt)
         del sim
     # relative to max(|E|, 1): a configuration that unwinds to the vacuum (E -> 0) compares absolutely
+    if args.no_serial:
+        serial = {k: dict(status=None, steps=None, energy=math.nan, seconds=None) for k in served}
     rel = [abs(served[k].energy - serial[k]["energy"]) / max(abs(serial[k]["energy"]), 1.0) for k in served
            if served[k].status == "converged" and serial[k]["status"] == "converged"]
     n_serial = sum(v["status"] == "converged" for v in serial.values())
@@ -854,10 +857,12 @@ def run_serve(args):
                        "tol_max_abs_gradient": GRAD_TOL, "defect_period": args.defect_period or 16,
                        "schedule": {"fp64": "fp64 throughout",
                                     "fp32d": "fp32d until max|g| <= tol or a stall, then fp64"}.get(
-                           args.schedule, f"{args.schedule} until twice the FP32 gradient floor, then fp64")},
+                           args.schedule, f"{args.schedule} until {args.switch_factor:g} x the FP32 gradient "
+                                          f"floor or a stall of {args.plateau_chunks * 64} steps, then fp64")},
             "served": summ,
             "by_theory": by_theory,
-            "serial_plain_fp64": {"converged": n_serial, "seconds": t_all, "solves_per_s": serial_sps},
+            "serial_plain_fp64": None if args.no_serial else {"converged": n_serial, "seconds": t_all,
+                                                              "solves_per_s": serial_sps},
             "speedup_solves_per_s": (summ["solves_per_s"] / serial_sps) if (summ["solves_per_s"] and serial_sps)
             else None,
             "max_rel_energy_diff_vs_plain_fp64": max(rel) if rel else None,
@@ -1095,6 +1100,11 @@ def main():
     ap.add_argument("--schedule", choices=("fp32d", "fp32c", "fp32", "fp64"), default="fp64",
                     help="serving precision schedule: FP32 phase then FP64, or FP64 throughout")
     ap.add_argument("--max-side", type=int, default=192)
+    ap.add_argument("--switch-factor", type=float, default=2.0,
+                    help="serving: fp32 / fp32c requests switch to FP64 at this multiple of the FP32 gradient floor")
+    ap.add_argument("--plateau-chunks", type=int, default=256,
+                    help="serving: 64-step chunks without a 1%% gain in max|g| after which the FP32 phase ends")
+    ap.add_argument("--no-serial", action="store_true", help="serving: skip the serial plain FP64 solves")
     ap.add_argument("--defect-period", type=int, default=None,
                     help="serving: steps between refreshes of the fp32d correction (default 16)")
     ap.add_argument("--render", action="store_true", help="headless viewer: volume builder and ray-march")

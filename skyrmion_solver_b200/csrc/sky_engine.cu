@@ -52,6 +52,7 @@ struct Group {
     std::vector<int> members;  // instance ids in slot order
     void* d_desc = nullptr;    // InstDesc<S>[cap]
     int* d_tile_inst = nullptr;
+    int* d_done = nullptr;     // blocks of the current tail stage launch finished (0 between launches)
     int desc_cap = 0, tile_cap = 0;
     int ntiles = 0;
     bool any_comp = false;  // holds a compensated-field instance (stage 1 stages the low parts too)
@@ -159,7 +160,7 @@ static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t s
     const size_t smem = stage_smem<Th, T, STAGE, WIDE, LO, TMA>();
     const dim3 block(PAIR ? PairShape<M>::TZ : M::BZ, M::BY);
     k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO, TMA, PAIR><<<blocks, block, smem, st>>>(
-        d, g.d_tile_inst, t_begin, t_end, tail);
+        d, d, g.d_tile_inst, t_begin, t_end, tail ? g.d_done : nullptr);
     return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
 }
 
@@ -319,9 +320,9 @@ static int tile_shape(int theory, int prec, int& bz, int& by, int& tx, int& per_
 static int launch_control(const Group& g, int ib, int ie, int mode, cudaStream_t st) {
     if (ie <= ib) return SKY_OK;
     if (g.prec)
-        k_engine_control<double><<<ie - ib, 256, 0, st>>>(reinterpret_cast<InstDesc<double>*>(g.d_desc), ib, ie, mode);
+        k_engine_control<double><<<ie - ib, 32, 0, st>>>(reinterpret_cast<InstDesc<double>*>(g.d_desc), ib, ie, mode);
     else
-        k_engine_control<float><<<ie - ib, 256, 0, st>>>(reinterpret_cast<InstDesc<float>*>(g.d_desc), ib, ie, mode);
+        k_engine_control<float><<<ie - ib, 32, 0, st>>>(reinterpret_cast<InstDesc<float>*>(g.d_desc), ib, ie, mode);
     return check_cuda(cudaGetLastError(), "launch engine control", __LINE__);
 }
 
@@ -514,6 +515,11 @@ static int rebuild_group_t(Engine& e, Group& g) {
         int rc = check_cuda(cudaMalloc(&g.d_desc, sizeof(InstDesc<S>) * g.desc_cap), "cudaMalloc(desc)", __LINE__);
         if (rc) return rc;
         cudaMemsetAsync(g.d_desc, 0, sizeof(InstDesc<S>) * g.desc_cap, e.stream);
+    }
+    if (!g.d_done) {
+        int rc = check_cuda(cudaMalloc(&g.d_done, sizeof(int)), "cudaMalloc(done)", __LINE__);
+        if (rc) return rc;
+        cudaMemsetAsync(g.d_done, 0, sizeof(int), e.stream);
     }
     if ((int)tile_inst.size() > g.tile_cap) {
         if (g.d_tile_inst) cudaFree(g.d_tile_inst);
@@ -871,6 +877,7 @@ int sky_engine_destroy(void* handle) {
         for (int p = 0; p < 2; ++p) {
             if (e->groups[t][p].d_desc) cudaFree(e->groups[t][p].d_desc);
             if (e->groups[t][p].d_tile_inst) cudaFree(e->groups[t][p].d_tile_inst);
+            if (e->groups[t][p].d_done) cudaFree(e->groups[t][p].d_done);
         }
     if (e->d_status) cudaFree(e->d_status);
     cudaStreamDestroy(e->stream);

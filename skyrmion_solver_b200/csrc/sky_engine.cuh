@@ -78,7 +78,6 @@ struct InstDesc {
     int cur;           // which half of the F / V ping-pong pairs is current
     int refresh;       // this step's stage 1 refreshes the defect correction
     int refresh_period;  // steps between refreshes of the defect correction
-    int tiles_done;    // tiles of the current stage launch finished (0 between launches)
 };
 
 // RK4 update of one site (core/integrator.py:163-175): V' = V + (l1 + 2 l2 + 2 l3 + l4)/6,
@@ -211,29 +210,37 @@ __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __r
 // ---------------------------------------------------------------------------
 // mode 0: end of a step (arrest decision); 1: admission (step 0, no arrest);
 // 2: resume after a precision change (keeps the pending arrest decision).
-// The control work of one instance, by one whole block (the control kernel, or the
-// block that finished an instance's last stage-1 tile).  The partials are read through
-// L2: in the stage kernel they were written by other blocks of the same launch.
+// The control work of one instance, by one warp (the control kernel, or warp 0 of the
+// block that finished an instance's last stage-1 tile): lane-strided compensated sums of
+// the per-tile partials and a fixed shuffle tree, so the order depends on the tile count
+// only.  The partials are read through L2: in the stage kernel they were written by
+// other blocks of the same launch.
 template <typename S>
-__device__ __forceinline__ void engine_control_body(InstDesc<S>& in, int mode, KSum* shk, double* shm) {
-    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+__device__ __forceinline__ void engine_control_warp(InstDesc<S>& in, int mode) {
+    const int lane = (threadIdx.x + blockDim.x * threadIdx.y) & 31;
     KSum e{0.0, 0.0}, b{0.0, 0.0}, kin{0.0, 0.0};
     double gm = -1.0e300, ga = 0.0;
-    for (int t = tid; t < in.ntiles; t += nthreads) {
+    for (int t = lane; t < in.ntiles; t += 32) {
         ksum_merge(e, KSum{__ldcg(&in.epart[t].s), __ldcg(&in.epart[t].c)});
         ksum_merge(b, KSum{__ldcg(&in.bpart[t].s), __ldcg(&in.bpart[t].c)});
         gm = fmax(gm, __ldcg(&in.gpart[4 * t]));
         ga = fmax(ga, __ldcg(&in.gpart[4 * t + 1]));
         ksum_merge(kin, KSum{__ldcg(&in.gpart[4 * t + 2]), __ldcg(&in.gpart[4 * t + 3])});
     }
-    KSum E = block_ksum(e, shk);
-    KSum B = block_ksum(b, shk);
-    KSum K = block_ksum(kin, shk);
-    const double GM = block_max(gm, shm);
-    const double GA = block_max(ga, shm);
-    if (tid == 0) {
-        const double en = E.s + E.c;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const KSum oe = ksum_shfl_down(e, off), ob = ksum_shfl_down(b, off), ok = ksum_shfl_down(kin, off);
+        const double om = __shfl_down_sync(0xffffffffu, gm, off), oa = __shfl_down_sync(0xffffffffu, ga, off);
+        if (lane + off < 32) {
+            ksum_merge(e, oe);
+            ksum_merge(b, ob);
+            ksum_merge(kin, ok);
+            gm = fmax(gm, om);
+            ga = fmax(ga, oa);
+        }
+    }
+    if (lane == 0) {
+        const double en = e.s + e.c;
         if (mode == 1) in.step = 0;
         const int n = in.step;
         // arrest (core/integrator.py:403-407): the energy after step n exceeds the one after step n-1
@@ -242,11 +249,11 @@ __device__ __forceinline__ void engine_control_body(InstDesc<S>& in, int mode, K
         if (mode == 1) arrest = 0;
         StepStats& st = in.stats[n % in.stats_cap];
         st.energy = en;
-        st.baryon = B.s + B.c;
+        st.baryon = b.s + b.c;
         if (mode != 2) {  // a resume keeps the step's gradient statistics
-            st.err = (n > 0) ? GM : 0.0;
-            st.kinetic = (n > 0) ? K.s + K.c : 0.0;
-            st.gabs = (n > 0) ? GA : 0.0;
+            st.err = (n > 0) ? gm : 0.0;
+            st.kinetic = (n > 0) ? kin.s + kin.c : 0.0;
+            st.gabs = (n > 0) ? ga : 0.0;
         }
         st.arrested = arrest;
         st.step = n;
@@ -265,15 +272,13 @@ __device__ __forceinline__ void engine_control_body(InstDesc<S>& in, int mode, K
 // 2: resume after a precision change (keeps the pending arrest decision).
 // (The steps themselves fold mode 0 into stage 1: k_march_stage with tail.)
 template <typename S>
-__global__ void __launch_bounds__(256) k_engine_control(InstDesc<S>* __restrict__ insts, int i_begin, int i_end,
-                                                        int mode) {
-    __shared__ KSum shk[32];
-    __shared__ double shm[32];
+__global__ void __launch_bounds__(32) k_engine_control(InstDesc<S>* __restrict__ insts, int i_begin, int i_end,
+                                                       int mode) {
     const int ii = i_begin + blockIdx.x;
     if (ii >= i_end) return;
     InstDesc<S>& in = insts[ii];
     if (!in.active) return;
-    engine_control_body(in, mode, shk, shm);
+    engine_control_warp(in, mode);
 }
 
 // Default number of steps between refreshes of the defect correction of an FP32
@@ -500,8 +505,8 @@ constexpr int stage_threads() {
 template <template <typename> class Th, class M, typename T, int STAGE, int MINB, bool LO = false, bool TMA = false,
           bool PAIR = false>
 __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
-    k_march_stage(InstDesc<T>* __restrict__ insts, const int* __restrict__ tile_inst, int t_begin, int t_end,
-                  int tail) {
+    k_march_stage(const InstDesc<T>* __restrict__ insts, InstDesc<T>* ctl, const int* __restrict__ tile_inst,
+                  int t_begin, int t_end, int* done) {
     static_assert(!PAIR || (TMA && sizeof(T) == 4), "z-pair tiles: FP32 with TMA staging");
     constexpr int NSRC = STAGE == 1 ? (LO ? 2 : 1) : (STAGE == 2 ? 2 : 3);
     constexpr bool CENTRE = stage_centre<M, T, STAGE, MINB, TMA>();
@@ -512,7 +517,6 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
     __shared__ KSum shk[M::NTHREADS / 32];  // one entry per warp (kept small: two blocks
     __shared__ double shm[M::NTHREADS / 32];  // per SM need all but 1 KB of shared memory)
     __shared__ uint64_t tma_bar[3];
-    __shared__ int last_tile;  // this block finished its instance's last tile (tail)
     TmaTile tt{tma_bar, 0u, {nullptr, nullptr, nullptr}, nullptr};
     CentreStage<T> cst;
     if constexpr (TMA) {
@@ -609,29 +613,38 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
                 in.gpart[4 * lt + 3] = kk.c;
             }
         }
-        // tail: the block that finishes an instance's last tile does that instance's advance
-        // (stage 4) or its control (stage 1: reduction, statistics, arrest decision), so a
-        // step needs no separate launches for them.  Each block publishes its tile's
-        // partials (fence) before counting the tile; the counter returns to 0.
-        if constexpr (STAGE == 1 || STAGE == 4) {
-            if (tail) {
-                if (threadIdx.x == 0 && threadIdx.y == 0) {
-                    __threadfence();
-                    last_tile = atomicAdd(&insts[ii].tiles_done, 1) == in.ntiles - 1 ? 1 : 0;
-                }
-                __syncthreads();
-                if (last_tile) {
-                    __threadfence();
+        if (!ok) break;
+    }
+    // tail (done != null, stages 1 and 4): the last block of the launch to finish runs the
+    // advance (stage 4) or the control (stage 1: reductions, statistics, arrest decision) of
+    // every active instance of the launch, one warp per instance, so a step needs no separate
+    // launches for them.  Each block publishes its partials (fence) before it is counted; the
+    // counter returns to 0 for the next launch.  The tail sits after the tile loop so that its
+    // registers do not add to the stencil loop's.
+    if constexpr (STAGE == 1 || STAGE == 4) {
+        if (done != nullptr) {
+            __shared__ int last_block;
+            const int ltid = threadIdx.x + blockDim.x * threadIdx.y;
+            if (ltid == 0) {
+                __threadfence();
+                last_block = atomicAdd(done, 1) == int(gridDim.x) - 1 ? 1 : 0;
+            }
+            __syncthreads();
+            if (last_block) {
+                __threadfence();
+                const int nw = int(blockDim.x * blockDim.y) >> 5;
+                const int i1 = __ldg(tile_inst + t_end - 1) + 1;
+                for (int i = __ldg(tile_inst + t_begin) + (ltid >> 5); i < i1; i += nw) {
+                    if (!ctl[i].active) continue;
                     if constexpr (STAGE == 4) {
-                        if (threadIdx.x == 0 && threadIdx.y == 0) engine_advance_one(insts[ii]);
+                        if ((ltid & 31) == 0) engine_advance_one(ctl[i]);
                     } else {
-                        engine_control_body(insts[ii], 0, shk, shm);
+                        engine_control_warp(ctl[i], 0);
                     }
-                    if (threadIdx.x == 0 && threadIdx.y == 0) insts[ii].tiles_done = 0;
                 }
+                if (ltid == 0) *done = 0;
             }
         }
-        if (!ok) return;
     }
 }
 

@@ -123,12 +123,14 @@ class Server:
                  switch_tol: float | None = None, plateau_chunks: int = 256, plateau_gain: float = 0.99,
                  polish: bool = True,
                  keep_fields: bool = True, free_bytes=None, clock=time.perf_counter, sleep=time.sleep,
-                 fp32_mode: str = "fp32d", tune_cache=None, defect_period: int | None = None):
+                 fp32_mode: str = "fp32d", tune_cache=None, defect_period: int | None = None,
+                 switch_factor: float = 2.0):
         self.engine = engine
         self.mem_cap = float(mem_cap_bytes)
         self.reserve = float(reserve_bytes)
         self.chunk = int(chunk)
-        self.switch_tol = switch_tol   # None: twice the request's estimated FP32 gradient floor
+        self.switch_tol = switch_tol   # None: switch_factor x the request's estimated FP32 gradient floor
+        self.switch_factor = float(switch_factor)
         self.plateau_chunks = int(plateau_chunks)
         self.plateau_gain = float(plateau_gain)
         self.polish = polish
@@ -197,7 +199,7 @@ class Server:
             return float(self.switch_tol)
         if self.fp32_mode == "fp32d":      # the corrected gradient reaches the tolerance itself
             return req.tol
-        return 2.0 * fp32_gradient_floor(req.p_f)
+        return self.switch_factor * fp32_gradient_floor(req.p_f)
 
     def _retire(self, lv: _Live, st, status: str):
         f = None

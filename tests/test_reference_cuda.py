@@ -7,7 +7,9 @@
    observable on Numba device arrays.  Three steps from the golden inputs match the golden steps
    that the reference produced (1e-10 relative per step, as the other step parity tests).
 2. The reference's own theory kernels (its Numba gradient, energy and norm kernels) and this
-   package's drop-in path agree step by step from the same field (1e-10 relative energy).
+   package's drop-in path agree step by step from the same field (1e-10 relative energy), on a
+   ragged 40 x 36 x 44 lattice and at the full sizes of two benchmark configurations: the
+   nuclear 64^3 seeded hedgehog (h = 0.2) and the omega B = 4 rational map on 128^3 (h = 0.15).
 
 Skipped when the reference is not installed (``tests/_reference.py`` says how to install it).
 """
@@ -79,3 +81,39 @@ def test_reference_kernels_and_drop_in_agree(name):
     fr = ref.Field.copy_to_host()
     fo = ours.Field.cpu().numpy()
     assert G.rel_err(fo, fr) <= STEP_TOL
+
+
+def _configured(name):
+    from tests.test_config_parity import _nuclear64, _omega128
+    return {"nuclear64": _nuclear64, "omega128": _omega128}[name]()
+
+
+@pytest.mark.parametrize("key", ["nuclear64", "omega128"])
+def test_reference_kernels_and_drop_in_agree_at_config_size(key):
+    """The reference's Simulation with its own theory module against this package's Simulation on a
+    benchmark configuration's full lattice, from the field this package's initialiser builds (the
+    seeded hedgehog with noise, or the B = 4 rational map with omega seeded as -c_omega B0): two
+    FP64 arrested-Newton steps, energy, err and field within 1e-10 relative."""
+    import torch
+    from skyrmion_solver_b200.core.simulation import Simulation as OurSimulation
+    th, p, cfg = _configured(key)
+    theories, Simulation, _ = R.load((th.SHORT_NAME,))
+    ref_th = theories[th.SHORT_NAME]
+    ours = OurSimulation(p, th)
+    ours.initialize(cfg)
+    torch.cuda.synchronize()
+    kw = {k: getattr(p, k) for k in ("xlen", "ylen", "zlen", "lsx", "lsy", "lsz", "xsize", "ysize", "zsize",
+                                     "time_step", "killkinen")}
+    ref = Simulation(ref_th.params.Params(**kw), ref_th)
+    assert np.array_equal(ref.p_i_h, ours.p_i_h) and np.array_equal(ref.p_f_h, ours.p_f_h)
+    ref.Field.copy_to_device(np.ascontiguousarray(ours.Field.cpu().numpy()))
+    ref.Velocity.copy_to_device(np.zeros(ours.Velocity.numel()))
+    er = ref.observables()["energy"]
+    eo = ours.observables()["energy"]
+    assert abs(er - eo) <= STEP_TOL * abs(er)
+    for s in range(2):
+        er, errr = ref.step(er)
+        eo, erro = ours.step(eo)
+        assert abs(er - eo) <= STEP_TOL * abs(er), (s, er, eo)
+        assert abs(errr - erro) <= STEP_TOL * max(1.0, abs(errr)), (s, errr, erro)
+    assert G.rel_err(ours.Field.cpu().numpy(), ref.Field.copy_to_host()) <= STEP_TOL
