@@ -303,6 +303,16 @@ int sky_engine_set_precision(void* engine, int id, int precision);
  * (0 = automatic choice from the grid and the SM count).  The state and the
  * pending arrest decision carry over. */
 int sky_engine_retile(void* engine, int id, int xc);
+/* Staging of an instance's planes in the marching stage kernels: tma = 1 copies
+ * each haloed plane with one tensor-memory-accelerator box copy per source (Z *
+ * element size a multiple of 16 bytes; not FP64 rho), 0 with per-thread cp.async
+ * copies; pair = 1 runs two z-sites per thread with packed FP32x2 arithmetic (TMA,
+ * FP32 omega only).  Admission takes both from library options 2 and 3; a group of
+ * instances of one theory and precision stages by TMA (z-pairs) only when every
+ * member does.  The state and the pending arrest decision carry over; the
+ * stagings are bitwise identical, z-pairs agree to FP32 rounding. */
+int sky_engine_set_staging(void* engine, int id, int tma, int pair);
+int sky_engine_get_staging(void* engine, int id, int* tma, int* pair);
 /* Steps between refreshes of a defect-corrected instance's FP64 correction
  * (precision 3; default 16, period >= 1).  A shorter period follows a field
  * that moves (a drifting soliton) at the cost of more FP64 gradient passes. */

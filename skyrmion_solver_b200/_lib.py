@@ -89,6 +89,8 @@ SIGNATURES = {
     "sky_engine_set_precision": ([_P, _I, _I], _I),
     "sky_engine_set_active": ([_P, _I, _I], _I),
     "sky_engine_retile": ([_P, _I, _I], _I),
+    "sky_engine_set_staging": ([_P, _I, _I, _I], _I),
+    "sky_engine_get_staging": ([_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
     "sky_engine_get_xc": ([_P, _I], _I),
     "sky_engine_set_defect_period": ([_P, _I, _I], _I),
     "sky_engine_audit": ([_P, _I, _F64P], _I),

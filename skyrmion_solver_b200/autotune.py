@@ -1,16 +1,22 @@
-"""Autotuner for the engine's per-instance tiling.
+"""Autotuner for the engine's per-instance tiling and plane staging.
 
 The marching stage kernels split a lattice into (x-chunk, 8-row y, 32-column z)
 tiles; the x-chunk sets how many tiles one launch has (and so how evenly they
-spread over the 148 SMs) against how many halo planes each block re-reads.
-``sky_engine_add`` picks it with a cost model; this module measures instead:
-for one (theory, precision, lattice shape, device) it admits a probe instance,
-times a few steps per candidate chunk with CUDA events on the engine's stream
+spread over the 148 SMs) against how many halo planes each block re-reads.  The
+planes of a tile are staged either by TMA box copies or by per-thread cp.async
+copies, and an FP32 omega tile can run as z-pairs (16 x 8 threads, two z-sites
+each, packed FP32x2 arithmetic) instead of one site per thread (32 x 8).
+``sky_engine_add`` picks the chunk with a cost model and the staging from the
+library options; this module measures instead: for one (theory, precision,
+lattice shape, device) it admits a probe instance, times a few steps per
+candidate (staging, chunk) with CUDA events on the engine's stream
 (``Engine.time_stages``) and keeps the fastest.  Results are cached in a JSON
 file so that a serving process tunes each shape once.
 
 Tiling changes only the order of the per-tile energy partial sums, so a tuned
-instance follows the same trajectory as an untuned one (``tests/test_march.py``).
+instance follows the same trajectory as an untuned one (``tests/test_march.py``);
+the two stagings are bitwise identical and z-pairs agree to FP32 rounding
+(``tests/test_tma.py``).
 """
 from __future__ import annotations
 
@@ -84,9 +90,23 @@ def time_chunks(engine, iid, chunks, steps: int = 12, warm: int = 2) -> dict:
     return out
 
 
+def candidate_stagings(engine, iid, theory, precision: str) -> list:
+    """(tma, pair) stagings worth timing for an admitted instance: the admission's own, and
+    when it stages by TMA also cp.async and (FP32 omega) z-pair tiles."""
+    cur = engine.staging(iid)
+    out = [cur]
+    if cur[0]:
+        for st in ((True, False), (True, True), (False, False)):
+            if st in out or (st[1] and not (theory == "omega" and precision != "fp64")):
+                continue
+            out.append(st)
+    return out
+
+
 def tune(theory, p_i, p_f, precision: str = "fp32c", field=None, device: int = 0, cache: TuneCache | None = None,
          steps: int = 12) -> dict:
-    """Best x-chunk for one lattice shape; cached.  Returns {"xc", "ms_per_step", "timings"}."""
+    """Best (staging, x-chunk) for one lattice shape; cached.  Returns {"xc", "tma", "pair",
+    "ms_per_step", "timings"} (timings keyed "tma,pair,xc")."""
     from .engine import Engine
     cache = cache if cache is not None else TuneCache()
     key = shape_key(theory, precision, p_i, _device_name(device))
@@ -101,18 +121,27 @@ def tune(theory, p_i, p_f, precision: str = "fp32c", field=None, device: int = 0
     with Engine(device) as eng:
         iid = eng.add(theory, (np.asarray(p_i, np.int32), np.asarray(p_f, np.float64)), field, None,
                       precision=precision)
-        t = time_chunks(eng, iid, candidate_chunks(X), steps=steps)
+        t = {}
+        for st in candidate_stagings(eng, iid, theory, precision):
+            eng.set_staging(iid, *st)
+            for xc, ms in time_chunks(eng, iid, candidate_chunks(X), steps=steps).items():
+                t[(int(st[0]), int(st[1]), int(xc))] = ms
         best = min(t, key=t.get)
-        res = {"xc": int(best), "ms_per_step": float(t[best]), "timings": {str(k): v for k, v in t.items()}}
+        res = {"xc": best[2], "tma": best[0], "pair": best[1], "ms_per_step": float(t[best]),
+               "timings": {"%d,%d,%d" % k: v for k, v in t.items()}}
     cache.put(key, res)
     return res
 
 
 def apply(engine, iid, theory, precision: str, p_i, cache: TuneCache | None = None, device: int = 0) -> bool:
-    """Re-tile `iid` with a cached choice for its shape, if one exists; returns whether it did."""
+    """Re-tile (and re-stage) `iid` with a cached choice for its shape, if one exists; returns
+    whether it did.  A cached staging the instance cannot use (TMA switched off by option 2, or
+    a lattice that breaks its alignment rule) is skipped; the chunk is still applied."""
     cache = cache if cache is not None else TuneCache()
     hit = cache.get(shape_key(theory, precision, p_i, _device_name(device)))
-    if hit and hit.get("xc"):
-        engine.retile(iid, int(hit["xc"]))
-        return True
-    return False
+    if not hit or not hit.get("xc"):
+        return False
+    if "tma" in hit and (engine.staging(iid)[0] or not hit["tma"]):
+        engine.set_staging(iid, bool(hit["tma"]), bool(hit.get("pair", 0)))
+    engine.retile(iid, int(hit["xc"]))
+    return True

@@ -499,6 +499,7 @@ static int rebuild_group_t(Engine& e, Group& g) {
             d.step = o.step;
             d.arrested = o.arrested;
             d.cur = o.cur;
+            d.refresh = (o.refresh && d.Dlt != nullptr) ? 1 : 0;  // a pending defect refresh survives
         }
         h.group_slot = (int)k;
         if (h.comp) g.any_comp = true;
@@ -563,14 +564,17 @@ static void free_inst(HostInst& h) {
 // Whether an instance's planes can be staged by TMA box copies: the option is on,
 // the row pitch Z * sizeof(T) is a multiple of 16 bytes, and its (theory,
 // precision) uses wide rows (every one but FP64 rho).
-static bool tma_ok_for(const HostInst& h) {
-    return option(2) == 1 && wide_ok(h.prec, h.p.Z) && !(h.prec && theory_components(h.theory) > 5);
+static bool tma_possible(const HostInst& h) {
+    return wide_ok(h.prec, h.p.Z) && !(h.prec && theory_components(h.theory) > 5);
 }
+static bool tma_ok_for(const HostInst& h) { return option(2) == 1 && tma_possible(h); }
+// Whether an instance can run as z-pair tiles (TMA staging, FP32, omega).
+static bool pair_possible(const HostInst& h) { return h.prec == 0 && h.theory == SKY_THEORY_OMEGA; }
 
 static int alloc_inst(Engine& e, HostInst& h) {
     const size_t es = h.prec ? sizeof(double) : sizeof(float);
     h.tma = tma_ok_for(h);
-    h.pair = h.tma && option(3) == 1 && h.prec == 0 && h.theory == SKY_THEORY_OMEGA;
+    h.pair = h.tma && option(3) == 1 && pair_possible(h);
     const size_t fb = es * (size_t)h.C * (size_t)h.N;
     int bz, by, tx, per_sm;
     int rc0 = tile_shape(h.theory, h.prec, bz, by, tx, per_sm);
@@ -1075,12 +1079,38 @@ int sky_engine_retile(void* handle, int id, int xc) {
     h.xc_request = xc;
     h.xc = nxc;
     h.tnx = (h.p.X + nxc - 1) / nxc;
-    h.ntiles = ntiles;
-    h.tma = tma_ok_for(h);
-    h.pair = h.tma && option(3) == 1 && h.prec == 0 && h.theory == SKY_THEORY_OMEGA;
+    h.ntiles = ntiles;  // the staging (TMA, z-pairs) carries over
     Group& g = e->groups[h.theory][h.prec];
     if ((rc = rebuild_group(*e, g))) return rc;
     return init_instance(*e, h, 2);
+}
+
+int sky_engine_set_staging(void* handle, int id, int tma, int pair) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e) return invalid("null engine");
+    HostInst* hp = find(e, id);
+    if (!hp) return invalid("unknown instance id");
+    if ((tma != 0 && tma != 1) || (pair != 0 && pair != 1)) return invalid("tma and pair must be 0 or 1");
+    HostInst& h = *hp;
+    if (tma && !tma_possible(h))
+        return invalid("TMA staging needs Z * element size a multiple of 16 bytes (and no FP64 rho)");
+    if (pair && !(tma && pair_possible(h))) return invalid("z-pair tiles need TMA staging and an FP32 omega instance");
+    if (h.tma == tma && h.pair == pair) return SKY_OK;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    h.tma = tma;
+    h.pair = pair;
+    return rebuild_group(*e, e->groups[h.theory][h.prec]);  // keeps the control state
+}
+
+int sky_engine_get_staging(void* handle, int id, int* tma, int* pair) {
+    Engine* e = reinterpret_cast<Engine*>(handle);
+    if (!e || !tma || !pair) return invalid("null argument");
+    HostInst* hp = find(e, id);
+    if (!hp) return invalid("unknown instance id");
+    *tma = hp->tma;
+    *pair = hp->pair;
+    return SKY_OK;
 }
 
 int sky_engine_audit(void* handle, int id, double* out2) {

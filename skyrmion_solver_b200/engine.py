@@ -151,6 +151,16 @@ class Engine:
         """x-chunk of the marching kernels for this instance (0 = automatic)."""
         self._call("sky_engine_retile", int(iid), int(xc))
 
+    def set_staging(self, iid: int, tma: bool, pair: bool = False):
+        """Plane staging of this instance: TMA box copies or cp.async, and z-pair tiles."""
+        self._call("sky_engine_set_staging", int(iid), int(bool(tma)), int(bool(pair)))
+
+    def staging(self, iid: int) -> tuple:
+        """(tma, pair) of this instance."""
+        t, q = ctypes.c_int(0), ctypes.c_int(0)
+        self._call("sky_engine_get_staging", int(iid), ctypes.byref(t), ctypes.byref(q))
+        return bool(t.value), bool(q.value)
+
     def set_defect_period(self, iid: int, period: int):
         """Steps between refreshes of an fp32d instance's FP64 correction (default 16)."""
         self._call("sky_engine_set_defect_period", int(iid), int(period))

@@ -309,6 +309,26 @@ def test_fp32d_tracks_fp64(engine, name):
         engine.remove(b)
 
 
+def test_admission_keeps_the_pending_refresh_flag():
+    """An admission rebuilds the group's descriptors; the refresh flag of a defect-corrected
+    member (set by the advance of step 16, read by the next step: its l2 is not taken as l1
+    when arrested) must survive, so the member's trajectory does not depend on the admission.
+    The omega golden flow is arrested on every step from step 6."""
+    from skyrmion_solver_b200.engine import Engine
+    d, F, V, p_i, p_f = _inputs("omega")
+    out = []
+    for admit in (False, True):
+        with Engine(0) as eng:
+            a = eng.add("omega", (p_i, p_f), F, V, precision="fp32d")
+            eng.step(16)
+            if admit:
+                eng.add("omega", (p_i, p_f), F, V, precision="fp32d")
+            eng.step(4)
+            assert eng.stats(a).arrested
+            out.append((eng.stats(a).energy, eng.read(a, velocity=False)[0]))
+    assert out[0][0] == out[1][0] and np.array_equal(out[0][1], out[1][1])
+
+
 def test_fp32d_schedule_reaches_the_fp64_fixed_point():
     """The served schedule: defect-corrected FP32 steps, then FP64 until max|g| <= 1e-6, ends at the
     FP64 solve's energy; the plain FP32 gradient alone stalls near its noise floor (~2e-5 at h = 0.2).

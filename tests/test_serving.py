@@ -221,9 +221,18 @@ def test_autotune_picks_a_measured_chunk(tmp_path):
     th, p_i, p_f = params_for("omega", (40, 24, 36))
     cache = autotune.TuneCache(str(tmp_path / "tune.json"))
     res = autotune.tune("omega", p_i, p_f, "fp32c", cache=cache, steps=4)
-    assert res["xc"] in [int(k) for k in res["timings"]]
+    keys = [tuple(int(v) for v in k.split(",")) for k in res["timings"]]
+    assert (res["tma"], res["pair"], res["xc"]) in keys
+    assert {(k[0], k[1]) for k in keys} == {(1, 0), (1, 1), (0, 0)}   # TMA, z-pairs, cp.async
     assert res["ms_per_step"] == min(res["timings"].values())
     assert autotune.tune("omega", p_i, p_f, "fp32c", cache=cache) == res      # cached
+    from skyrmion_solver_b200.engine import Engine
+    from tests.test_march import inputs
+    F, _ = inputs(int(p_i[5]), (40, 24, 36), seed=3)
+    with Engine(0) as eng:
+        i = eng.add("omega", (p_i, p_f), F, None, precision="fp32c")
+        assert autotune.apply(eng, i, "omega", "fp32c", p_i, cache)
+        assert eng.staging(i) == (bool(res["tma"]), bool(res["pair"])) and eng.xc(i) == res["xc"]
 
 
 @pytest.mark.gpu

@@ -117,3 +117,36 @@ def test_z_pair_tiles_track_one_site_tiles(precision):
         for x, y in zip(ra, rb):
             assert abs(x - y) <= 2e-6 * max(1.0, abs(y)), (ra, rb)
     assert G.rel_err(fa, fb) <= 2e-6
+
+
+def test_staging_switch_keeps_the_trajectory():
+    """sky_engine_set_staging between steps (TMA -> cp.async -> TMA) leaves an instance on the
+    trajectory of one that stays on TMA staging, bitwise; invalid stagings are refused."""
+    from skyrmion_solver_b200._lib import SkyInvalidArgument
+    from skyrmion_solver_b200.engine import Engine
+    dims = (23, 13, 44)
+    th, p_i, p_f = params_for("omega", dims)
+    F, V = inputs(int(p_i[5]), dims, seed=5)
+    out = []
+    for switch in (False, True):
+        with Engine(0) as eng:
+            i = eng.add("omega", (p_i, p_f), F, V, precision="fp32d")
+            assert eng.staging(i)[0]
+            for n in range(6):
+                if switch and n in (2, 4):
+                    eng.set_staging(i, n == 4)
+                eng.step(1)
+            out.append((eng.stats(i).energy, eng.stats(i).gabs, eng.read(i)))
+            if switch:
+                with pytest.raises(SkyInvalidArgument):
+                    eng.set_staging(i, False, True)          # z-pairs need TMA
+                j = eng.add("nuclear", params_for("nuclear", dims)[1:], F[:4], None, precision="fp32")
+                with pytest.raises(SkyInvalidArgument):
+                    eng.set_staging(j, True, True)           # z-pairs: omega only
+                k = eng.add("omega", params_for("omega", (23, 13, 37))[1:], inputs(5, (23, 13, 37), seed=1)[0],
+                            None, precision="fp32")
+                with pytest.raises(SkyInvalidArgument):
+                    eng.set_staging(k, True)                 # Z * 4 bytes is not a multiple of 16
+    (ea, ga, (fa, va)), (eb, gb, (fb, vb)) = out
+    assert ea == eb and ga == gb
+    assert np.array_equal(fa, fb) and np.array_equal(va, vb)
