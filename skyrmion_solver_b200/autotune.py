@@ -118,14 +118,21 @@ def tune(theory, p_i, p_f, precision: str = "fp32c", field=None, device: int = 0
         from .initial import exp_profile, hedgehog, with_extra_components
         h = (float(p_f[3]), float(p_f[4]), float(p_f[5]))
         field = with_extra_components(hedgehog((X, Y, Z), h, exp_profile(1.5)), C)
+    packed = (np.asarray(p_i, np.int32), np.asarray(p_f, np.float64))
     with Engine(device) as eng:
-        iid = eng.add(theory, (np.asarray(p_i, np.int32), np.asarray(p_f, np.float64)), field, None,
-                      precision=precision)
+        probe = eng.add(theory, packed, field, None, precision=precision)
+        stagings = candidate_stagings(eng, probe, theory, precision)
+        eng.remove(probe)
         t = {}
-        for st in candidate_stagings(eng, iid, theory, precision):
-            eng.set_staging(iid, *st)
-            for xc, ms in time_chunks(eng, iid, candidate_chunks(X), steps=steps).items():
-                t[(int(st[0]), int(st[1]), int(xc))] = ms
+        # every candidate starts from the same field: a flow that has begun to arrest runs
+        # cheaper steps (stage 2 skips an arrested step), which would favour later candidates
+        for st in stagings:
+            for xc in candidate_chunks(X):
+                iid = eng.add(theory, packed, field, None, precision=precision)
+                eng.set_staging(iid, *st)
+                (got, ms), = time_chunks(eng, iid, [xc], steps=steps).items()
+                t[(int(st[0]), int(st[1]), int(got))] = ms
+                eng.remove(iid)
         best = min(t, key=t.get)
         res = {"xc": best[2], "tma": best[0], "pair": best[1], "ms_per_step": float(t[best]),
                "timings": {"%d,%d,%d" % k: v for k, v in t.items()}}
