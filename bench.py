@@ -782,33 +782,52 @@ def serve_requests(n, rate, seed, mix, bmax, max_side, tol, max_steps):
 
 
 def run_serve(args):
+    """The serving stream on N GPUs (torchrun for N > 1): every rank draws the same request
+    list and serves its share (replicas.partition: least work so far, in arrival order) on
+    its own engine; no data crosses GPUs.  The serial plain FP64 baseline solves each rank's
+    share one request after another on that rank's GPU.  Rank 0 merges and prints."""
     import numpy as np
     import torch
     from skyrmion_solver_b200.core.simulation import Simulation
     from skyrmion_solver_b200.engine import Engine
+    from skyrmion_solver_b200.replicas import gather_objects, max_over_ranks, merge_served, partition
     from skyrmion_solver_b200.serving import Server
     from skyrmion_solver_b200.theories._init_common import build_device_field, seed_omega
-    torch.cuda.set_device(0)
-    dev = torch.device("cuda", 0)
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
     mix = dict(kv.split(":") for kv in args.mix.split(","))
     mix = {k: float(v) for k, v in mix.items()}
     reqs = serve_requests(args.requests, args.rate, args.seed, mix, args.bmax, args.max_side, GRAD_TOL,
                           args.max_steps)
+    mine = {r.rid for r in partition([r for r, _, _ in reqs], world)[rank]}
+    my_reqs = [x for x in reqs if x[0].rid in mine]
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
     # 1. continuous batching on the resident engine
-    with Engine(0) as eng:
+    barrier()
+    with Engine(local) as eng:
         srv = Server(eng, chunk=64, fp32_mode=args.schedule, defect_period=args.defect_period,
                      switch_factor=args.switch_factor, plateau_chunks=args.plateau_chunks)
-        for r, _, _ in reqs:
+        for r, _, _ in my_reqs:
             srv.submit(r)
         torch.cuda.synchronize()
         served = {x.rid: x for x in srv.run()}
-        summ = srv.summary()
+    barrier()
     # 2. the same requests solved one after another on the plain FP64 drop-in path
     serial = {}
     t_all = 0.0
-    for r, prm, th in ([] if args.no_serial else reqs):
+    for r, prm, th in ([] if args.no_serial else my_reqs):
         sim = Simulation(prm, th)
-        f0 = build_device_field(r.theory, r.p_i, r.p_f, r.init)      # the same field the server built
+        f0 = build_device_field(r.theory, r.p_i, r.p_f, r.init, device=local)   # the field the server built
         if r.theory == "omega":
             seed_omega(f0, r.p_i, r.p_f)
         sim.Field.copy_(f0)
@@ -832,48 +851,60 @@ def run_serve(args):
         t_all += dt
         serial[r.rid] = dict(status=status, steps=n, energy=e, seconds=dt)
         del sim
-    # relative to max(|E|, 1): a configuration that unwinds to the vacuum (E -> 0) compares absolutely
     if args.no_serial:
         serial = {k: dict(status=None, steps=None, energy=math.nan, seconds=None) for k in served}
-    rel = [abs(served[k].energy - serial[k]["energy"]) / max(abs(serial[k]["energy"]), 1.0) for k in served
-           if served[k].status == "converged" and serial[k]["status"] == "converged"]
-    n_serial = sum(v["status"] == "converged" for v in serial.values())
-    serial_sps = n_serial / t_all if t_all > 0 else None
+    # merge over ranks
+    theory_of = {r.rid: r.theory for r, _, _ in reqs}
+    rows = [(k, served[k].status, served[k].latency, served[k].finished) for k in sorted(served)]
+    summ = merge_served(gather_objects(rows))
+    summ["batch_steps_per_rank"] = max_over_ranks([srv.steps_run], device=dev)[0]
+    per_request = [dict(rid=k, theory=theory_of[k], sites=int(reqs[k][0].p_i[6]), rank=rank,
+                        energy=served[k].energy, baryon=served[k].baryon, serial_energy=serial[k]["energy"],
+                        served_steps=served[k].steps, fp32_steps=served[k].fp32_steps,
+                        latency_s=served[k].latency, status=served[k].status,
+                        serial_status=serial[k]["status"], serial_steps=serial[k]["steps"],
+                        serial_s=serial[k]["seconds"]) for k in sorted(served)]
+    per_request = sorted((d for part in gather_objects(per_request) for d in part), key=lambda d: d["rid"])
+    serial_wall = max_over_ranks([t_all], device=dev)[0]     # the ranks' serial solves run side by side
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return 0
+    # relative to max(|E|, 1): a configuration that unwinds to the vacuum (E -> 0) compares absolutely
+    rel = [abs(d["energy"] - d["serial_energy"]) / max(abs(d["serial_energy"]), 1.0) for d in per_request
+           if d["status"] == "converged" and d["serial_status"] == "converged"]
+    n_serial = sum(d["serial_status"] == "converged" for d in per_request)
+    serial_sps = n_serial / serial_wall if serial_wall > 0 else None
     # per theory: counts by outcome and time-to-converged percentiles, served and serial
     by_theory = {}
-    for th_name in sorted({r.theory for r, _, _ in reqs}):
-        ks = [r.rid for r, _, _ in reqs if r.theory == th_name]
-        lat = np.array([served[k].latency for k in ks if served[k].status == "converged"])
+    for th_name in sorted(set(theory_of.values())):
+        ds = [d for d in per_request if d["theory"] == th_name]
+        lat = np.array([d["latency_s"] for d in ds if d["status"] == "converged"])
         by_theory[th_name] = {
-            "requests": len(ks),
-            "served": {st: sum(served[k].status == st for k in ks) for st in ("converged", "failed", "not_converged")},
-            "serial": {st: sum(serial[k]["status"] == st for k in ks) for st in ("converged", "failed",
-                                                                                  "not_converged")},
+            "requests": len(ds),
+            "served": {st: sum(d["status"] == st for d in ds) for st in ("converged", "failed", "not_converged")},
+            "serial": {st: sum(d["serial_status"] == st for d in ds) for st in ("converged", "failed",
+                                                                                 "not_converged")},
             "p50_s": float(np.percentile(lat, 50)) if lat.size else None,
             "p99_s": float(np.percentile(lat, 99)) if lat.size else None}
-    line = {"mode": "serve", "metric": METRIC, "unit": UNIT,
+    line = {"mode": "serve", "metric": METRIC, "unit": UNIT, "n_gpus": world,
             "config": {"workload": "poisson_stream", "requests": args.requests, "rate_per_s": args.rate,
                        "mix": mix, "B": f"1..{args.bmax}", "max_side": args.max_side,
                        "h": "0.2 (rho 0.05)", "dt": "0.2 h (rho 0.05 h)",
                        "tol_max_abs_gradient": GRAD_TOL, "defect_period": args.defect_period or 16,
+                       "routing": "replicas.partition (least work first, arrival order)" if world > 1 else None,
                        "schedule": {"fp64": "fp64 throughout",
                                     "fp32d": "fp32d until max|g| <= tol or a stall, then fp64"}.get(
                            args.schedule, f"{args.schedule} until {args.switch_factor:g} x the FP32 gradient "
                                           f"floor or a stall of {args.plateau_chunks * 64} steps, then fp64")},
             "served": summ,
             "by_theory": by_theory,
-            "serial_plain_fp64": None if args.no_serial else {"converged": n_serial, "seconds": t_all,
+            "serial_plain_fp64": None if args.no_serial else {"converged": n_serial, "seconds": serial_wall,
                                                               "solves_per_s": serial_sps},
             "speedup_solves_per_s": (summ["solves_per_s"] / serial_sps) if (summ["solves_per_s"] and serial_sps)
             else None,
             "max_rel_energy_diff_vs_plain_fp64": max(rel) if rel else None,
-            "per_request": [dict(rid=k, theory=reqs[k][0].theory, sites=int(reqs[k][0].p_i[6]),
-                                 energy=served[k].energy, baryon=served[k].baryon,
-                                 serial_energy=serial[k]["energy"],
-                                 served_steps=served[k].steps, fp32_steps=served[k].fp32_steps,
-                                 latency_s=served[k].latency, status=served[k].status,
-                                 serial_steps=serial[k]["steps"], serial_s=serial[k]["seconds"])
-                            for k in sorted(served)]}
+            "per_request": per_request}
     emit(line)
     return 0
 

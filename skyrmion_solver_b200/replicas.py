@@ -49,3 +49,38 @@ def partition(requests, world: int):
         out[r].append(req)
         heapq.heappush(heap, (load + request_cost(req), r))
     return out
+
+
+def gather_objects(obj, group=None) -> list:
+    """`obj` of every rank in rank order, on every rank ([obj] without a process group)."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return [obj]
+    out = [None] * dist.get_world_size(group)
+    dist.all_gather_object(out, obj, group=group)
+    return out
+
+
+def merge_served(per_rank) -> dict:
+    """Whole-job serving summary from each rank's results, given as lists of
+    (rid, status, latency_s, finished_s) with `finished` on the rank's own clock, which
+    starts at a common barrier.  Counts add up; the job's wall time is the latest finish
+    on any rank; solves/s = converged requests / that wall time; p50 / p99 are over every
+    converged request's time-to-converged."""
+    import numpy as np
+    rows = [r for part in per_rank for r in part]
+    lat = np.array([r[2] for r in rows if r[1] == "converged"], dtype=np.float64)
+    wall = max((r[3] for r in rows), default=0.0)
+    done = int(lat.size)
+    return {
+        "requests": len(rows),
+        "converged": done,
+        "failed": sum(r[1] == "failed" for r in rows),
+        "not_converged": sum(r[1] == "not_converged" for r in rows),
+        "solves_per_s": done / wall if wall > 0 else None,
+        "p50_s": float(np.percentile(lat, 50)) if done else None,
+        "p99_s": float(np.percentile(lat, 99)) if done else None,
+        "wall_s": wall,
+        "ranks": len(per_rank),
+        "requests_per_rank": [len(p) for p in per_rank],
+    }

@@ -36,7 +36,11 @@ def _worker(rank, world, port, q):
         sm = sum_over_ranks([float(rank + 1)])
         reqs = [_req(k, 0.01 * k, 48 + 16 * (k % 3)) for k in range(10)]
         mine = [r.rid for r in partition(reqs, world)[rank]]
-        q.put((rank, mx, sm, mine))
+        # each rank "serves" its share: converged after 1 + rid seconds, failed for rid 3
+        from skyrmion_solver_b200.replicas import gather_objects, merge_served
+        rows = [(k, "failed" if k == 3 else "converged", 1.0 + k, 0.01 * k + 1.0 + k) for k in mine]
+        merged = merge_served(gather_objects(rows))
+        q.put((rank, mx, sm, mine, merged))
     finally:
         dist.destroy_process_group()
 
@@ -52,10 +56,18 @@ def test_two_gloo_ranks_reduce_and_split():
     ps = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
     for p in ps:
         p.start()
-    out = dict((r, (mx, sm, mine)) for r, mx, sm, mine in (q.get(timeout=120) for _ in ps))
+    out = dict((r, (mx, sm, mine, merged)) for r, mx, sm, mine, merged in (q.get(timeout=120) for _ in ps))
     for p in ps:
         p.join(timeout=60)
         assert p.exitcode == 0
     assert out[0][0] == out[1][0] == [2.0, 10.0]
     assert out[0][1] == out[1][1] == [3.0]
     assert sorted(out[0][2] + out[1][2]) == list(range(10)) and not set(out[0][2]) & set(out[1][2])
+    m = out[0][3]
+    assert m == out[1][3]                                  # every rank holds the same summary
+    assert (m["requests"], m["converged"], m["failed"], m["ranks"]) == (10, 9, 1, 2)
+    assert m["wall_s"] == pytest.approx(0.09 + 10.0)       # the latest finish, request 9
+    assert m["solves_per_s"] == pytest.approx(9 / 10.09)
+    lat = [1.0 + k for k in range(10) if k != 3]
+    assert m["p50_s"] == pytest.approx(float(np.percentile(lat, 50)))
+    assert sorted(m["requests_per_rank"]) == sorted([len(out[0][2]), len(out[1][2])])
