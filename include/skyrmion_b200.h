@@ -56,10 +56,16 @@ const char* sky_last_error(void);
  * kernels.  Key 1: x-chunk of those marching launches (0 = automatic).  Key 2:
  * staging of the resident engine's stage kernels, 1 = tensor-memory-accelerator
  * box copies (default; lattices whose Z gives 16-byte row pitches), 0 = per-thread
- * cp.async copies; it applies to instances admitted (or re-tiled) afterwards.
+ * cp.async copies; it applies to instances admitted afterwards
+ * (sky_engine_set_staging changes one instance).
  * Key 3: 1 = the FP32 stages of theories whose gradient needs no mixed second
  * derivatives (omega) compute two adjacent z-sites per thread with packed FP32x2
  * arithmetic; 0 = one site per thread (default).  Applies at admission.
+ * Key 4: 1 = the engine's stage launches use programmatic dependent launch, so a
+ * launch is scheduled while the previous one's last blocks finish (each waits for
+ * the previous launch before reading its results), 0 = plain stream order (default;
+ * inside the step graphs the two measure the same).
+ * It applies to the next step call (captured graphs are rebuilt).
  * Process-wide; not synchronised with launches in flight on other threads. */
 int sky_set_option(int key, int value);
 int sky_get_option(int key);

@@ -71,6 +71,7 @@ struct Engine {
     cudaGraphExec_t graph = nullptr;   // kGraphSteps steps
     cudaGraphExec_t graph1 = nullptr;  // one step (the remainder of a step call)
     bool graph_valid = false;
+    int graph_pdl = -1;                // option 4 when the graphs were captured
     int64_t bytes = 0;
     int* d_status = nullptr;  // device error word the stage kernels set (bit 0: a TMA wait gave up)
 };
@@ -159,8 +160,24 @@ static int launch_stage_w(const Group& g, int t_begin, int t_end, cudaStream_t s
     using M = MShape<Th, T, WIDE>;
     const size_t smem = stage_smem<Th, T, STAGE, WIDE, LO, TMA>();
     const dim3 block(PAIR ? PairShape<M>::TZ : M::BZ, M::BY);
-    k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO, TMA, PAIR><<<blocks, block, smem, st>>>(
-        d, d, g.d_tile_inst, t_begin, t_end, tail ? g.d_done : nullptr);
+    auto kern = k_march_stage<Th, M, T, STAGE, march_minb<Th, T>(), LO, TMA, PAIR>;
+    int* done = tail ? g.d_done : nullptr;
+    if (option(4) == 1) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.gridDim = dim3(blocks);
+        cfg.blockDim = block;
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return check_cuda(cudaLaunchKernelEx(&cfg, kern, static_cast<const InstDesc<T>*>(d), d,
+                                             static_cast<const int*>(g.d_tile_inst), t_begin, t_end, done),
+                          "launch engine stage", __LINE__);
+    }
+    kern<<<blocks, block, smem, st>>>(d, d, g.d_tile_inst, t_begin, t_end, done);
     return check_cuda(cudaGetLastError(), "launch engine stage", __LINE__);
 }
 
@@ -751,6 +768,7 @@ static int build_graph(Engine& e) {
             if (!e.groups[t][pr].members.empty() && (rc = setup_group(e.groups[t][pr]))) return rc;
     if ((rc = capture_steps(e, kGraphSteps, &e.graph)) || (rc = capture_steps(e, 1, &e.graph1))) return rc;
     e.graph_valid = true;
+    e.graph_pdl = option(4);
     return SKY_OK;
 }
 
@@ -1181,6 +1199,7 @@ int sky_engine_step(void* handle, int nsteps) {
     cudaSetDevice(e->device);
     int rc;
     int done = 0;
+    if (e->graph_valid && e->graph_pdl != option(4)) e->graph_valid = false;
     if (nsteps > 0 && !e->graph_valid && (rc = build_graph(*e))) return rc;
     while (nsteps - done >= kGraphSteps) {
         if ((rc = check_cuda(cudaGraphLaunch(e->graph, e->stream), "graph launch", __LINE__))) return rc;

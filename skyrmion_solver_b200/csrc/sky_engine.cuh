@@ -527,6 +527,8 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
         }
         __syncthreads();
     }
+    // the previous launch of the step (its tail writes the control state) must be complete
+    grid_dep_wait();
     if constexpr (CENTRE) {
         cst.buf = sm + M::template smem_bytes_tma<T>(3) / sizeof(T);
         cst.bar = &tma_bar[2];
@@ -615,6 +617,7 @@ __global__ void __launch_bounds__(stage_threads<M, PAIR>(), MINB)
         }
         if (!ok) break;
     }
+    grid_dep_launch();  // the next launch may be scheduled while the last blocks finish
     // tail (done != null, stages 1 and 4): the last block of the launch to finish runs the
     // advance (stage 4) or the control (stage 1: reductions, statistics, arrest decision) of
     // every active instance of the launch, one warp per instance, so a step needs no separate
@@ -671,6 +674,7 @@ __global__ void __launch_bounds__(M::NTHREADS, 1)
     static_assert(TBY % M::BY == 0, "sub-tiles of the engine tile's rows");
     extern __shared__ __align__(16) unsigned char smraw[];
     double* sm = reinterpret_cast<double*>(smraw);
+    grid_dep_wait();
     for (int t = t_begin + blockIdx.x; t < t_end; t += gridDim.x) {
         const int ii = __ldg(tile_inst + t);
         const InstDesc<float>& in = insts[ii];

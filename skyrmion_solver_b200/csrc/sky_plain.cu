@@ -324,8 +324,8 @@ int choose_xc(int X, int tiles_yz, int resident) {
 // z-pair tiles for the FP32 stages of theories without mixed derivatives (1 = on; off
 // by default: on the omega 128^3 stages they issue a third fewer instructions per site
 // but run at half the resident warps, and measured no faster).
-static int g_options[4] = {1, 0, 1, 0};
-int option(int key) { return (key >= 0 && key < 4) ? g_options[key] : 0; }
+static int g_options[5] = {1, 0, 1, 0, 0};
+int option(int key) { return (key >= 0 && key < 5) ? g_options[key] : 0; }
 
 // ---------------------------------------------------------------------------
 // templated launchers
@@ -652,7 +652,9 @@ int sky_set_option(int key, int value) {
     if (key == 1 && value < 0) return invalid("option 1 (x-chunk) must be >= 0");
     if (key == 2 && value != 0 && value != 1) return invalid("option 2 takes 0 (cp.async staging) or 1 (TMA staging)");
     if (key == 3 && value != 0 && value != 1) return invalid("option 3 takes 0 (one site per thread) or 1 (z-pairs)");
-    if (key < 0 || key > 3) return invalid("unknown option key");
+    if (key == 4 && value != 0 && value != 1)
+        return invalid("option 4 takes 0 (stream order) or 1 (programmatic dependent launch)");
+    if (key < 0 || key > 4) return invalid("unknown option key");
     g_options[key] = value;
     return SKY_OK;
 }

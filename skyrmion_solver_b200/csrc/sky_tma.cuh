@@ -80,6 +80,15 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start while the previous kernel of the stream finishes.  Before it
+// reads anything that kernel wrote it waits for its completion (and memory flush);
+// without the launch attribute the wait returns at once.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// This block has done the work the next kernel may overlap: once every block of the
+// grid has signalled (or exited), the dependent kernel may be scheduled.
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ void prefetch_tmap(const TmaMap* map) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(&map->m) : "memory");
 }

@@ -150,3 +150,33 @@ def test_staging_switch_keeps_the_trajectory():
     (ea, ga, (fa, va)), (eb, gb, (fb, vb)) = out
     assert ea == eb and ga == gb
     assert np.array_equal(fa, fb) and np.array_equal(va, vb)
+
+
+def test_programmatic_dependent_launch_equals_stream_order():
+    """Library option 4 (stage launches with programmatic dependent launch, graph-captured)
+    against plain stream order: bitwise identical statistics and fields over twenty steps
+    (a defect refresh at step 16, arrests), for FP32 and FP64 instances in one engine."""
+    from skyrmion_solver_b200 import _lib
+    from skyrmion_solver_b200.engine import Engine
+    dims = (23, 13, 44)
+    runs = []
+    old = int(_lib.load().sky_get_option(4))
+    try:
+        for pdl in (1, 0):
+            _lib.call("sky_set_option", 4, pdl)
+            with Engine(0) as eng:
+                ids = []
+                for name, prec in (("omega", "fp32d"), ("nuclear", "fp64"), ("rho", "fp32")):
+                    th, p_i, p_f = params_for(name, dims)
+                    F, V = inputs(int(p_i[5]), dims, seed=7)
+                    ids.append(eng.add(name, (p_i, p_f), F, V, precision=prec))
+                eng.step(13)
+                eng.step(7)
+                runs.append([(eng.stats(i).energy, eng.stats(i).gabs, eng.read(i, velocity=False)[0]) for i in ids])
+    finally:
+        _lib.call("sky_set_option", 4, old)
+    for a, b in zip(*runs):
+        assert a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2])
+    from skyrmion_solver_b200._lib import SkyInvalidArgument
+    with pytest.raises(SkyInvalidArgument):
+        _lib.call("sky_set_option", 4, 2)
