@@ -345,7 +345,7 @@ static int launch_control(const Group& g, int ib, int ie, int mode, cudaStream_t
 
 
 // Defect refresh of the group's defect-corrected FP32 instances (those whose
-// refresh flag the advance kernel just set; the others' tiles are skipped).
+// refresh flag the stage-4 advance just set; the others' tiles are skipped).
 template <template <typename> class Th, bool WIDE>
 static int launch_defect_t(const Group& g, cudaStream_t st) {
     using M = MarchShape<Th<double>::C, march_by<Th, double>(), WIDE && march_wide_allowed<Th, double>()>;
@@ -1387,8 +1387,8 @@ int sky_engine_time_stages(void* handle, int nsteps, double* ms_out) {
     ms_out[1] = acc[kKindS2] / nsteps;
     ms_out[2] = acc[kKindS3] / nsteps;
     ms_out[3] = acc[kKindS4] / nsteps;
-    ms_out[4] = acc[kKindControl] / nsteps;
-    ms_out[5] = acc[kKindAdvance] / nsteps;
+    ms_out[4] = 0.0;  // the control and the advance run inside stages 1 and 4
+    ms_out[5] = 0.0;
     return SKY_OK;
 }
 

@@ -204,14 +204,14 @@ __device__ __forceinline__ void finalize_site(int64_t s, int64_t N, const S* __r
 }
 
 // ---------------------------------------------------------------------------
-// Control: one block per instance.  Reduces the stage-1 partials (energy and
-// baryon number of the field entering this step) and the previous step's
-// stage-4 gradient partials, records StepStats and sets the arrest flag.
+// Control of one instance: reduces the stage-1 partials (energy and baryon number
+// of the field entering this step) and the previous step's stage-4 gradient
+// partials, records StepStats and sets the arrest flag.
 // ---------------------------------------------------------------------------
 // mode 0: end of a step (arrest decision); 1: admission (step 0, no arrest);
 // 2: resume after a precision change (keeps the pending arrest decision).
-// The control work of one instance, by one warp (the control kernel, or warp 0 of the
-// block that finished an instance's last stage-1 tile): lane-strided compensated sums of
+// The work is one warp's (the control kernel, or a warp of the last block to finish a
+// stage-1 launch, one warp per instance): lane-strided compensated sums of
 // the per-tile partials and a fixed shuffle tree, so the order depends on the tile count
 // only.  The partials are read through L2: in the stage kernel they were written by
 // other blocks of the same launch.
