@@ -117,3 +117,36 @@ def test_reference_kernels_and_drop_in_agree_at_config_size(key):
         assert abs(er - eo) <= STEP_TOL * abs(er), (s, er, eo)
         assert abs(errr - erro) <= STEP_TOL * max(1.0, abs(errr)), (s, errr, erro)
     assert G.rel_err(ours.Field.cpu().numpy(), ref.Field.copy_to_host()) <= STEP_TOL
+
+
+def test_config1_time_step_diverges_in_the_reference_too():
+    """The nuclear 64^3 configuration's dt = 0.5 h is beyond RK4's stability limit for the
+    reference's own code: its unmodified Simulation (Numba-CUDA kernels) and this package's
+    drop-in path both blow up, at the same step, from the same seeded field."""
+    import math
+    import torch
+    from skyrmion_solver_b200.core.simulation import Simulation as OurSimulation
+    th, p, cfg = _configured("nuclear64")
+    theories, Simulation, _ = R.load(("nuclear",))
+    ours = OurSimulation(p, th)
+    ours.initialize(cfg)
+    torch.cuda.synchronize()
+    kw = {k: getattr(p, k) for k in ("xlen", "ylen", "zlen", "lsx", "lsy", "lsz", "xsize", "ysize", "zsize",
+                                     "time_step", "killkinen")}
+    ref = Simulation(theories["nuclear"].params.Params(**kw), theories["nuclear"])
+    ref.Field.copy_to_device(np.ascontiguousarray(ours.Field.cpu().numpy()))
+    ref.Velocity.copy_to_device(np.zeros(ours.Velocity.numel()))
+    er, eo = ref.observables()["energy"], ours.observables()["energy"]
+    first = {}
+    for n in range(1, 121):
+        if "ref" not in first:
+            er, _ = ref.step(er)
+            if not math.isfinite(er):
+                first["ref"] = n
+        if "ours" not in first:
+            eo, _ = ours.step(eo)
+            if not math.isfinite(eo):
+                first["ours"] = n
+        if len(first) == 2:
+            break
+    assert len(first) == 2 and first["ref"] == first["ours"], first
