@@ -927,6 +927,7 @@ def run_batch(args):
     eng = Engine(0)
     sites = {"nuclear": 0, "rho": 0}
     comps = 0
+    members = {}
     for k in range(args.instances):
         name = "nuclear" if rng.random() < 0.5 else "rho"
         B = int(rng.integers(1, 9))
@@ -941,21 +942,49 @@ def run_batch(args):
         p_i, p_f = np.asarray(p_i, np.int32), np.asarray(p_f, np.float64)
         f = build_host_field(name, p_i, p_f, {"mode": "cloud", "count": B, "seed": 100 + k, "scale": 1.5,
                                                 "vacuum_shell": 2})
-        eng.add(name, (p_i, p_f), f, None, precision=FAST)
+        members[eng.add(name, (p_i, p_f), f, None, precision=FAST)] = (name, p_i, p_f)
         sites[name] += side ** 3
         comps += int(p_i[5]) * side ** 3
     N = sites["nuclear"] + sites["rho"]
     warmup = max(3, args.warmup)
     K = args.steps
-    eng.step(warmup)
     stream = torch.cuda.ExternalStream(eng.stream)
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    eng.step(K)
-    b.record(stream)
-    b.synchronize()
-    ms = a.elapsed_time(b) / K
+
+    def timed():
+        eng.step(warmup)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.step(K)
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / K
+
+    ms = timed()
+    tuned = None
+    if args.tune:
+        # the autotuner's (staging, x-chunk) per lattice shape, measured on probe instances
+        # (untimed), then applied to every instance of the batch in place
+        from skyrmion_solver_b200 import autotune
+        cache = autotune.TuneCache(None)
+        choices = {}
+        default = {iid: (eng.staging(iid), eng.xc(iid)) for iid in members}
+        for iid, (name, p_i, p_f) in members.items():
+            res = autotune.tune(name, p_i, p_f, FAST, cache=cache, steps=6)
+            autotune.apply(eng, iid, name, FAST, p_i, cache)
+            choices[f"{name} {int(p_i[0])}^3"] = {k: res[k] for k in ("xc", "tma", "pair")}
+        ms_tuned = timed()
+        # the flow has moved on (arrested steps are cheaper): time the defaults again, now
+        for iid, (st, xc) in default.items():
+            eng.set_staging(iid, *st)
+            eng.retile(iid, xc)
+        ms_default_after = timed()
+        # batch-aware chunking: a full batch fills the GPU with tiles anyway, so whole-lattice
+        # x-chunks (fewest halo re-reads) may beat the per-shape choice made for an instance alone
+        for iid, (name, p_i, p_f) in members.items():
+            eng.retile(iid, int(p_i[0]))
+        tuned = {"ms_per_step": ms_tuned, "defaults_ms_per_step_after": ms_default_after,
+                 "whole_lattice_chunks_ms_per_step": timed(), "choices": choices}
     stages = eng.time_stages(max(3, min(20, K)))
     stats = eng.stats_all()
     finite = sum(math.isfinite(st.energy) for st in stats.values())
@@ -963,7 +992,7 @@ def run_batch(args):
           "field_values": comps, "device_bytes": eng.bytes, "ms_per_step": ms,
           "site_steps_per_s": N / (ms * 1e-3), "algorithmic_gbs": 18 * 4 * comps / (ms * 1e-3) / 1e9,
           "stage_ms": stages, "finite_instances": finite, "launches_per_step": eng.launches_per_step,
-          "precision": FAST, "dt": {"nuclear": "0.2 h", "rho": "0.05 h"}})
+          "precision": FAST, "dt": {"nuclear": "0.2 h", "rho": "0.05 h"}, "tuned": tuned})
     eng.close()
     return 0
 
@@ -1142,6 +1171,7 @@ def main():
     ap.add_argument("--render", action="store_true", help="headless viewer: volume builder and ray-march")
     ap.add_argument("--batch", action="store_true", help="48 mixed pion / rho instances in one engine")
     ap.add_argument("--instances", type=int, default=48)
+    ap.add_argument("--tune", action="store_true", help="batch: also time the batch with autotuned staging and chunks")
     ap.add_argument("--dynamics", action="store_true", help="RK4 dynamics of two boosted tori with energy audit")
     ap.add_argument("--side", type=int, default=192)
     ap.add_argument("--theory", choices=("coulomb", "nuclear", "omega"), default="coulomb",
