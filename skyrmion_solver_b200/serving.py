@@ -11,8 +11,8 @@ admission) arrive open-loop.  The loop:
   a time (graph-replayed launches, all theories and sizes in the same step);
 * after each chunk reads every instance's latest statistics in one call and
   - switches an FP32 instance to FP64 once its gradient max-norm reaches
-    ``switch_tol`` (by default twice the estimated FP32 stencil noise floor,
-    ``fp32_gradient_floor``) or has not improved by 1 % over
+    ``switch_tol`` (by default ``switch_factor`` = 2 times the estimated FP32
+    stencil noise floor, ``fp32_gradient_floor``) or has not improved by 1 % over
     ``plateau_chunks`` chunks, so the last digits are polished in FP64,
   - retires an instance whose FP64 gradient max-norm is at or below ``tol``
     (converged), whose energy is not finite (failed) or that used up
@@ -136,7 +136,9 @@ class Server:
         self.polish = polish
         # "fp32d" (compensated, defect-corrected), "fp32c" (compensated), "fp32", or "fp64" (no FP32 phase)
         self.fp32_mode = fp32_mode
-        self.tune_cache = tune_cache  # autotune.TuneCache: re-tile admitted instances with cached choices
+        # autotune.TuneCache: re-stage and re-tile admitted instances with cached per-shape choices
+        # (tuned for an instance alone; in a full batch the admission's chunks measured faster)
+        self.tune_cache = tune_cache
         self.keep_fields = keep_fields
         self.defect_period = defect_period  # refresh period of fp32d corrections (None: the engine's 16)
         self.clock = clock
