@@ -309,6 +309,38 @@ def test_fp32d_tracks_fp64(engine, name):
         engine.remove(b)
 
 
+def test_many_instances_in_one_group_equal_alone():
+    """Eleven instances of one (theory, precision) group, more than the warps of the block
+    that runs their controls and advances at the end of stages 1 and 4 (8 warps, so some
+    warps take two instances), one of them paused: each active one steps bitwise as it does
+    alone, and the paused one does not move."""
+    from skyrmion_solver_b200.engine import Engine
+    from tests.test_march import inputs, params_for
+    dims = [(20 + k, 12 + (k % 3), 36) for k in range(11)]
+    setups = []
+    for k, d in enumerate(dims):
+        th, p_i, p_f = params_for("omega", d)
+        F, V = inputs(int(p_i[5]), d, seed=20 + k)
+        setups.append((p_i, p_f, F, V))
+    alone = []
+    for p_i, p_f, F, V in setups:
+        with Engine(0) as eng:
+            i = eng.add("omega", (p_i, p_f), F, V, precision="fp32")
+            eng.step(5)
+            alone.append((eng.stats(i).energy, eng.stats(i).gabs, eng.read(i, velocity=False)[0]))
+    with Engine(0) as eng:
+        ids = [eng.add("omega", (p_i, p_f), F, V, precision="fp32") for p_i, p_f, F, V in setups]
+        eng.set_active(ids[4], False)
+        eng.step(5)
+        for k, i in enumerate(ids):
+            st, f = eng.stats(i), eng.read(i, velocity=False)[0]
+            if k == 4:
+                assert st.step == 0
+                continue
+            assert (st.energy, st.gabs) == alone[k][:2], k
+            assert np.array_equal(f, alone[k][2]), k
+
+
 def test_admission_keeps_the_pending_refresh_flag():
     """An admission rebuilds the group's descriptors; the refresh flag of a defect-corrected
     member (set by the advance of step 16, read by the next step: its l2 is not taken as l1
